@@ -1,0 +1,234 @@
+"""gahhg_b200 - point-in-spherical-polygon tests on one NVIDIA B200.
+
+Host-side mirror of the reference's objects (source/GPISPPolygon.cuh,
+source/GPISPTP.cuh, source/GPISPAHHG.cuh) over the C ABI of libgahhg.so:
+
+    poly = GPISPPolygon(); poly.loadPolyFromTXT("NA0.txt")
+    tp = GPISPTP(); tp.loadTPFromCSV("query.csv")
+    g = GPISP(poly, tp, semantics="reference")
+    g.createAHHGInit(); g.createAHHG(15); g.classifyAHHG(); g.test()
+    g.getStat(); g.exportStat2TXT("report.txt", 1); tp.exportResult2CSV("result.csv")
+
+and a numpy-level API (Polygon, Grid) used by the tests and the benchmark.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import (BORDER_DTYPE, CELL_DTYPE, LEVEL_DTYPE, QUERY_AUTO, QUERY_FP32_FILTER,
+                   QUERY_FP64_FILTER, QUERY_REFERENCE_FP64, SEMANTICS_EXACT, SEMANTICS_REFERENCE,
+                   GahhgError, check)
+
+CELL_UNDEFINED, CELL_OUT, CELL_IN = 0, 1, 2
+
+
+class Polygon:
+    """A loaded spherical polygon (rings re-oriented as the reference does)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def from_file(cls, path):
+        h = ctypes.c_void_p()
+        check(_lib.lib().gahhg_polygon_load(str(path).encode(), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_rings(cls, rings):
+        """rings: list of (k, 2) lon/lat arrays without closing vertex; ring 0 is outer."""
+        ll = np.ascontiguousarray(np.concatenate([np.asarray(r, dtype=np.float64).reshape(-1, 2) for r in rings]))
+        offs = np.zeros(len(rings) + 1, dtype=np.int64)
+        offs[1:] = np.cumsum([len(r) for r in rings])
+        h = ctypes.c_void_p()
+        check(_lib.lib().gahhg_polygon_from_rings(_lib.ptr(ll), _lib.ptr(offs), len(rings), ctypes.byref(h)))
+        return cls(h)
+
+    @property
+    def num_edges(self):
+        return _lib.lib().gahhg_polygon_num_edges(self._h)
+
+    def export(self):
+        n = self.num_edges
+        xyz = np.zeros((n, 3), dtype=np.float64)
+        pe = np.zeros((n, 2), dtype=np.int32)
+        check(_lib.lib().gahhg_polygon_export(self._h, _lib.ptr(xyz), _lib.ptr(pe)))
+        return xyz, pe
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _lib.lib().gahhg_polygon_free(self._h)
+            self._h = None
+
+
+def load_points(path):
+    """GPISPTP::loadTPFromCSV -> (n, 2) float64 lon/lat."""
+    h = ctypes.c_void_p()
+    L = _lib.lib()
+    check(L.gahhg_points_load(str(path).encode(), ctypes.byref(h)))
+    n = L.gahhg_points_count(h)
+    out = np.zeros((n, 2), dtype=np.float64)
+    if n:
+        ctypes.memmove(out.ctypes.data, L.gahhg_points_lonlat(h), n * 16)
+    L.gahhg_points_free(h)
+    return out
+
+
+class Grid:
+    """The hexagon hierarchy (+ the exact-label lattice for exact semantics)."""
+
+    def __init__(self, polygon, semantics=SEMANTICS_EXACT, max_depth=15, auto_depth=True, device=0,
+                 verbose=False, lattice_top=0, lattice_leaf=0):
+        L = _lib.lib()
+        o = _lib.BuildOpts()
+        L.gahhg_build_opts_init(ctypes.byref(o))
+        o.max_depth = max_depth
+        o.auto_depth = 1 if auto_depth else 0
+        o.semantics = semantics
+        o.device = device
+        o.verbose = 1 if verbose else 0
+        o.lattice_top = lattice_top
+        o.lattice_leaf = lattice_leaf
+        self.polygon = polygon  # the native grid keeps a pointer to it
+        self.semantics = semantics
+        h = ctypes.c_void_p()
+        check(L.gahhg_build(polygon._h, ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+
+    def classify(self):
+        check(_lib.lib().gahhg_classify(self._h))
+        return self
+
+    def query(self, lonlat, precision=QUERY_AUTO):
+        ll = np.ascontiguousarray(np.asarray(lonlat, dtype=np.float64).reshape(-1, 2))
+        out = np.zeros(len(ll), dtype=np.uint8)
+        check(_lib.lib().gahhg_query(self._h, _lib.ptr(ll), len(ll), _lib.ptr(out), precision))
+        return out
+
+    def query_device(self, d_lonlat, n, d_labels, precision=QUERY_AUTO, stream=0, sync=False):
+        """Device pointers (ints), e.g. from torch tensors' data_ptr()."""
+        check(_lib.lib().gahhg_query_device(self._h, ctypes.c_void_p(d_lonlat), n, ctypes.c_void_p(d_labels),
+                                            precision, ctypes.c_void_p(stream), 1 if sync else 0))
+
+    def stats(self):
+        s = _lib.Stats()
+        check(_lib.lib().gahhg_stats_get(self._h, ctypes.byref(s)))
+        return s.as_dict()
+
+    @property
+    def depth(self):
+        return _lib.lib().gahhg_grid_depth(self._h)
+
+    def export(self):
+        """(levels, V, B, C, refs) as numpy arrays."""
+        L = _lib.lib()
+        d = self.depth
+        lv = np.zeros(d, dtype=LEVEL_DTYPE)
+        L.gahhg_grid_export(self._h, _lib.ptr(lv), None, None, None, None)
+        last = lv[-1]
+        nv = int(last["vstart"] + last["vnum"])
+        nb = int(last["bstart"] + last["bnum"])
+        nc = int(last["cstart"] + last["cnum"])
+        nr = int(last["rnum"])
+        V = np.zeros((nv, 3), dtype=np.float64)
+        B = np.zeros(nb, dtype=BORDER_DTYPE)
+        C = np.zeros(nc, dtype=CELL_DTYPE)
+        R = np.zeros(max(nr, 1), dtype=np.int32)
+        check(L.gahhg_grid_export(self._h, _lib.ptr(lv), _lib.ptr(V), _lib.ptr(B), _lib.ptr(C), _lib.ptr(R)))
+        return lv, V, B, C, R[:nr]
+
+    def report_append(self, polyfile, tpfile, npoints, path, to_stdout=False):
+        check(_lib.lib().gahhg_report_append(self._h, str(polyfile).encode(), str(tpfile).encode(), npoints,
+                                             str(path).encode(), 1 if to_stdout else 0))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _lib.lib().gahhg_grid_free(self._h)
+            self._h = None
+
+
+def write_result(path, labels):
+    labels = np.ascontiguousarray(labels, dtype=np.uint8)
+    check(_lib.lib().gahhg_result_write(str(path).encode(), _lib.ptr(labels), len(labels)))
+
+
+def grid0():
+    V = np.zeros((80, 3), dtype=np.float64)
+    B = np.zeros(240, dtype=BORDER_DTYPE)
+    C = np.zeros(42, dtype=CELL_DTYPE)
+    check(_lib.lib().gahhg_grid0_export(_lib.ptr(V), _lib.ptr(B), _lib.ptr(C)))
+    return V, B, C
+
+
+# ---------------------------------------------------------------------------
+# Mirror of the reference's host objects (names and call order of
+# source/GPISP.cu:15-70 and source/GPISPAHHG.cuh:59-75).
+
+class GPISPPolygon:
+    def __init__(self):
+        self.poly = None
+
+    def loadPolyFromTXT(self, filename):
+        """0 on success, -1 on failure (message printed), as the reference."""
+        try:
+            self.poly = Polygon.from_file(filename)
+        except GahhgError:
+            return -1
+        self.filename = str(filename)
+        return 0
+
+    @property
+    def pv_num(self):
+        return self.poly.num_edges
+
+
+class GPISPTP:
+    def __init__(self):
+        self.tp = None
+        self.result = None
+
+    def loadTPFromCSV(self, filename):
+        try:
+            self.tp = load_points(filename)
+        except GahhgError:
+            return -1
+        self.filename = str(filename)
+        return 0
+
+    @property
+    def tpNum(self):
+        return 0 if self.tp is None else len(self.tp)
+
+    def exportResult2CSV(self, filename):
+        write_result(filename, self.result)
+
+
+class GPISP:
+    def __init__(self, polygon, tp, semantics=SEMANTICS_REFERENCE, precision=QUERY_AUTO):
+        self.pPolygon = polygon
+        self.pTP = tp
+        self.semantics = semantics
+        self.precision = precision
+        self.grid = None
+        self.maxDepth = 15
+
+    def createAHHGInit(self):
+        pass  # capacities and the level-0 grid are set up inside createAHHG
+
+    def createAHHG(self, maxdepth=15):
+        self.grid = Grid(self.pPolygon.poly, semantics=self.semantics, max_depth=maxdepth)
+
+    def classifyAHHG(self):
+        self.grid.classify()
+
+    def test(self):
+        self.pTP.result = self.grid.query(self.pTP.tp, self.precision)
+
+    def getStat(self):
+        self.stat = self.grid.stats()
+        return self.stat
+
+    def exportStat2TXT(self, filename, desttype=1):
+        self.grid.report_append(self.pPolygon.filename, self.pTP.filename, self.pTP.tpNum, filename,
+                                to_stdout=(desttype == 0))

@@ -1,0 +1,429 @@
+// api.cpp - the C ABI (include/gahhg.h) over the host objects.
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <ctime>
+
+#include "gahhg_internal.h"
+
+namespace gahhg {
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char* fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+const char* last_error() { return g_err; }
+
+double now_seconds()
+{
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+gahhg_status Polygon::upload()
+{
+    if (d_pv) return GAHHG_OK;
+    if (pv_num <= 0) {
+        set_error("polygon has no edges");
+        return GAHHG_ERR_ARG;
+    }
+    GAHHG_CUDA_TRY(cudaMalloc(&d_pv, sizeof(D3) * pv_num));
+    GAHHG_CUDA_TRY(cudaMalloc(&d_pe, sizeof(int) * 2 * pv_num));
+    GAHHG_CUDA_TRY(cudaMemcpy(d_pv, pv.data(), sizeof(D3) * pv_num, cudaMemcpyHostToDevice));
+    GAHHG_CUDA_TRY(cudaMemcpy(d_pe, pe.data(), sizeof(int) * 2 * pv_num, cudaMemcpyHostToDevice));
+    return GAHHG_OK;
+}
+
+Polygon::~Polygon()
+{
+    if (d_pv) cudaFree(d_pv);
+    if (d_pe) cudaFree(d_pe);
+}
+
+void free_query_layout(void* p);
+size_t query_layout_bytes(const void* p);
+void scan_state_destroy(void* state);
+
+Grid::~Grid()
+{
+    V.release();
+    B.release();
+    C.release();
+    refs.release();
+    cell_a.release();
+    cell_b.release();
+    off_a.release();
+    off_b.release();
+    edge_cur.release();
+    edge_prev.release();
+    edge_cnt.release();
+    edge_off.release();
+    ref_cell.release();
+    ref_flag.release();
+    ref_edge.release();
+    type_old.release();
+    type_cur.release();
+    type_next.release();
+    if (d_err) cudaFree(d_err);
+    if (d_counts) cudaFree(d_counts);
+    if (h_counts) cudaFreeHost(h_counts);
+    scan_state_destroy(scan_state);
+    free_query_layout(qlayout);
+    lattice_free(lattice);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+static void fill_stats(Grid* g)
+{
+    gahhg_stats& s = g->stats;
+    const Level& L = g->levels[g->gnum - 1];
+    s.depth = g->gnum;
+    s.pv_num = g->poly->pv_num;
+    s.vnum = L.vstart + L.vnum;
+    s.bnum = L.bstart + L.bnum;
+    s.cnum = L.cstart + L.cnum;
+    s.rnum = L.rnum;
+    // sizeof(GAHHG) + sizeof(GAHHGGrid)*gnum + sizeof(GPISPParam) + sizeof(GPISPStat)
+    // on x64 (source/GPISPAHHG.cu:2100): 144 + 28*gnum + 552 + 96
+    s.cpu_space = 792 + 28 * g->gnum;
+    s.gpu_min_space = 24 * s.vnum + 48 * s.bnum + 28 * s.cnum + 4 * s.rnum;
+    s.gamma = g->gamma;
+    s.lattice_bytes = (long long)lattice_bytes(g->lattice);
+}
+
+}  // namespace gahhg
+
+using namespace gahhg;
+
+extern "C" {
+
+void gahhg_build_opts_init(gahhg_build_opts* o)
+{
+    if (!o) return;
+    memset(o, 0, sizeof(*o));
+    o->max_depth = 15;
+    o->auto_depth = 1;
+    o->semantics = GAHHG_SEMANTICS_EXACT;
+    o->lattice_top = 0;
+    o->lattice_leaf = 0;
+    o->device = 0;
+    o->verbose = 0;
+}
+
+const char* gahhg_last_error(void) { return last_error(); }
+int gahhg_abi_version(void) { return GAHHG_ABI_VERSION; }
+
+gahhg_status gahhg_polygon_load(const char* path, gahhg_polygon** out)
+{
+    if (!path || !out) return GAHHG_ERR_ARG;
+    gahhg_polygon* p = new gahhg_polygon();
+    gahhg_status s = load_polygon_file(path, &p->p);
+    if (s != GAHHG_OK) {
+        delete p;
+        return s;
+    }
+    *out = p;
+    return GAHHG_OK;
+}
+
+gahhg_status gahhg_polygon_from_rings(const double* lonlat, const int64_t* ring_offsets, int nrings,
+                                      gahhg_polygon** out)
+{
+    if (!out) return GAHHG_ERR_ARG;
+    gahhg_polygon* p = new gahhg_polygon();
+    gahhg_status s = polygon_from_rings(lonlat, ring_offsets, nrings, &p->p);
+    if (s != GAHHG_OK) {
+        delete p;
+        return s;
+    }
+    *out = p;
+    return GAHHG_OK;
+}
+
+int gahhg_polygon_num_edges(const gahhg_polygon* p) { return p ? p->p.pv_num : 0; }
+
+gahhg_status gahhg_polygon_export(const gahhg_polygon* p, double* xyz, int* pe)
+{
+    if (!p) return GAHHG_ERR_ARG;
+    if (xyz) memcpy(xyz, p->p.pv.data(), sizeof(D3) * p->p.pv_num);
+    if (pe) memcpy(pe, p->p.pe.data(), sizeof(int) * 2 * p->p.pv_num);
+    return GAHHG_OK;
+}
+
+void gahhg_polygon_free(gahhg_polygon* p) { delete p; }
+
+gahhg_status gahhg_points_load(const char* path, gahhg_points** out)
+{
+    if (!path || !out) return GAHHG_ERR_ARG;
+    gahhg_points* p = new gahhg_points();
+    gahhg_status s = load_points_file(path, &p->p);
+    if (s != GAHHG_OK) {
+        delete p;
+        return s;
+    }
+    *out = p;
+    return GAHHG_OK;
+}
+
+size_t gahhg_points_count(const gahhg_points* p) { return p ? p->p.lonlat.size() / 2 : 0; }
+const double* gahhg_points_lonlat(const gahhg_points* p) { return p ? p->p.lonlat.data() : nullptr; }
+void gahhg_points_free(gahhg_points* p) { delete p; }
+
+gahhg_status gahhg_build(const gahhg_polygon* poly, const gahhg_build_opts* opts, gahhg_grid** out)
+{
+    if (!poly || !out) {
+        set_error("gahhg_build: null argument");
+        return GAHHG_ERR_ARG;
+    }
+    gahhg_build_opts o;
+    if (opts)
+        o = *opts;
+    else
+        gahhg_build_opts_init(&o);
+    if (o.max_depth < 1 || o.max_depth > 30) {
+        set_error("max_depth must be in [1, 30]");
+        return GAHHG_ERR_ARG;
+    }
+    GAHHG_CUDA_TRY(cudaSetDevice(o.device));
+    gahhg_polygon* mp = const_cast<gahhg_polygon*>(poly);
+    GAHHG_TRY(mp->p.upload());
+    gahhg_grid* G = new gahhg_grid();
+    Grid* g = &G->g;
+    g->poly = &poly->p;
+    g->opts = o;
+    g->device = o.device;
+    cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        set_error("cudaStreamCreate: %s", cudaGetErrorString(e));
+        delete G;
+        return GAHHG_ERR_CUDA;
+    }
+    gahhg_status s = grid_build(g);
+    if (s == GAHHG_OK && o.semantics == GAHHG_SEMANTICS_EXACT) {
+        const double t0 = now_seconds();
+        s = lattice_build(g);
+        g->stats.lattice_s = now_seconds() - t0;
+    }
+    if (s != GAHHG_OK) {
+        delete G;
+        return s;
+    }
+    fill_stats(g);
+    *out = G;
+    return GAHHG_OK;
+}
+
+gahhg_status gahhg_classify(gahhg_grid* G)
+{
+    if (!G) return GAHHG_ERR_ARG;
+    GAHHG_CUDA_TRY(cudaSetDevice(G->g.device));
+    GAHHG_TRY(grid_classify(&G->g));
+    GAHHG_TRY(grid_prepare_query(&G->g));
+    fill_stats(&G->g);
+    return GAHHG_OK;
+}
+
+void gahhg_grid_free(gahhg_grid* G)
+{
+    if (!G) return;
+    cudaSetDevice(G->g.device);
+    delete G;
+}
+
+static gahhg_status run_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels, int precision,
+                              cudaStream_t s, uint64_t* d_counters)
+{
+    if (!g->classified) {
+        set_error("query before classify");
+        return GAHHG_ERR_STATE;
+    }
+    if (precision == GAHHG_QUERY_AUTO)
+        precision = g->lattice ? GAHHG_QUERY_FP32_FILTER : GAHHG_QUERY_REFERENCE_FP64;
+    if (precision == GAHHG_QUERY_REFERENCE_FP64) return grid_query_ref(g, d_lonlat, n, d_labels, s);
+    if (precision == GAHHG_QUERY_FP32_FILTER || precision == GAHHG_QUERY_FP64_FILTER) {
+        if (!g->lattice) {
+            set_error("exact precision needs a grid built with GAHHG_SEMANTICS_EXACT");
+            return GAHHG_ERR_STATE;
+        }
+        return lattice_query(g, d_lonlat, n, d_labels, precision, s, d_counters);
+    }
+    set_error("unknown precision %d", precision);
+    return GAHHG_ERR_ARG;
+}
+
+gahhg_status gahhg_query_device(gahhg_grid* G, const double* d_lonlat, size_t n, uint8_t* d_labels, int precision,
+                                void* stream, int sync)
+{
+    if (!G || (n && (!d_lonlat || !d_labels))) return GAHHG_ERR_ARG;
+    Grid* g = &G->g;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!sync) return run_query(g, d_lonlat, n, d_labels, precision, s, nullptr);
+    uint64_t* d_cnt = nullptr;
+    GAHHG_CUDA_TRY(cudaMallocAsync(&d_cnt, 4 * sizeof(uint64_t), s));
+    GAHHG_CUDA_TRY(cudaMemsetAsync(d_cnt, 0, 4 * sizeof(uint64_t), s));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    gahhg_status st = run_query(g, d_lonlat, n, d_labels, precision, s, d_cnt);
+    cudaEventRecord(e1, s);
+    uint64_t cnt[4] = {0, 0, 0, 0};
+    if (st == GAHHG_OK) {
+        cudaMemcpyAsync(cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, s);
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            set_error("query: %s", cudaGetErrorString(e));
+            st = GAHHG_ERR_CUDA;
+        }
+    }
+    float ms = 0.f;
+    if (st == GAHHG_OK) cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFreeAsync(d_cnt, s);
+    if (st != GAHHG_OK) return st;
+    g->stats.query_s = ms * 1e-3;
+    g->stats.query_points = (long long)n;
+    g->stats.esc_fp64 = (long long)cnt[0];
+    g->stats.esc_exact = (long long)cnt[1];
+    g->stats.boundary_points = (long long)cnt[2];
+    return GAHHG_OK;
+}
+
+gahhg_status gahhg_query(gahhg_grid* G, const double* lonlat, size_t n, uint8_t* labels, int precision)
+{
+    if (!G || (n && (!lonlat || !labels))) return GAHHG_ERR_ARG;
+    Grid* g = &G->g;
+    GAHHG_CUDA_TRY(cudaSetDevice(g->device));
+    cudaStream_t s = g->stream;
+    double* d_ll = nullptr;
+    uint8_t* d_lab = nullptr;
+    if (n) {
+        GAHHG_CUDA_TRY(cudaMallocAsync(&d_ll, n * 2 * sizeof(double), s));
+        GAHHG_CUDA_TRY(cudaMallocAsync(&d_lab, n, s));
+        GAHHG_CUDA_TRY(cudaMemcpyAsync(d_ll, lonlat, n * 2 * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    gahhg_status st = gahhg_query_device(G, d_ll, n, d_lab, precision, s, 1);
+    if (st == GAHHG_OK && n) {
+        cudaError_t e = cudaMemcpyAsync(labels, d_lab, n, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            set_error("query copy-out: %s", cudaGetErrorString(e));
+            st = GAHHG_ERR_CUDA;
+        }
+    }
+    if (d_ll) cudaFreeAsync(d_ll, s);
+    if (d_lab) cudaFreeAsync(d_lab, s);
+    cudaStreamSynchronize(s);
+    if (st == GAHHG_OK) {
+        long long in = 0;
+        for (size_t i = 0; i < n; i++) in += labels[i] == CELL_IN;
+        g->stats.in_count = in;
+    }
+    return st;
+}
+
+gahhg_status gahhg_stats_get(const gahhg_grid* G, gahhg_stats* s)
+{
+    if (!G || !s) return GAHHG_ERR_ARG;
+    *s = G->g.stats;
+    return GAHHG_OK;
+}
+
+int gahhg_grid_depth(const gahhg_grid* G) { return G ? G->g.gnum : 0; }
+
+gahhg_status gahhg_grid_export(const gahhg_grid* G, int* levels, double* v, void* b, void* c, int* refs)
+{
+    if (!G) return GAHHG_ERR_ARG;
+    const Grid* g = &G->g;
+    const Level& L = g->levels[g->gnum - 1];
+    GAHHG_CUDA_TRY(cudaSetDevice(g->device));
+    if (levels) memcpy(levels, g->levels.data(), sizeof(Level) * g->gnum);
+    if (v) GAHHG_CUDA_TRY(cudaMemcpy(v, g->V.ptr, sizeof(D3) * (L.vstart + L.vnum), cudaMemcpyDeviceToHost));
+    if (b) GAHHG_CUDA_TRY(cudaMemcpy(b, g->B.ptr, sizeof(Border) * (L.bstart + L.bnum), cudaMemcpyDeviceToHost));
+    if (c) GAHHG_CUDA_TRY(cudaMemcpy(c, g->C.ptr, sizeof(Cell) * (L.cstart + L.cnum), cudaMemcpyDeviceToHost));
+    if (refs && L.rnum) GAHHG_CUDA_TRY(cudaMemcpy(refs, g->refs.ptr, sizeof(int) * L.rnum, cudaMemcpyDeviceToHost));
+    return GAHHG_OK;
+}
+
+gahhg_status gahhg_grid0_export(double* v, void* b, void* c)
+{
+    std::vector<D3> V;
+    std::vector<Border> B;
+    std::vector<Cell> C;
+    build_grid0(V, B, C);
+    if (v) memcpy(v, V.data(), sizeof(D3) * V.size());
+    if (b) memcpy(b, B.data(), sizeof(Border) * B.size());
+    if (c) memcpy(c, C.data(), sizeof(Cell) * C.size());
+    return GAHHG_OK;
+}
+
+gahhg_status gahhg_report_append(const gahhg_grid* G, const char* polyfile, const char* tpfile, long long npoints,
+                                 const char* path, int dest_stdout)
+{
+    if (!G) return GAHHG_ERR_ARG;
+    const gahhg_stats& s = G->g.stats;
+    FILE* fp = stdout;
+    if (!dest_stdout) {
+        fp = fopen(path, "a");
+        if (!fp) {
+            printf("Can not open file %s\n.", path);
+            set_error("cannot open %s", path);
+            return GAHHG_ERR_IO;
+        }
+    }
+    // GPISP::exportStat2TXT (source/GPISPAHHG.cu:2115-2161)
+    time_t now = time(nullptr);
+    struct tm lt;
+    localtime_r(&now, &lt);
+    fprintf(fp, "\n----------------------------------------%d/%d/%d %d:%d:%d-----------------------------------------\n",
+            lt.tm_year + 1900, lt.tm_mon + 1, lt.tm_mday, lt.tm_hour, lt.tm_min, lt.tm_sec);
+    fprintf(fp, "\nPolygon file: %s\n", polyfile);
+    fprintf(fp, "Number of polygon vertice: %d\n", s.pv_num);
+    fprintf(fp, "Query point file: %s\n", tpfile);
+    fprintf(fp, "Number of query points: %d\n", (int)npoints);
+    fprintf(fp, "Depth of GAHHG: %d\n", s.depth);
+    fprintf(fp, "Time of preprocessing: %f seconds (creat GAHHG: %f seconds, classify GAHHG: %f seconds)\n",
+            s.pre_s, s.create_s, s.classify_s);
+    fprintf(fp, "Storage overhead of GAHHG on CPU: %d Bytes\n", s.cpu_space);
+    fprintf(fp, "Storage overhead of GAHHG on GPU: %d KB\n", (int)(s.gpu_min_space / 1000));
+    fprintf(fp, "Total test time for all query points: %f seconds\n", s.query_s);
+    fprintf(fp, "Average test time per query point: %.5e seconds\n", npoints ? s.query_s / npoints : 0.0);
+    fprintf(fp, "Test result: inside %d, outside %d\n", (int)s.in_count, (int)(npoints - s.in_count));
+    fprintf(fp, "\n---------------------------------------------------------------------------------------------------\n");
+    if (!dest_stdout) fclose(fp);
+    return GAHHG_OK;
+}
+
+gahhg_status gahhg_result_write(const char* path, const uint8_t* labels, size_t n)
+{
+    FILE* fp = fopen(path, "w");
+    if (!fp) {
+        printf("Can not open file %s\n.", path);
+        set_error("cannot open %s", path);
+        return GAHHG_ERR_IO;
+    }
+    // one "1\n" or "0\n" per point (source/GPISPTP.cu:92-96), written in blocks
+    std::vector<char> buf;
+    buf.reserve(1 << 20);
+    for (size_t i = 0; i < n; i++) {
+        buf.push_back(labels[i] == CELL_IN ? '1' : '0');
+        buf.push_back('\n');
+        if (buf.size() >= (1 << 20)) {
+            fwrite(buf.data(), 1, buf.size(), fp);
+            buf.clear();
+        }
+    }
+    if (!buf.empty()) fwrite(buf.data(), 1, buf.size(), fp);
+    fclose(fp);
+    return GAHHG_OK;
+}
+
+}  // extern "C"

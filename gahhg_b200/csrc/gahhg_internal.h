@@ -1,0 +1,172 @@
+// gahhg_internal.h - host-side objects behind the C ABI (include/gahhg.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "geom.cuh"
+#include "gahhg.h"
+
+namespace gahhg {
+
+// ---------------------------------------------------------------- errors --
+void set_error(const char* fmt, ...);
+const char* last_error();
+
+#define GAHHG_CUDA_TRY(expr)                                                          \
+    do {                                                                              \
+        cudaError_t e_ = (expr);                                                      \
+        if (e_ != cudaSuccess) {                                                      \
+            ::gahhg::set_error("%s:%d: %s: %s", __FILE__, __LINE__, #expr,            \
+                               cudaGetErrorString(e_));                               \
+            return GAHHG_ERR_CUDA;                                                    \
+        }                                                                             \
+    } while (0)
+
+#define GAHHG_TRY(expr)                              \
+    do {                                             \
+        gahhg_status s_ = (expr);                    \
+        if (s_ != GAHHG_OK) return s_;               \
+    } while (0)
+
+// Device word where kernels record problems instead of trapping: a walk that
+// hit its step limit, an index that would leave its array, a scan whose
+// look-back gave up.  Read by the host after each phase.
+struct DeviceErrors {
+    int walk_step_limit;
+    int walk_bad_index;
+    int scan_lookback_timeout;
+    int classify_no_converge;
+    int lattice_overflow;
+    int other;
+    int first_code;
+    int first_tid;
+};
+
+// Growable device array (explicit capacity, reallocated with a copy).
+template <class T> struct DevArray {
+    T* ptr = nullptr;
+    size_t cap = 0;
+    gahhg_status reserve(size_t n, cudaStream_t s, bool keep = true)
+    {
+        if (n <= cap) return GAHHG_OK;
+        size_t ncap = cap ? cap : 1024;
+        while (ncap < n) ncap *= 2;
+        T* np = nullptr;
+        if (cudaMalloc(&np, ncap * sizeof(T)) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("device allocation of %zu bytes failed", ncap * sizeof(T));
+            return GAHHG_ERR_NOMEM;
+        }
+        if (ptr) {
+            if (keep) GAHHG_CUDA_TRY(cudaMemcpyAsync(np, ptr, cap * sizeof(T), cudaMemcpyDeviceToDevice, s));
+            GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+            cudaFree(ptr);
+        }
+        ptr = np;
+        cap = ncap;
+        return GAHHG_OK;
+    }
+    void release()
+    {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        cap = 0;
+    }
+};
+
+// ---------------------------------------------------------------- polygon --
+struct Polygon {
+    int pv_num = 0;               // number of edges == number of ring vertices
+    int num_rings = 0;
+    std::vector<double> lonlat;   // per vertex lon, lat (degrees, as read)
+    std::vector<D3> pv;           // canonical XYZ
+    std::vector<int> pe;          // edge i = (pe[2i], pe[2i+1]), oriented
+    std::vector<int> ring_start;  // first vertex of each ring (num_rings + 1)
+    std::string path;
+    // device copies
+    D3* d_pv = nullptr;
+    int* d_pe = nullptr;
+    gahhg_status upload();
+    ~Polygon();
+};
+
+gahhg_status load_polygon_file(const char* path, Polygon* out);
+gahhg_status polygon_from_rings(const double* lonlat, const int64_t* ring_offsets, int nrings,
+                                Polygon* out);
+
+struct Points {
+    std::vector<double> lonlat;
+    std::string path;
+};
+gahhg_status load_points_file(const char* path, Points* out);
+
+// ------------------------------------------------------------ level-0 grid --
+void build_grid0(std::vector<D3>& V, std::vector<Border>& B, std::vector<Cell>& C);
+
+// --------------------------------------------------------------- the grid --
+struct Lattice;  // exact-semantics query index (lattice.cu)
+
+struct Grid {
+    const Polygon* poly = nullptr;
+    gahhg_build_opts opts{};
+    cudaStream_t stream = nullptr;
+    int device = 0;
+
+    std::vector<Level> levels;    // levels[0..gnum-1]
+    int gnum = 0;
+    float gamma = 0.f;
+
+    DevArray<D3> V;
+    DevArray<Border> B;
+    DevArray<Cell> C;
+    DevArray<int> refs;           // bottom-level cell -> edge CSR
+    // build scratch
+    DevArray<int> cell_a, cell_b, off_a, off_b;
+    DevArray<int> edge_cur, edge_prev, edge_cnt, edge_off, ref_cell, ref_flag, ref_edge;
+    DevArray<int> type_old, type_cur, type_next;
+    DeviceErrors* d_err = nullptr;
+    int* d_counts = nullptr;      // small device header of counts
+    int* h_counts = nullptr;      // pinned mirror
+    void* scan_state = nullptr;   // decoupled look-back tile status
+
+    // query-layout copies (FP64 reference-semantics query)
+    void* qlayout = nullptr;
+    Lattice* lattice = nullptr;
+
+    gahhg_stats stats{};
+    bool classified = false;
+
+    ~Grid();
+};
+
+gahhg_status grid_build(Grid* g);
+gahhg_status grid_classify(Grid* g);
+gahhg_status grid_query_ref(Grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels, cudaStream_t s);
+gahhg_status grid_prepare_query(Grid* g);
+gahhg_status check_device_errors(Grid* g, const char* phase);
+
+// exact engine
+gahhg_status lattice_build(Grid* g);
+gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels, int precision,
+                           cudaStream_t s, uint64_t* d_counters);
+void lattice_free(Lattice* L);
+size_t lattice_bytes(const Lattice* L);
+
+// scans (scan.cu)
+size_t scan_state_bytes(size_t n);
+gahhg_status scan_state_reserve(void** state, size_t max_n);
+void scan_state_destroy(void* state);
+gahhg_status scan_exclusive(const int* d_in, int* d_out, int n, int* d_total, void* state, DeviceErrors* err,
+                            cudaStream_t s);
+
+double now_seconds();
+
+}  // namespace gahhg
+
+struct gahhg_polygon { gahhg::Polygon p; };
+struct gahhg_points { gahhg::Points p; };
+struct gahhg_grid { gahhg::Grid g; };

@@ -1,0 +1,162 @@
+/*
+ * gahhg.h - C ABI of the B200 point-in-spherical-polygon engine.
+ *
+ * Drop-in for the build -> classify -> query path of GAHHG.  Each entry point
+ * names the reference interface it replaces (paths relative to the GAHHG
+ * repository).  Plain pointers and sizes only; `stream` is a cudaStream_t
+ * passed as void* (NULL = the legacy default stream).
+ *
+ * Labels are one byte per point with the reference's cell codes
+ * (source/GPISPParam.h:9-11): 0 = undefined, 1 = outside, 2 = inside.  The
+ * result CSV prints "1" for 2 and "0" otherwise (source/GPISPTP.cu:92-96).
+ *
+ * Two label semantics:
+ *   GAHHG_SEMANTICS_REFERENCE  the reference's epsilon rules, FP64, bit for bit
+ *                              (points within ~1e-8 rad of an edge follow the
+ *                              reference's tolerance tests);
+ *   GAHHG_SEMANTICS_EXACT      the exact sign of the orientation determinants
+ *                              on the canonical FP64 XYZ (gahhg_canon.h), with
+ *                              symbolic perturbation for exact zeros.
+ * Every call returns a status; gahhg_last_error() holds the message of the
+ * last failure on the calling thread.
+ */
+#ifndef GAHHG_H
+#define GAHHG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GAHHG_ABI_VERSION 1
+
+typedef enum {
+    GAHHG_OK = 0,
+    GAHHG_ERR_IO = -1,        /* file cannot be opened (reference returns -1) */
+    GAHHG_ERR_FORMAT = -2,    /* malformed POLYGON / CSV content (reference returns -1) */
+    GAHHG_ERR_ARG = -3,       /* invalid argument */
+    GAHHG_ERR_CUDA = -4,      /* CUDA runtime error */
+    GAHHG_ERR_DEVICE = -5,    /* a kernel reported a bounded failure (walk limit, bad index) */
+    GAHHG_ERR_NOMEM = -6,     /* device or host allocation failed */
+    GAHHG_ERR_STATE = -7,     /* call out of order (e.g. query before classify) */
+    GAHHG_ERR_CAPACITY = -8   /* request exceeds a fixed maximum */
+} gahhg_status;
+
+typedef enum { GAHHG_SEMANTICS_EXACT = 0, GAHHG_SEMANTICS_REFERENCE = 1 } gahhg_semantics;
+
+typedef enum {
+    GAHHG_QUERY_AUTO = 0,          /* exact grids: FP32 filter; reference grids: FP64 */
+    GAHHG_QUERY_FP32_FILTER = 1,   /* exact labels: FP32 certified filter -> FP64 -> expansion */
+    GAHHG_QUERY_FP64_FILTER = 2,   /* exact labels: FP64 certified filter -> expansion */
+    GAHHG_QUERY_REFERENCE_FP64 = 3 /* reference semantics: hierarchy descent in FP64 */
+} gahhg_precision;
+
+typedef struct gahhg_polygon gahhg_polygon;
+typedef struct gahhg_points gahhg_points;
+typedef struct gahhg_grid gahhg_grid;
+
+typedef struct {
+    int max_depth;      /* GPISPParam::maxDepth (source/GPISPParam.h:67), default 15 */
+    int auto_depth;     /* GPISPParam::autoDepth (:68), default 1 */
+    int semantics;      /* gahhg_semantics; GAHHG_SEMANTICS_EXACT builds both indexes */
+    int lattice_top;    /* exact index: top lattice columns (0 = automatic) */
+    int lattice_leaf;   /* exact index: max edges per leaf before refining (0 = automatic) */
+    int device;         /* CUDA device ordinal */
+    int verbose;        /* print the reference's progress lines */
+} gahhg_build_opts;
+
+typedef struct {
+    int depth;                 /* Depth of GAHHG (gnum) */
+    int pv_num;                /* Number of polygon vertice */
+    int vnum, bnum, cnum, rnum;
+    int cpu_space;             /* sizeof(GAHHG)+28*gnum+sizeof(GPISPParam)+sizeof(GPISPStat) on x64 */
+    int gpu_min_space;         /* 24 V + 48 B + 28 C + 4 R bytes */
+    float gamma;
+    double create_s;           /* createAHHGTime: level loop + edge dispatch */
+    double classify_s;         /* classifyAHHGTime */
+    double pre_s;              /* preTime = create + classify */
+    double lattice_s;          /* exact index build (0 for reference semantics) */
+    long long lattice_bytes;   /* device bytes of the exact index */
+    double query_s;            /* PISPTime of the last gahhg_query* call */
+    long long query_points;
+    long long in_count;        /* labels == 2 in the last query */
+    long long esc_fp64;        /* exact query: (point, edge) tests escalated to FP64 */
+    long long esc_exact;       /* exact query: tests escalated to expansion arithmetic */
+    long long boundary_points; /* exact query: points that ran crossing tests */
+} gahhg_stats;
+
+/* Defaults as in GPISPParam::GPISPParam (source/GPISPParam.h:64-77). */
+void gahhg_build_opts_init(gahhg_build_opts* o);
+
+/* ---- loaders ------------------------------------------------------------ */
+
+/* GPISPPolygon::loadPolyFromTXT (source/GPISPPolygon.cu:32-278): same
+ * validation, the same messages on stdout, rings re-oriented so the outer
+ * ring is counter-clockwise and holes clockwise (:209-264). */
+gahhg_status gahhg_polygon_load(const char* path, gahhg_polygon** out);
+/* In-memory variant: lonlat = 2 doubles per vertex, rings given without the
+ * closing vertex, ring r spans vertices [ring_offsets[r], ring_offsets[r+1]),
+ * ring 0 is the outer ring.  Same orientation rule as the file loader. */
+gahhg_status gahhg_polygon_from_rings(const double* lonlat, const int64_t* ring_offsets, int nrings,
+                                      gahhg_polygon** out);
+int gahhg_polygon_num_edges(const gahhg_polygon* p);
+/* Canonical vertex XYZ (3 doubles each) and edge list (2 ints each). */
+gahhg_status gahhg_polygon_export(const gahhg_polygon* p, double* xyz, int* pe);
+void gahhg_polygon_free(gahhg_polygon* p);
+
+/* GPISPTP::loadTPFromCSV (source/GPISPTP.cu:13-79): "lon,lat" per line. */
+gahhg_status gahhg_points_load(const char* path, gahhg_points** out);
+size_t gahhg_points_count(const gahhg_points* p);
+const double* gahhg_points_lonlat(const gahhg_points* p);
+void gahhg_points_free(gahhg_points* p);
+
+/* ---- build / classify --------------------------------------------------- */
+
+/* GPISP::createAHHGInit + createAHHG (source/GPISPAHHG.cu:1947-2015): the
+ * level-synchronous refinement on the GPU plus the bottom-level edge lists;
+ * for GAHHG_SEMANTICS_EXACT also the exact-label lattice.  The polygon must
+ * outlive the grid. */
+gahhg_status gahhg_build(const gahhg_polygon* poly, const gahhg_build_opts* opts, gahhg_grid** out);
+/* GPISP::classifyAHHG (source/GPISPAHHG.cu:2018-2059). */
+gahhg_status gahhg_classify(gahhg_grid* g);
+void gahhg_grid_free(gahhg_grid* g);
+
+/* ---- query -------------------------------------------------------------- */
+
+/* GPISP::test / kernel_PISP (source/GPISPAHHG.cu:2062-2085, 1422-1504).
+ * Device pointers: lonlat (2 doubles per point), labels (1 byte per point).
+ * Asynchronous on `stream`; statistics are updated when `sync` is non-zero. */
+gahhg_status gahhg_query_device(gahhg_grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels,
+                                int precision, void* stream, int sync);
+/* Host pointers: copies lon/lat in, labels out, timing the kernel alone as
+ * PISPTime does.  Synchronous. */
+gahhg_status gahhg_query(gahhg_grid* g, const double* lonlat, size_t n, uint8_t* labels, int precision);
+
+/* ---- statistics / report ------------------------------------------------ */
+
+gahhg_status gahhg_stats_get(const gahhg_grid* g, gahhg_stats* s);
+/* Level table: 7 ints per level (vstart vnum bstart bnum cstart cnum rnum). */
+int gahhg_grid_depth(const gahhg_grid* g);
+/* Grid arrays for inspection: levels, vertices (3 doubles), borders (48 B),
+ * cells (28 B), bottom-level refs.  Any pointer may be NULL. */
+gahhg_status gahhg_grid_export(const gahhg_grid* g, int* levels, double* v, void* b, void* c, int* refs);
+/* GPISP::exportStat2TXT (source/GPISPAHHG.cu:2115-2161): appends the report
+ * block to `path` (dest_stdout != 0 prints it instead). */
+gahhg_status gahhg_report_append(const gahhg_grid* g, const char* polyfile, const char* tpfile,
+                                 long long npoints, const char* path, int dest_stdout);
+/* GPISPTP::exportResult2CSV (source/GPISPTP.cu:81-99). */
+gahhg_status gahhg_result_write(const char* path, const uint8_t* labels, size_t n);
+
+/* The level-0 grid (80 vertices, 240 borders, 42 cells). */
+gahhg_status gahhg_grid0_export(double* v, void* b, void* c);
+
+const char* gahhg_last_error(void);
+int gahhg_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GAHHG_H */
