@@ -1,20 +1,1108 @@
-// lattice.cu - exact-semantics query index (placeholder until the exact engine lands).
+// lattice.cu - exact-label query index and query kernel.
+//
+// The reference answers a query by descending the hexagon hierarchy from 42
+// level-0 cells (kernel_PISP, source/GPISPAHHG.cu:1422-1504): about ten
+// dependent levels of plane tests per point.  Here the same question is
+// answered from a lattice over longitude/latitude that is indexed directly
+// from the input coordinates:
+//
+//   * top level: W x H cells of equal angular size (H = W/2) covering
+//     lon [-180,180) x lat [-90,90]; a cell's region is its rectangle of
+//     (lon, lat) mapped through the canonical conversion;
+//   * each cell owns a cap (center R = canonical XYZ of the cell center,
+//     radius 2 * (half-height + half-width * cos(center lat)) + margin), which
+//     contains the cell, every point within the margin of it, and the caps of
+//     all its descendants; a polygon edge is listed in a cell when it may meet
+//     the cap (conservative test);
+//   * a cell listing more than K edges is split 4 x 4, down to a depth limit;
+//   * every cell center has an exact label: the top row and each column are
+//     chained by the crossing parity of the arc between neighbouring centers
+//     (both ends lie in the union of the two caps), the first center is
+//     reached from a point just left of an outer-ring edge through six fixed
+//     hub points, and a child takes its parent's label XOR the parity of the
+//     arc parent-center -> child-center against the parent's edges.
+//
+// A query reads lon/lat (16 B), computes the top cell with two FP64
+// multiply-adds, follows inner nodes by exact power-of-two scaling, and
+//   - in a cell without edges writes the cell's label (no trigonometry);
+//   - in a leaf counts crossings of arc(R, q) with the leaf's edges:
+//       s2 = orient(A,B,q) = q.(A x B), s3 = orient(R,q,A) = q.(A x R),
+//       s4 = orient(R,q,B) = q.(B x R), s1 = orient(A,B,R) stored exactly;
+//     each sign is first taken in FP32 (q from __sincosf, vectors rounded to
+//     FP32) against a forward error bound, then in FP64 on the canonical q,
+//     then exactly (exact_pred.cuh).  Labels are therefore those of the exact
+//     oracle; the FP32 stage only decides when its bound proves the sign.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+
+#include "exact_pred.cuh"
+#include "gahhg_canon.h"
 #include "gahhg_internal.h"
 
 namespace gahhg {
-struct Lattice {
-    int unused;
+
+namespace {
+
+constexpr int TPB = 256;
+inline int blocks_for(long long n) { return (int)std::max(1LL, (n + TPB - 1) / TPB); }
+
+constexpr int FAN = 4;                     // children per axis
+constexpr uint32_t KIND_MASK = 0xC0000000u;
+constexpr uint32_t KIND_PURE = 0x00000000u;  // low bits: label (1 out, 2 in)
+constexpr uint32_t KIND_INNER = 0x80000000u;  // low 30 bits: first child node
+constexpr uint32_t KIND_LEAF = 0xC0000000u;  // low 30 bits: leaf index
+constexpr uint32_t INDEX_MASK = 0x3FFFFFFFu;
+
+// Margin (radians) between where the index arithmetic places a query and
+// where its canonical XYZ lies: index rounding (~1e-14), conversion error
+// (~1e-15), longitudes up to +-540 (2 pi' differs from 2 pi by 7.2e-9).
+constexpr double LOC_MARGIN = 2.0e-8;
+constexpr double RAD = GAHHG_PI_TRUNC / 180.0;  // degrees -> canonical radians (approx., bounds only)
+
+// Bound on |q32 - q| per component for q32 from __sincosf (documented error
+// 2^-21.41 on [-pi, pi]) of FP32-rounded canonical radians; see DESIGN.
+constexpr float E_Q32 = 2.0e-6f;
+constexpr float C32 = E_Q32 + 5.0f * 5.9604645e-8f;
+
+struct __align__(32) LeafRec {
+    double R[3];
+    uint32_t off;
+    uint16_t cnt;
+    uint8_t label;
+    uint8_t pad;
 };
-gahhg_status lattice_build(Grid* g)
+static_assert(sizeof(LeafRec) == 32, "LeafRec");
+
+struct EdgeRec {
+    float n1[3];  // A x B
+    float n2[3];  // A x R
+    float n3[3];  // B x R
+    uint32_t es;  // edge index | (orient(A,B,R) > 0) << 31
+};
+static_assert(sizeof(EdgeRec) == 40, "EdgeRec");
+
+struct Geo {
+    int W, H;
+    double dlon0, dlat0;  // degrees at level 0
+};
+
+// Node geometry from (level, ix, iy): center (degrees, exact), cap radius.
+struct NodeCap {
+    double R[3];
+    double r;
+    double lonc, latc;
+};
+
+__host__ __device__ inline double level_scale(int lvl)
 {
-    (void)g;
+    double s = 1.0;
+    for (int i = 0; i < lvl; i++) s *= FAN;
+    return s;
+}
+
+__host__ __device__ inline NodeCap node_cap(const Geo& g, int lvl, long long ix, long long iy)
+{
+    const double sc = level_scale(lvl);
+    const double dlon = g.dlon0 / sc, dlat = g.dlat0 / sc;
+    NodeCap c;
+    c.lonc = -180.0 + ((double)ix + 0.5) * dlon;
+    c.latc = -90.0 + ((double)iy + 0.5) * dlat;
+    gahhg_canon_vertex_xyz(c.lonc, c.latc, c.R);
+    double sa, ca;
+    gahhg_canon_sincos(gahhg_canon_rad(c.latc), &sa, &ca);
+    const double hlat = 0.5 * dlat * RAD, hlon = 0.5 * dlon * RAD;
+    c.r = 2.0 * (hlat + hlon * fabs(ca)) * (1.0 + 1e-9) + LOC_MARGIN + 1e-12;
+    return c;
+}
+
+// Moves R off a polygon vertex it coincides with (exact comparison).
+__host__ __device__ inline void nudge_center(const Geo& g, int lvl, NodeCap& c, const D3* pv, const int* pe,
+                                             const int* list, int cnt)
+{
+    const double sc = level_scale(lvl);
+    for (int tries = 0; tries < 8; tries++) {
+        bool hit = false;
+        for (int k = 0; k < cnt && !hit; k++) {
+            const int e = list[k];
+            const D3 a = pv[pe[2 * e]], b = pv[pe[2 * e + 1]];
+            hit = (a.x == c.R[0] && a.y == c.R[1] && a.z == c.R[2]) || (b.x == c.R[0] && b.y == c.R[1] && b.z == c.R[2]);
+        }
+        if (!hit) return;
+        c.lonc += g.dlon0 / sc * (1.0 / 1024.0);
+        c.latc += g.dlat0 / sc * (1.0 / 2048.0);
+        gahhg_canon_vertex_xyz(c.lonc, c.latc, c.R);
+    }
+}
+
+__host__ __device__ inline bool same3(const double* a, const D3& b) { return a[0] == b.x && a[1] == b.y && a[2] == b.z; }
+
+// Conservative: may arc AB (unit vectors) come within angle r of R?
+__host__ __device__ inline bool edge_hits_cap(const D3& A, const D3& B, const double* R, double r)
+{
+    const double chord = 2.0 * sin(0.5 * r) * (1.0 + 1e-9) + 1e-12;
+    const double c2 = chord * chord;
+    const double ax = A.x - R[0], ay = A.y - R[1], az = A.z - R[2];
+    if (ax * ax + ay * ay + az * az <= c2) return true;
+    const double bx = B.x - R[0], by = B.y - R[1], bz = B.z - R[2];
+    if (bx * bx + by * by + bz * bz <= c2) return true;
+    const D3 N = cross(A, B);
+    const double nn = sqrt(dot(N, N));
+    if (!(nn > 1e-300)) return false;
+    const double s = (N.x * R[0] + N.y * R[1] + N.z * R[2]) / nn;
+    if (fabs(s) > sin(r) * (1.0 + 1e-9) + 1e-12) return false;
+    const D3 Rv = d3(R[0], R[1], R[2]);
+    const double t1 = dot(cross(N, A), Rv), t2 = dot(cross(B, N), Rv);
+    const double tol = 1e-12 * nn;
+    return t1 >= -tol && t2 >= -tol;
+}
+
+__device__ inline double lat_of(const D3& p) { return asin(fmin(1.0, fmax(-1.0, p.y))) / RAD; }
+__device__ inline double lon_of(const D3& p) { return atan2(p.x, p.z) / RAD; }
+
+// Latitude/longitude box (degrees) of arc AB; full_lon when it may cross a pole.
+__device__ inline void arc_box(const D3& A, const D3& B, double& la0, double& la1, double& lo0, double& lo1,
+                               bool& full_lon)
+{
+    double a = lat_of(A), b = lat_of(B);
+    la0 = fmin(a, b);
+    la1 = fmax(a, b);
+    const D3 N = cross(A, B);
+    const double nn = sqrt(dot(N, N));
+    if (nn > 1e-300) {
+        const D3 n = N * (1.0 / nn);
+        D3 V = d3(-n.y * n.x, 1.0 - n.y * n.y, -n.y * n.z);  // highest point of the great circle
+        const double vv = sqrt(dot(V, V));
+        if (vv > 1e-300) {
+            V = V * (1.0 / vv);
+            for (int sgn = 0; sgn < 2; sgn++) {
+                const D3 P = sgn ? -V : V;
+                if (dot(cross(N, A), P) >= 0 && dot(cross(B, N), P) >= 0) {
+                    const double lp = lat_of(P);
+                    la0 = fmin(la0, lp);
+                    la1 = fmax(la1, lp);
+                }
+            }
+        }
+    }
+    full_lon = false;
+    double oa = lon_of(A), ob = lon_of(B);
+    if (fabs(a) > 89.999 || fabs(b) > 89.999 || la1 > 89.99 || la0 < -89.99) {
+        full_lon = true;
+        lo0 = -180;
+        lo1 = 180;
+        return;
+    }
+    if (oa > ob) {
+        double t = oa;
+        oa = ob;
+        ob = t;
+    }
+    if (ob - oa <= 180.0) {
+        lo0 = oa;
+        lo1 = ob;
+    } else {
+        lo0 = ob;
+        lo1 = oa + 360.0;
+    }
+}
+
+struct BuildView {
+    Geo g;
+    const D3* pv;
+    const int* pe;
+    int n;
+};
+
+// Level-0 pairs: one thread per edge, candidate cells from the edge's box.
+template <int PASS>
+__global__ void k_l0_pairs(BuildView v, int* cnt, const int* off, int* cursor, int* list)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= v.n) return;
+    const D3 A = v.pv[v.pe[2 * t]], B = v.pv[v.pe[2 * t + 1]];
+    if (A.x == B.x && A.y == B.y && A.z == B.z) return;
+    const int W = v.g.W, H = v.g.H;
+    double la0, la1, lo0, lo1;
+    bool full;
+    arc_box(A, B, la0, la1, lo0, lo1, full);
+    const double rmax = (2.0 * (0.5 * v.g.dlat0 + 0.5 * v.g.dlon0) * RAD) * (1.0 + 1e-6) + LOC_MARGIN;
+    const double rdeg = rmax / RAD + 1e-9;
+    la0 -= rdeg;
+    la1 += rdeg;
+    int iy0 = (int)floor((la0 + 90.0) / v.g.dlat0), iy1 = (int)floor((la1 + 90.0) / v.g.dlat0);
+    iy0 = max(iy0, 0);
+    iy1 = min(iy1, H - 1);
+    const double maxlat = fmax(fabs(la0), fabs(la1));
+    long long ix0, ix1;
+    if (full || maxlat >= 89.0) {
+        ix0 = 0;
+        ix1 = W - 1;
+    } else {
+        const double c = cos(maxlat * RAD);
+        const double wdeg = rdeg / c;
+        if (lo1 - lo0 + 2 * wdeg >= 360.0) {
+            ix0 = 0;
+            ix1 = W - 1;
+        } else {
+            ix0 = (long long)floor((lo0 - wdeg + 180.0) / v.g.dlon0);
+            ix1 = (long long)floor((lo1 + wdeg + 180.0) / v.g.dlon0);
+        }
+    }
+    for (int iy = iy0; iy <= iy1; iy++) {
+        for (long long xx = ix0; xx <= ix1; xx++) {
+            const int ix = (int)(((xx % W) + W) % W);
+            const NodeCap c = node_cap(v.g, 0, ix, iy);
+            if (!edge_hits_cap(A, B, c.R, c.r)) continue;
+            const int node = iy * W + ix;
+            if (PASS == 0) {
+                atomicAdd(&cnt[node], 1);
+            } else {
+                const int pos = off[node] + atomicAdd(&cursor[node], 1);
+                list[pos] = t;
+            }
+        }
+    }
+}
+
+// Children pairs: one thread per (refined parent, edge) pair.
+template <int PASS>
+__global__ void k_child_pairs(BuildView v, int lvl, int npairs, const int* pair_node, const int* plist,
+                              const int* child_base, const long long* pix, const long long* piy, int cstart,
+                              int* cnt, const int* off, int* cursor, int* list)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= npairs) return;
+    const int p = pair_node[k];
+    const int cb = child_base[p];
+    if (cb < 0) return;
+    const int e = plist[k];
+    const D3 A = v.pv[v.pe[2 * e]], B = v.pv[v.pe[2 * e + 1]];
+    for (int cy = 0; cy < FAN; cy++)
+        for (int cx = 0; cx < FAN; cx++) {
+            const NodeCap c = node_cap(v.g, lvl + 1, pix[p] * FAN + cx, piy[p] * FAN + cy);
+            if (!edge_hits_cap(A, B, c.R, c.r)) continue;
+            const int node = cb + cy * FAN + cx - cstart;
+            if (PASS == 0) {
+                atomicAdd(&cnt[node], 1);
+            } else {
+                const int pos = off[node] + atomicAdd(&cursor[node], 1);
+                list[pos] = e;
+            }
+        }
+}
+
+__global__ void k_fill_pair_node(const int* cnt, const int* off, int nn, int* pair_node)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nn) return;
+    for (int k = 0; k < cnt[p]; k++) pair_node[off[p] + k] = p;
+}
+
+__global__ void k_sort_lists(const int* cnt, const int* off, int nn, int* list)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nn) return;
+    int* L = list + off[p];
+    const int n = cnt[p];
+    for (int i = 1; i < n; i++) {
+        int x = L[i], j = i - 1;
+        while (j >= 0 && L[j] > x) {
+            L[j + 1] = L[j];
+            j--;
+        }
+        L[j + 1] = x;
+    }
+}
+
+__global__ void k_refine_flags(const int* cnt, int nn, int K, int* flag)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < nn) flag[p] = cnt[p] > K ? 1 : 0;
+}
+
+// child_base[p] = first child node (global index) or -1; child coordinates.
+__global__ void k_make_children(const int* flag, const int* foff, int nn, int cstart, const long long* pix,
+                                const long long* piy, int lvl0_W, int* child_base, long long* cix, long long* ciy)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nn) return;
+    if (!flag[p]) {
+        child_base[p] = -1;
+        return;
+    }
+    const int base = cstart + foff[p] * FAN * FAN;
+    child_base[p] = base;
+    const long long px = pix ? pix[p] : (p % lvl0_W), py = piy ? piy[p] : (p / lvl0_W);
+    for (int cy = 0; cy < FAN; cy++)
+        for (int cx = 0; cx < FAN; cx++) {
+            const int c = foff[p] * FAN * FAN + cy * FAN + cx;
+            cix[c] = px * FAN + cx;
+            ciy[c] = py * FAN + cy;
+        }
+}
+
+__global__ void k_l0_coords(int W, int nn, long long* ix, long long* iy)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nn) return;
+    ix[p] = p % W;
+    iy[p] = p / W;
+}
+
+// parity of edges (from up to two sorted lists, union) crossing arc P->Q
+__device__ int arc_parity_lists(const D3* pv, const int* pe, const double* P, const double* Q, const int* L1, int n1,
+                                const int* L2, int n2, int* bad)
+{
+    int par = 0, i = 0, j = 0;
+    while (i < n1 || j < n2) {
+        int e;
+        if (j >= n2 || (i < n1 && L1[i] < L2[j])) {
+            e = L1[i++];
+        } else if (i >= n1 || L2[j] < L1[i]) {
+            e = L2[j++];
+        } else {
+            e = L1[i];
+            i++;
+            j++;
+        }
+        const D3 a = pv[pe[2 * e]], b = pv[pe[2 * e + 1]];
+        const double A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z};
+        if (exact::same(A, B)) continue;
+        if (exact::same(A, P) || exact::same(B, P) || exact::same(A, Q) || exact::same(B, Q)) {
+            atomicAdd(bad, 1);
+            continue;
+        }
+        par ^= exact::crossing(P, Q, A, B) ? 1 : 0;
+    }
+    return par;
+}
+
+// Level-0 neighbour parities: vertical (i,j)->(i,j+1) for all, horizontal on row 0.
+__global__ void k_l0_neighbour_parity(BuildView v, const int* cnt, const int* off, const int* list, uint8_t* vpar,
+                                      uint8_t* hpar, int* bad)
+{
+    const int W = v.g.W, H = v.g.H;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nv = (long long)W * (H - 1);
+    if (t < nv) {
+        const int i = (int)(t % W), j = (int)(t / W);
+        const int p = j * W + i, q = (j + 1) * W + i;
+        uint8_t par = 0;
+        if (cnt[p] || cnt[q]) {
+            NodeCap a = node_cap(v.g, 0, i, j), b = node_cap(v.g, 0, i, j + 1);
+            nudge_center(v.g, 0, a, v.pv, v.pe, list + off[p], cnt[p]);
+            nudge_center(v.g, 0, b, v.pv, v.pe, list + off[q], cnt[q]);
+            par = (uint8_t)arc_parity_lists(v.pv, v.pe, a.R, b.R, list + off[p], cnt[p], list + off[q], cnt[q], bad);
+        }
+        vpar[t] = par;
+    } else if (t < nv + W - 1) {
+        const int i = (int)(t - nv);
+        const int p = i, q = i + 1;
+        uint8_t par = 0;
+        if (cnt[p] || cnt[q]) {
+            NodeCap a = node_cap(v.g, 0, i, 0), b = node_cap(v.g, 0, i + 1, 0);
+            nudge_center(v.g, 0, a, v.pv, v.pe, list + off[p], cnt[p]);
+            nudge_center(v.g, 0, b, v.pv, v.pe, list + off[q], cnt[q]);
+            par = (uint8_t)arc_parity_lists(v.pv, v.pe, a.R, b.R, list + off[p], cnt[p], list + off[q], cnt[q], bad);
+        }
+        hpar[i] = par;
+    }
+}
+
+// labels of level-0 centers: row 0 by prefix XOR of hpar, columns by vpar
+__global__ void k_l0_labels(int W, int H, const uint8_t* vpar, const uint8_t* hpar, const int* origin_label,
+                            uint8_t* label)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= W) return;
+    int l = *origin_label;  // 1 or 2
+    for (int k = 0; k < i; k++)
+        if (hpar[k]) l = 3 - l;
+    label[i] = (uint8_t)l;
+    for (int j = 1; j < H; j++) {
+        if (vpar[(long long)(j - 1) * W + i]) l = 3 - l;
+        label[(long long)j * W + i] = (uint8_t)l;
+    }
+}
+
+// child label = parent label XOR parity(arc parent center -> child center)
+__global__ void k_child_labels(BuildView v, int lvl, int nchild, const int* child_parent, const long long* cix,
+                               const long long* ciy, const int* ccnt, const int* coff, const int* clist,
+                               const long long* pix, const long long* piy, const int* pcnt, const int* poff,
+                               const int* plist, const uint8_t* plabel, uint8_t* clabel, int* bad)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nchild) return;
+    const int p = child_parent[c];
+    NodeCap pc = node_cap(v.g, lvl, pix[p], piy[p]);
+    nudge_center(v.g, lvl, pc, v.pv, v.pe, plist + poff[p], pcnt[p]);
+    NodeCap cc = node_cap(v.g, lvl + 1, cix[c], ciy[c]);
+    nudge_center(v.g, lvl + 1, cc, v.pv, v.pe, clist + coff[c], ccnt[c]);
+    // nesting of caps: the child's cap must lie inside the parent's
+    const double dx = pc.R[0] - cc.R[0], dy = pc.R[1] - cc.R[1], dz = pc.R[2] - cc.R[2];
+    const double dist = 2.0 * asin(fmin(1.0, 0.5 * sqrt(dx * dx + dy * dy + dz * dz)));
+    if (dist + cc.r > pc.r) atomicAdd(bad + 1, 1);
+    const int par = arc_parity_lists(v.pv, v.pe, pc.R, cc.R, plist + poff[p], pcnt[p], nullptr, 0, bad);
+    clabel[c] = (uint8_t)(par ? 3 - plabel[p] : plabel[p]);
+}
+
+__global__ void k_child_parent(const int* child_base, int np, int cstart, int* child_parent)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np || child_base[p] < 0) return;
+    const int b = child_base[p] - cstart;
+    for (int k = 0; k < FAN * FAN; k++) child_parent[b + k] = p;
+}
+
+// Arc parity against all edges (one arc), with vertex-coincidence flag.
+__global__ void k_arc_parity_all(const D3* pv, const int* pe, int n, const double* PQ, int* out)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const D3 a = pv[pe[2 * e]], b = pv[pe[2 * e + 1]];
+    const double A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z};
+    if (exact::same(A, B)) return;
+    const double* P = PQ;
+    const double* Q = PQ + 3;
+    if (exact::same(A, P) || exact::same(B, P) || exact::same(A, Q) || exact::same(B, Q)) {
+        atomicAdd(out + 1, 1);
+        return;
+    }
+    if (exact::crossing(P, Q, A, B)) {
+        atomicXor(out, 1);
+        atomicAdd(out + 2, 1);
+        atomicMax(out + 3, e);
+    }
+}
+
+// Final node words, leaf records.
+__global__ void k_encode(int nn, int gstart, const int* cnt, const int* child_base, const uint8_t* label,
+                         const int* leaf_off, uint32_t* nodes)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nn) return;
+    uint32_t w;
+    if (child_base && child_base[p] >= 0)
+        w = KIND_INNER | (uint32_t)child_base[p];
+    else if (cnt[p] == 0)
+        w = KIND_PURE | label[p];
+    else
+        w = KIND_LEAF | (uint32_t)leaf_off[p];
+    nodes[gstart + p] = w;
+}
+
+__global__ void k_leaf_flags(int nn, const int* cnt, const int* child_base, int* is_leaf, int* nrec)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nn) return;
+    const bool leaf = cnt[p] > 0 && !(child_base && child_base[p] >= 0);
+    is_leaf[p] = leaf ? 1 : 0;
+    nrec[p] = leaf ? cnt[p] : 0;
+}
+
+__global__ void k_leaf_records(BuildView v, int lvl, int nn, const int* is_leaf, const int* leaf_off,
+                               const int* rec_off, int leaf_base, long long rec_base, const long long* ix,
+                               const long long* iy, const int* cnt, const int* off, const int* list,
+                               const uint8_t* label, LeafRec* leaves, EdgeRec* recs, int* bad)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nn || !is_leaf[p]) return;
+    NodeCap c = node_cap(v.g, lvl, ix[p], iy[p]);
+    nudge_center(v.g, lvl, c, v.pv, v.pe, list + off[p], cnt[p]);
+    LeafRec L;
+    L.R[0] = c.R[0];
+    L.R[1] = c.R[1];
+    L.R[2] = c.R[2];
+    const long long ro = rec_base + rec_off[p];
+    L.off = (uint32_t)ro;
+    L.cnt = (uint16_t)min(cnt[p], 65535);
+    L.label = label[p];
+    L.pad = 0;
+    leaves[leaf_base + leaf_off[p]] = L;
+    if (cnt[p] > 65535) atomicAdd(bad + 2, 1);
+    const D3 R = d3(c.R[0], c.R[1], c.R[2]);
+    for (int k = 0; k < cnt[p]; k++) {
+        const int e = list[off[p] + k];
+        const D3 a = v.pv[v.pe[2 * e]], b = v.pv[v.pe[2 * e + 1]];
+        const D3 n1 = cross(a, b), n2 = cross(a, R), n3 = cross(b, R);
+        EdgeRec r;
+        r.n1[0] = (float)n1.x;
+        r.n1[1] = (float)n1.y;
+        r.n1[2] = (float)n1.z;
+        r.n2[0] = (float)n2.x;
+        r.n2[1] = (float)n2.y;
+        r.n2[2] = (float)n2.z;
+        r.n3[0] = (float)n3.x;
+        r.n3[1] = (float)n3.y;
+        r.n3[2] = (float)n3.z;
+        const double A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z};
+        const int s1 = exact::orient(A, B, c.R);
+        if (s1 == 0) atomicAdd(bad, 1);
+        r.es = (uint32_t)e | (s1 > 0 ? 0x80000000u : 0u);
+        recs[ro + k] = r;
+    }
+}
+
+__global__ void k_shift_leaf_words(uint32_t* nodes, int start, int nn, int add)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nn) return;
+    const uint32_t w = nodes[start + p];
+    if ((w & KIND_MASK) == KIND_LEAF) nodes[start + p] = w + (uint32_t)add;
+}
+
+// ------------------------------------------------------------- query ----
+
+struct QueryView {
+    int W, H;
+    double su;  // W / 360 (= H / 180)
+    const uint32_t* nodes;
+    const LeafRec* leaves;
+    const EdgeRec* recs;
+    const D3* pv;
+    const int* pe;
+};
+
+__device__ __forceinline__ int sign32(const float* n, float qx, float qy, float qz)
+{
+    const float d = fmaf(qz, n[2], fmaf(qy, n[1], qx * n[0]));
+    const float b = (fabsf(n[0]) + fabsf(n[1]) + fabsf(n[2])) * C32 + 4e-15f;
+    return d > b ? 1 : (d < -b ? -1 : 0);
+}
+
+struct PointCtx {
+    double lon, lat;      // input longitude and FakeLL latitude (canonical XYZ)
+    double lon_r, lat_r;  // the same point with lon in [-180, 180], lat in [-90, 90]
+    bool have64;
+    double q[3];
+    __device__ void need64()
+    {
+        if (!have64) {
+            gahhg_canon_vertex_xyz(lon, lat, q);
+            have64 = true;
+        }
+    }
+};
+
+// exact sign of orient(x, y, z) given a failed FP32 stage; `code` reports a
+// decided label (vertex rule / coincident center) through *early.
+__device__ __forceinline__ int sign_escalate(const double* x, const double* y, const double* z,
+                                             unsigned long long* cnt64, unsigned long long* cntx)
+{
+    int s = exact::orient_fp64(x, y, z);
+    if (cnt64) atomicAdd(cnt64, 1ull);
+    if (s != 0) return s;
+    if (cntx) atomicAdd(cntx, 1ull);
+    return exact::orient_exact(x, y, z);
+}
+
+__device__ uint8_t leaf_label(const QueryView& Q, uint32_t leaf, PointCtx& P, bool fp32, unsigned long long* ctr)
+{
+    const LeafRec L = Q.leaves[leaf];
+    float qx = 0.f, qy = 0.f, qz = 0.f;
+    if (fp32) {
+        float sa, ca, so, co;
+        // arguments stay inside [-pi, pi], where __sincosf's error bound is documented
+        __sincosf((float)gahhg_canon_rad(P.lat_r), &sa, &ca);
+        __sincosf((float)gahhg_canon_rad(P.lon_r), &so, &co);
+        qx = ca * so;
+        qy = sa;
+        qz = ca * co;
+    } else {
+        P.need64();
+    }
+    unsigned long long* c64 = ctr ? ctr + 0 : nullptr;
+    unsigned long long* cx = ctr ? ctr + 1 : nullptr;
+    int par = 0;
+    for (int k = 0; k < L.cnt; k++) {
+        const EdgeRec r = Q.recs[L.off + k];
+        const int e = (int)(r.es & 0x7fffffffu);
+        const int s1 = (r.es >> 31) ? 1 : -1;
+        int s2 = fp32 ? sign32(r.n1, qx, qy, qz) : 0;
+        double A[3], B[3];
+        bool haveAB = false;
+        auto needAB = [&]() {
+            if (!haveAB) {
+                const D3 a = Q.pv[Q.pe[2 * e]], b = Q.pv[Q.pe[2 * e + 1]];
+                A[0] = a.x;
+                A[1] = a.y;
+                A[2] = a.z;
+                B[0] = b.x;
+                B[1] = b.y;
+                B[2] = b.z;
+                haveAB = true;
+            }
+        };
+        if (s2 == 0) {
+            P.need64();
+            needAB();
+            if (exact::same(P.q, A) || exact::same(P.q, B)) return CELL_IN;  // vertex rule
+            if (exact::same(P.q, L.R)) return L.label;                       // q is the center
+            s2 = sign_escalate(A, B, P.q, c64, cx);
+        }
+        if (s2 == s1) continue;
+        // s3 = orient(R, q, A) = q . (A x R); crossing needs s3 == s2
+        int s3 = fp32 ? sign32(r.n2, qx, qy, qz) : 0;
+        if (s3 == 0) {
+            P.need64();
+            needAB();
+            if (exact::same(P.q, A) || exact::same(P.q, B)) return CELL_IN;
+            if (exact::same(P.q, L.R)) return L.label;
+            s3 = sign_escalate(L.R, P.q, A, c64, cx);
+        }
+        if (s3 != s2) continue;
+        int s4 = fp32 ? sign32(r.n3, qx, qy, qz) : 0;
+        if (s4 == 0) {
+            P.need64();
+            needAB();
+            if (exact::same(P.q, A) || exact::same(P.q, B)) return CELL_IN;
+            if (exact::same(P.q, L.R)) return L.label;
+            s4 = sign_escalate(L.R, P.q, B, c64, cx);
+        }
+        if (s4 == -s2) par ^= 1;
+    }
+    return (uint8_t)(par ? 3 - L.label : L.label);
+}
+
+__device__ __forceinline__ uint8_t lattice_point(const QueryView& Q, double lon, double lat, bool fp32,
+                                                 unsigned long long* ctr)
+{
+    PointCtx P;
+    P.lat = gahhg_canon_query_lat(lat);
+    P.lon = lon;
+    P.have64 = false;
+    double lo = lon, la = P.lat;
+    if (!(fabs(lo) <= 540.0 && fabs(la) <= 90.0)) {
+        if (!(isfinite(lo) && isfinite(la))) return CELL_UNDEFINED;
+        // unusual input: locate from the canonical XYZ itself
+        P.need64();
+        la = asin(fmin(1.0, fmax(-1.0, P.q[1]))) / RAD;
+        lo = atan2(P.q[0], P.q[2]) / RAD;
+    }
+    double u = (lo + 180.0) * Q.su;
+    if (u >= Q.W) u -= Q.W;
+    if (u < 0) u += Q.W;
+    const double v = (la + 90.0) * Q.su;
+    P.lon_r = fmin(180.0, fmax(-180.0, u / Q.su - 180.0));
+    P.lat_r = la;
+    int ix = (int)u, iy = (int)v;
+    ix = min(max(ix, 0), Q.W - 1);
+    iy = min(max(iy, 0), Q.H - 1);
+    double fu = u - ix, fv = v - iy;
+    uint32_t w = __ldg(Q.nodes + (size_t)iy * Q.W + ix);
+    while ((w & KIND_MASK) == KIND_INNER) {
+        fu *= FAN;
+        fv *= FAN;
+        int cx = min(max((int)fu, 0), FAN - 1), cy = min(max((int)fv, 0), FAN - 1);
+        fu -= cx;
+        fv -= cy;
+        w = __ldg(Q.nodes + (w & INDEX_MASK) + cy * FAN + cx);
+    }
+    if ((w & KIND_MASK) == KIND_PURE) return (uint8_t)(w & 3u);
+    if (ctr) atomicAdd(ctr + 2, 1ull);
+    return leaf_label(Q, w & INDEX_MASK, P, fp32, ctr);
+}
+
+template <bool FP32>
+__global__ void __launch_bounds__(TPB) k_lattice_query(const double2* __restrict__ ll, long long n,
+                                                       uint8_t* __restrict__ out, QueryView Q,
+                                                       unsigned long long* ctr)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const double2 p = ll[i];
+        out[i] = lattice_point(Q, p.x, p.y, FP32, ctr);
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host --
+
+struct Lattice {
+    Geo geo{};
+    int K = 8, maxlev = 10, nlev = 0;
+    DevArray<uint32_t> nodes;
+    DevArray<LeafRec> leaves;
+    DevArray<EdgeRec> recs;
+    long long nnodes = 0, nleaves = 0, nrecs = 0;
+    int origin_label = 0;
+    double x_in[3]{};
+};
+
+void lattice_free(Lattice* L)
+{
+    if (!L) return;
+    L->nodes.release();
+    L->leaves.release();
+    L->recs.release();
+    delete L;
+}
+
+size_t lattice_bytes(const Lattice* L)
+{
+    if (!L) return 0;
+    return L->nnodes * sizeof(uint32_t) + L->nleaves * sizeof(LeafRec) + L->nrecs * sizeof(EdgeRec);
+}
+
+namespace {
+
+struct LevelBuf {
+    int nn = 0;     // nodes at this level
+    int gstart = 0; // global index of the first node
+    DevArray<int> cnt, off, cursor, list, pair_node, child_base, flag, foff;
+    DevArray<long long> ix, iy;
+    DevArray<uint8_t> label;
+    int npairs = 0;
+    void release()
+    {
+        cnt.release();
+        off.release();
+        cursor.release();
+        list.release();
+        pair_node.release();
+        child_base.release();
+        flag.release();
+        foff.release();
+        ix.release();
+        iy.release();
+        label.release();
+    }
+};
+
+const double HUBS[6][3] = {
+    {1.0, 0.000731, 0.000419},  {-1.0, 0.000627, -0.000883}, {0.000577, 1.0, 0.000941},
+    {-0.000351, -1.0, 0.000713}, {0.000809, -0.000467, 1.0}, {-0.000689, 0.000523, -1.0},
+};
+
+// parity of all edges crossing arc P->Q (device), -1 on vertex coincidence
+gahhg_status arc_parity_all(Grid* g, const double* P, const double* Q, int* parity, int* ncross, int* last_edge)
+{
+    cudaStream_t s = g->stream;
+    double* d_pq = reinterpret_cast<double*>(g->d_counts + 40);  // 6 doubles in the counts scratch (8-aligned)
+    double pq[6] = {P[0], P[1], P[2], Q[0], Q[1], Q[2]};
+    int* d_out = g->d_counts + 56;
+    GAHHG_CUDA_TRY(cudaMemcpyAsync(d_pq, pq, sizeof(pq), cudaMemcpyHostToDevice, s));
+    int init[4] = {0, 0, 0, -1};
+    GAHHG_CUDA_TRY(cudaMemcpyAsync(d_out, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    const int n = g->poly->pv_num;
+    k_arc_parity_all<<<blocks_for(n), TPB, 0, s>>>(g->poly->d_pv, g->poly->d_pe, n, d_pq, d_out);
+    int out[4];
+    GAHHG_CUDA_TRY(cudaMemcpyAsync(out, d_out, sizeof(out), cudaMemcpyDeviceToHost, s));
+    GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+    *parity = out[1] ? -1 : out[0];
+    if (ncross) *ncross = out[2];
+    if (last_edge) *last_edge = out[3];
     return GAHHG_OK;
 }
-gahhg_status lattice_query(Grid*, const double*, size_t, uint8_t*, int, cudaStream_t, uint64_t*)
+
+// A point just left of an outer-ring edge (the exact oracle takes the same
+// steps: first usable edge, offset 1e-3 * chord along the edge normal, the
+// tiny arc from its mirror image crossing exactly this one edge).
+gahhg_status reference_point(Grid* g, double* x_in)
 {
-    set_error("exact engine not available");
+    const Polygon* P = g->poly;
+    const int n_outer = P->ring_start[1];
+    for (int e = 0; e < n_outer; e++) {
+        const D3 a = P->pv[P->pe[2 * e]], b = P->pv[P->pe[2 * e + 1]];
+        const double A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z};
+        if (exact::same(A, B)) continue;
+        double m[3] = {A[0] + B[0], A[1] + B[1], A[2] + B[2]};
+        double nm = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+        if (!(nm > 1e-3)) continue;
+        double N[3] = {A[1] * B[2] - A[2] * B[1], A[2] * B[0] - A[0] * B[2], A[0] * B[1] - A[1] * B[0]};
+        double nn = sqrt(N[0] * N[0] + N[1] * N[1] + N[2] * N[2]);
+        if (!(nn > 0)) continue;
+        double d[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
+        double t = 1e-3 * sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        double xi[3], xo[3];
+        for (int k = 0; k < 3; k++) {
+            xi[k] = m[k] / nm + t * (N[k] / nn);
+            xo[k] = m[k] / nm - t * (N[k] / nn);
+        }
+        if (exact::orient(A, B, xi) <= 0 || exact::orient(A, B, xo) >= 0) continue;
+        int par, nc, le;
+        GAHHG_TRY(arc_parity_all(g, xo, xi, &par, &nc, &le));
+        if (par != 1 || nc != 1 || le != e) continue;
+        memcpy(x_in, xi, sizeof(xi));
+        return GAHHG_OK;
+    }
+    set_error("exact index: no outer-ring edge gives a reference point");
     return GAHHG_ERR_STATE;
 }
-void lattice_free(Lattice* L) { delete L; }
-size_t lattice_bytes(const Lattice*) { return 0; }
+
+int nearest_hub(const double* q)
+{
+    int best = 0;
+    double bd = -1e300;
+    for (int k = 0; k < 6; k++) {
+        double d = HUBS[k][0] * q[0] + HUBS[k][1] * q[1] + HUBS[k][2] * q[2];
+        if (d > bd) {
+            bd = d;
+            best = k;
+        }
+    }
+    return best;
+}
+
+}  // namespace
+
+gahhg_status lattice_build(Grid* g)
+{
+    cudaStream_t s = g->stream;
+    const Polygon* P = g->poly;
+    const int n = P->pv_num;
+    Lattice* L = new Lattice();
+    g->lattice = L;
+
+    int W = 64;
+    if (g->opts.lattice_top > 0) {
+        W = g->opts.lattice_top;
+    } else {
+        while (W < 4096 && (long long)W * W / 2 < 8LL * n) W *= 2;
+    }
+    if (W < 8 || W > 16384 || (W & (W - 1))) {
+        set_error("lattice_top must be a power of two in [8, 16384]");
+        return GAHHG_ERR_ARG;
+    }
+    L->K = g->opts.lattice_leaf > 0 ? g->opts.lattice_leaf : 8;
+    L->maxlev = 9;
+    L->geo.W = W;
+    L->geo.H = W / 2;
+    L->geo.dlon0 = 360.0 / W;
+    L->geo.dlat0 = 180.0 / (W / 2);
+    BuildView bv{L->geo, P->d_pv, P->d_pe, n};
+
+    // exact label of the first level-0 center, through the hubs
+    GAHHG_TRY(reference_point(g, L->x_in));
+    int label = CELL_IN;
+    {
+        const int h0 = nearest_hub(L->x_in);
+        const int south = 3;  // hub near -y
+        std::vector<const double*> path;
+        path.push_back(L->x_in);
+        path.push_back(HUBS[h0]);
+        if (h0 == 2) path.push_back(HUBS[0]);  // +y -> +x -> -y
+        if (h0 != south) path.push_back(HUBS[south]);
+        NodeCap c00 = node_cap(L->geo, 0, 0, 0);
+        // the origin center gets nudged like every other center (its list is
+        // not known yet; a vertex exactly at the center is rejected below)
+        path.push_back(c00.R);
+        for (size_t k = 0; k + 1 < path.size(); k++) {
+            int par;
+            GAHHG_TRY(arc_parity_all(g, path[k], path[k + 1], &par, nullptr, nullptr));
+            if (par < 0) {
+                set_error("exact index: a hub or the origin center coincides with a polygon vertex");
+                return GAHHG_ERR_STATE;
+            }
+            if (par) label = 3 - label;
+        }
+    }
+    L->origin_label = label;
+
+    std::vector<LevelBuf> lv(1);
+    // ---------------- level 0 ----------------
+    LevelBuf& l0 = lv[0];
+    l0.nn = W * (W / 2);
+    l0.gstart = 0;
+    GAHHG_TRY(l0.cnt.reserve(l0.nn, s, false));
+    GAHHG_TRY(l0.off.reserve(l0.nn, s, false));
+    GAHHG_TRY(l0.cursor.reserve(l0.nn, s, false));
+    GAHHG_CUDA_TRY(cudaMemsetAsync(l0.cnt.ptr, 0, sizeof(int) * l0.nn, s));
+    GAHHG_CUDA_TRY(cudaMemsetAsync(l0.cursor.ptr, 0, sizeof(int) * l0.nn, s));
+    k_l0_pairs<0><<<blocks_for(n), TPB, 0, s>>>(bv, l0.cnt.ptr, nullptr, nullptr, nullptr);
+    GAHHG_TRY(scan_state_reserve(&g->scan_state, l0.nn));
+    GAHHG_TRY(scan_exclusive(l0.cnt.ptr, l0.off.ptr, l0.nn, g->d_counts + 8, g->scan_state, g->d_err, s));
+    int total = 0;
+    GAHHG_CUDA_TRY(cudaMemcpyAsync(&total, g->d_counts + 8, sizeof(int), cudaMemcpyDeviceToHost, s));
+    GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+    l0.npairs = total;
+    GAHHG_TRY(l0.list.reserve(std::max(total, 1), s, false));
+    k_l0_pairs<1><<<blocks_for(n), TPB, 0, s>>>(bv, l0.cnt.ptr, l0.off.ptr, l0.cursor.ptr, l0.list.ptr);
+    k_sort_lists<<<blocks_for(l0.nn), TPB, 0, s>>>(l0.cnt.ptr, l0.off.ptr, l0.nn, l0.list.ptr);
+    GAHHG_TRY(l0.ix.reserve(l0.nn, s, false));
+    GAHHG_TRY(l0.iy.reserve(l0.nn, s, false));
+    k_l0_coords<<<blocks_for(l0.nn), TPB, 0, s>>>(W, l0.nn, l0.ix.ptr, l0.iy.ptr);
+
+    // level-0 labels
+    int* d_bad = g->d_counts + 48;  // [0] coincidences, [1] nesting, [2] long lists
+    GAHHG_CUDA_TRY(cudaMemsetAsync(d_bad, 0, 4 * sizeof(int), s));
+    {
+        DevArray<uint8_t> vpar, hpar;
+        GAHHG_TRY(vpar.reserve((size_t)W * (W / 2 - 1) + 1, s, false));
+        GAHHG_TRY(hpar.reserve(W, s, false));
+        GAHHG_TRY(l0.label.reserve(l0.nn, s, false));
+        const long long nthreads = (long long)W * (W / 2 - 1) + W - 1;
+        k_l0_neighbour_parity<<<blocks_for(nthreads), TPB, 0, s>>>(bv, l0.cnt.ptr, l0.off.ptr, l0.list.ptr, vpar.ptr,
+                                                                   hpar.ptr, d_bad);
+        int* d_origin = g->d_counts + 12;
+        GAHHG_CUDA_TRY(cudaMemcpyAsync(d_origin, &L->origin_label, sizeof(int), cudaMemcpyHostToDevice, s));
+        k_l0_labels<<<blocks_for(W), TPB, 0, s>>>(W, W / 2, vpar.ptr, hpar.ptr, d_origin, l0.label.ptr);
+        GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+        vpar.release();
+        hpar.release();
+    }
+
+    // ---------------- refinement ----------------
+    int gnext = l0.nn;
+    for (int lvl = 0; lvl < L->maxlev; lvl++) {
+        LevelBuf& pl = lv[lvl];
+        GAHHG_TRY(pl.flag.reserve(pl.nn, s, false));
+        GAHHG_TRY(pl.foff.reserve(pl.nn, s, false));
+        k_refine_flags<<<blocks_for(pl.nn), TPB, 0, s>>>(pl.cnt.ptr, pl.nn, L->K, pl.flag.ptr);
+        GAHHG_TRY(scan_state_reserve(&g->scan_state, pl.nn));
+        GAHHG_TRY(scan_exclusive(pl.flag.ptr, pl.foff.ptr, pl.nn, g->d_counts + 9, g->scan_state, g->d_err, s));
+        int nref = 0;
+        GAHHG_CUDA_TRY(cudaMemcpyAsync(&nref, g->d_counts + 9, sizeof(int), cudaMemcpyDeviceToHost, s));
+        GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+        if (nref == 0) break;
+        if ((long long)gnext + (long long)nref * FAN * FAN >= (long long)INDEX_MASK) {
+            set_error("exact index: node count exceeds 2^30");
+            return GAHHG_ERR_CAPACITY;
+        }
+        lv.emplace_back();
+        LevelBuf& cl = lv.back();
+        LevelBuf& pp = lv[lvl];  // re-fetch after emplace_back
+        cl.nn = nref * FAN * FAN;
+        cl.gstart = gnext;
+        GAHHG_TRY(pp.child_base.reserve(pp.nn, s, false));
+        GAHHG_TRY(cl.ix.reserve(cl.nn, s, false));
+        GAHHG_TRY(cl.iy.reserve(cl.nn, s, false));
+        k_make_children<<<blocks_for(pp.nn), TPB, 0, s>>>(pp.flag.ptr, pp.foff.ptr, pp.nn, cl.gstart, pp.ix.ptr,
+                                                          pp.iy.ptr, W, pp.child_base.ptr, cl.ix.ptr, cl.iy.ptr);
+        GAHHG_TRY(pp.pair_node.reserve(std::max(pp.npairs, 1), s, false));
+        k_fill_pair_node<<<blocks_for(pp.nn), TPB, 0, s>>>(pp.cnt.ptr, pp.off.ptr, pp.nn, pp.pair_node.ptr);
+        GAHHG_TRY(cl.cnt.reserve(cl.nn, s, false));
+        GAHHG_TRY(cl.off.reserve(cl.nn, s, false));
+        GAHHG_TRY(cl.cursor.reserve(cl.nn, s, false));
+        GAHHG_CUDA_TRY(cudaMemsetAsync(cl.cnt.ptr, 0, sizeof(int) * cl.nn, s));
+        GAHHG_CUDA_TRY(cudaMemsetAsync(cl.cursor.ptr, 0, sizeof(int) * cl.nn, s));
+        k_child_pairs<0><<<blocks_for(pp.npairs), TPB, 0, s>>>(bv, lvl, pp.npairs, pp.pair_node.ptr, pp.list.ptr,
+                                                               pp.child_base.ptr, pp.ix.ptr, pp.iy.ptr, cl.gstart,
+                                                               cl.cnt.ptr, nullptr, nullptr, nullptr);
+        GAHHG_TRY(scan_state_reserve(&g->scan_state, cl.nn));
+        GAHHG_TRY(scan_exclusive(cl.cnt.ptr, cl.off.ptr, cl.nn, g->d_counts + 10, g->scan_state, g->d_err, s));
+        int ctotal = 0;
+        GAHHG_CUDA_TRY(cudaMemcpyAsync(&ctotal, g->d_counts + 10, sizeof(int), cudaMemcpyDeviceToHost, s));
+        GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+        cl.npairs = ctotal;
+        GAHHG_TRY(cl.list.reserve(std::max(ctotal, 1), s, false));
+        k_child_pairs<1><<<blocks_for(pp.npairs), TPB, 0, s>>>(bv, lvl, pp.npairs, pp.pair_node.ptr, pp.list.ptr,
+                                                               pp.child_base.ptr, pp.ix.ptr, pp.iy.ptr, cl.gstart,
+                                                               cl.cnt.ptr, cl.off.ptr, cl.cursor.ptr, cl.list.ptr);
+        k_sort_lists<<<blocks_for(cl.nn), TPB, 0, s>>>(cl.cnt.ptr, cl.off.ptr, cl.nn, cl.list.ptr);
+        // child labels
+        DevArray<int> child_parent;
+        GAHHG_TRY(child_parent.reserve(cl.nn, s, false));
+        k_child_parent<<<blocks_for(pp.nn), TPB, 0, s>>>(pp.child_base.ptr, pp.nn, cl.gstart, child_parent.ptr);
+        GAHHG_TRY(cl.label.reserve(cl.nn, s, false));
+        k_child_labels<<<blocks_for(cl.nn), TPB, 0, s>>>(bv, lvl, cl.nn, child_parent.ptr, cl.ix.ptr, cl.iy.ptr,
+                                                         cl.cnt.ptr, cl.off.ptr, cl.list.ptr, pp.ix.ptr, pp.iy.ptr,
+                                                         pp.cnt.ptr, pp.off.ptr, pp.list.ptr, pp.label.ptr,
+                                                         cl.label.ptr, d_bad);
+        GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+        child_parent.release();
+        gnext += cl.nn;
+    }
+    L->nlev = (int)lv.size();
+    L->nnodes = gnext;
+
+    // ---------------- encode ----------------
+    GAHHG_TRY(L->nodes.reserve(L->nnodes, s, false));
+    std::vector<int> leaf_base(L->nlev), nleaf(L->nlev);
+    std::vector<long long> rec_base(L->nlev);
+    long long leaf_total = 0, rec_total = 0;
+    std::vector<DevArray<int>> is_leaf(L->nlev), leaf_off(L->nlev), nrec(L->nlev), rec_off(L->nlev);
+    for (int lvl = 0; lvl < L->nlev; lvl++) {
+        LevelBuf& b = lv[lvl];
+        const int* cb = (lvl + 1 < L->nlev) ? b.child_base.ptr : nullptr;
+        GAHHG_TRY(is_leaf[lvl].reserve(b.nn, s, false));
+        GAHHG_TRY(leaf_off[lvl].reserve(b.nn, s, false));
+        GAHHG_TRY(nrec[lvl].reserve(b.nn, s, false));
+        GAHHG_TRY(rec_off[lvl].reserve(b.nn, s, false));
+        k_leaf_flags<<<blocks_for(b.nn), TPB, 0, s>>>(b.nn, b.cnt.ptr, cb, is_leaf[lvl].ptr, nrec[lvl].ptr);
+        GAHHG_TRY(scan_state_reserve(&g->scan_state, b.nn));
+        GAHHG_TRY(scan_exclusive(is_leaf[lvl].ptr, leaf_off[lvl].ptr, b.nn, g->d_counts + 14, g->scan_state, g->d_err, s));
+        GAHHG_TRY(scan_exclusive(nrec[lvl].ptr, rec_off[lvl].ptr, b.nn, g->d_counts + 15, g->scan_state, g->d_err, s));
+        int tot[2];
+        GAHHG_CUDA_TRY(cudaMemcpyAsync(tot, g->d_counts + 14, sizeof(tot), cudaMemcpyDeviceToHost, s));
+        GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+        leaf_base[lvl] = (int)leaf_total;
+        nleaf[lvl] = tot[0];
+        rec_base[lvl] = rec_total;
+        leaf_total += tot[0];
+        rec_total += tot[1];
+        // leaf indices are global: shift by leaf_base when encoding
+        k_encode<<<blocks_for(b.nn), TPB, 0, s>>>(b.nn, b.gstart, b.cnt.ptr, cb, b.label.ptr, leaf_off[lvl].ptr,
+                                                  L->nodes.ptr);
+    }
+    if (rec_total >= 0xFFFFFFFFll) {
+        set_error("exact index: too many edge records");
+        return GAHHG_ERR_CAPACITY;
+    }
+    GAHHG_TRY(L->leaves.reserve(std::max(leaf_total, 1LL), s, false));
+    GAHHG_TRY(L->recs.reserve(std::max(rec_total, 1LL), s, false));
+    L->nleaves = leaf_total;
+    L->nrecs = rec_total;
+    for (int lvl = 0; lvl < L->nlev; lvl++) {
+        LevelBuf& b = lv[lvl];
+        k_leaf_records<<<blocks_for(b.nn), TPB, 0, s>>>(bv, lvl, b.nn, is_leaf[lvl].ptr, leaf_off[lvl].ptr,
+                                                        rec_off[lvl].ptr, leaf_base[lvl], rec_base[lvl], b.ix.ptr,
+                                                        b.iy.ptr, b.cnt.ptr, b.off.ptr, b.list.ptr, b.label.ptr,
+                                                        L->leaves.ptr, L->recs.ptr, d_bad);
+    }
+    GAHHG_CUDA_TRY(cudaGetLastError());
+    GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+    // leaf words were encoded with per-level leaf offsets; make them global
+    for (int lvl = 1; lvl < L->nlev; lvl++) {
+        if (leaf_base[lvl] == 0) continue;
+        k_shift_leaf_words<<<blocks_for(lv[lvl].nn), TPB, 0, s>>>(L->nodes.ptr, lv[lvl].gstart, lv[lvl].nn, leaf_base[lvl]);
+    }
+    int bad[4];
+    GAHHG_CUDA_TRY(cudaMemcpyAsync(bad, d_bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
+    GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+    for (auto& b : lv) b.release();
+    for (int lvl = 0; lvl < L->nlev; lvl++) {
+        is_leaf[lvl].release();
+        leaf_off[lvl].release();
+        nrec[lvl].release();
+        rec_off[lvl].release();
+    }
+    if (bad[0] || bad[1] || bad[2]) {
+        set_error("exact index: %d center/vertex coincidences, %d cap nesting violations, %d oversize leaves",
+                  bad[0], bad[1], bad[2]);
+        return GAHHG_ERR_DEVICE;
+    }
+    GAHHG_TRY(check_device_errors(g, "exact index build"));
+    return GAHHG_OK;
+}
+
+gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels, int precision,
+                           cudaStream_t s, uint64_t* d_counters)
+{
+    Lattice* L = g->lattice;
+    if (n == 0) return GAHHG_OK;
+    QueryView Q;
+    Q.W = L->geo.W;
+    Q.H = L->geo.H;
+    Q.su = (double)L->geo.W / 360.0;
+    Q.nodes = L->nodes.ptr;
+    Q.leaves = L->leaves.ptr;
+    Q.recs = L->recs.ptr;
+    Q.pv = g->poly->d_pv;
+    Q.pe = g->poly->d_pe;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
+    long long want = ((long long)n + TPB - 1) / TPB;
+    int grid = (int)std::min<long long>(want, (long long)sms * 16);
+    unsigned long long* ctr = (unsigned long long*)d_counters;
+    if (precision == GAHHG_QUERY_FP64_FILTER)
+        k_lattice_query<false><<<grid, TPB, 0, s>>>((const double2*)d_lonlat, (long long)n, d_labels, Q, ctr);
+    else
+        k_lattice_query<true><<<grid, TPB, 0, s>>>((const double2*)d_lonlat, (long long)n, d_labels, Q, ctr);
+    GAHHG_CUDA_TRY(cudaGetLastError());
+    return GAHHG_OK;
+}
+
 }  // namespace gahhg
