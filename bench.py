@@ -1,0 +1,370 @@
+"""Benchmark: exact-label point-in-spherical-polygon queries on one B200.
+
+Workload (C1): one polygon with a 1,000,000-vertex outer ring (midpoint
+displacement of a 64-gon of radius 60 deg around 170E 70N, crossing the
+antimeridian and containing the north pole) and ten 10,000-vertex holes;
+1e8 FP64 lon/lat query points uniform by area, generated on the device
+(seeded).  A step = one query pass over all points.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is the FP32-filtered exact query rate with inputs resident in HBM
+(1.6 GB, larger than L2), timed with CUDA events on the launching stream;
+`e2e` is the same metric through the public C ABI (gahhg_query) with pinned
+host buffers, host->device and device->host copies inside the timed region.
+With N > 1 (torchrun) each rank queries its own replica (the path shards by
+points, with no exchange); the slowest rank's time is used.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "query Mpts/s (FP32-filter vs FP64, exact labels), grid build ms, serve p99"
+BYTES_PER_POINT = 17  # 16 B lon/lat in + 1 B label out
+REF_DEPTH_C1 = 11     # deepest level at which the reference's edge walks terminate on C1
+
+
+def _peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def c1_polygon_cached():
+    from gahhg_b200 import synth
+    path = os.path.join(REPO, "_work", "bench_c1_rings.npz") if os.path.isdir(os.path.join(REPO, "_work")) else None
+    if path and os.path.exists(path):
+        z = np.load(path)
+        return [z["r%d" % i] for i in range(len(z.files))]
+    rings = synth.c1_polygon()
+    if path:
+        np.savez(path, **{"r%d" % i: r for i, r in enumerate(rings)})
+    return rings
+
+
+def device_points(n, seed, device):
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    u = torch.rand((n, 2), generator=g, device=device, dtype=torch.float64)
+    pts = torch.empty((n, 2), device=device, dtype=torch.float64)
+    pts[:, 0] = u[:, 0] * 360.0 - 180.0
+    pts[:, 1] = torch.rad2deg(torch.asin(u[:, 1] * 2.0 - 1.0))
+    return pts
+
+
+def timed_loop(fn, steps, stream):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) * 1e-3
+
+
+def cpu_reference_rate(rings, sample_points, threads, budget_s=12.0):
+    """The reference's own GAHHG code built for the CPU (oracle/_ref), all host
+    threads, on a bounded sample of the workload; returns (Mpts/s, info)."""
+    from oracle import ref
+    from gahhg_b200 import synth
+    if not ref.available():
+        return None, "oracle/_ref not built"
+    tmp = os.path.join("/tmp", "gahhg_bench_c1_%d.txt" % os.getpid())
+    synth.write_polygon(tmp, rings)
+    t0 = time.time()
+    r = ref.RefGPISP(tmp, maxdepth=REF_DEPTH_C1, threads=threads)
+    build_s = time.time() - t0
+    done, t1 = 0, time.time()
+    while time.time() - t1 < budget_s:
+        r.query(sample_points)
+        done += len(sample_points)
+    dt = time.time() - t1
+    r.close()
+    os.unlink(tmp)
+    return done / dt / 1e6, {"build_s": round(build_s, 3), "points": done, "seconds": round(dt, 3)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from gahhg_b200 import synth
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference built for the CPU) missing"}))
+        return 0
+    threads = os.cpu_count()
+    rings = c1_polygon_cached()
+    tmp = os.path.join("/tmp", "gahhg_bench_ref_%d.txt" % os.getpid())
+    synth.write_polygon(tmp, rings)
+    t0 = time.time()
+    r = ref.RefGPISP(tmp, maxdepth=REF_DEPTH_C1, threads=threads)
+    build_s = time.time() - t0
+    sample = synth.uniform_points(args.ref_sample, np.random.default_rng(0))
+    for _ in range(args.warmup):
+        r.query(sample)
+    t1 = time.time()
+    for _ in range(args.steps):
+        r.query(sample)
+    dt = time.time() - t1
+    r.close()
+    os.unlink(tmp)
+    rate = args.steps * len(sample) / dt / 1e6
+    desc = ("reference GAHHG kernels built for the CPU (oracle/_ref), OpenMP over %d threads, maxDepth %d; "
+            "each step queries %d of the 1e8 C1 points" % (threads, REF_DEPTH_C1, len(sample)))
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(rate, 3), "unit": "Mpts/s", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "C1: 1.1M-edge polygon, uniform FP64 lon/lat points (sampled)",
+                   "points_per_step": len(sample), "max_depth": REF_DEPTH_C1},
+        "cpu_baseline": {"value": round(rate, 3), "unit": "Mpts/s", "cores": threads, "kind": "reference",
+                         "sample": desc},
+        "build_ms": round(build_s * 1e3, 1),
+        "e2e": {"value": round(rate, 3), "unit": "Mpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--points", type=int, default=100_000_000)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--ref-sample", type=int, default=2_000_000)
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="DRAM bytes per launch of the query kernel from an ncu capture (profiles/)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    import gahhg_b200 as G
+
+    rings = c1_polygon_cached()
+    P = G.Polygon.from_rings(rings)
+    t0 = time.time()
+    g = G.Grid(P, semantics=G.SEMANTICS_EXACT, device=local).classify()
+    build_wall = time.time() - t0
+    st_build = g.stats()
+    t0 = time.time()
+    gref = G.Grid(P, semantics=G.SEMANTICS_REFERENCE, max_depth=REF_DEPTH_C1, device=local).classify()
+    ref_build_wall = time.time() - t0
+    st_ref = gref.stats()
+
+    n = args.points
+    pts = device_points(n, 1234 + rank, "cuda:%d" % local)
+    labels = torch.empty(n, dtype=torch.uint8, device="cuda:%d" % local)
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    lp, pp = labels.data_ptr(), pts.data_ptr()
+
+    def q32():
+        g.query_device(pp, n, lp, G.QUERY_FP32_FILTER, sh)
+
+    def q64():
+        g.query_device(pp, n, lp, G.QUERY_FP64_FILTER, sh)
+
+    def qref():
+        gref.query_device(pp, n, lp, G.QUERY_REFERENCE_FP64, sh)
+
+    # escalation statistics from one counted pass
+    g.query_device(pp, n, lp, G.QUERY_FP32_FILTER, sh, sync=True)
+    esc = g.stats()
+    inside = int((labels == 2).sum().item())
+
+    for _ in range(args.warmup):
+        q32()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t = timed_loop(q32, args.steps, stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if world > 1:
+        tt = torch.tensor([t], device="cuda:%d" % local, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    rate = world * n * args.steps / t / 1e6
+    per_launch = t / args.steps
+
+    # comparison paths (same points, same stream)
+    for _ in range(2):
+        q64()
+    t64 = timed_loop(q64, max(10, args.steps // 4), stream) / max(10, args.steps // 4)
+    for _ in range(2):
+        qref()
+    kref = max(3, args.steps // 40)
+    tref = timed_loop(qref, kref, stream) / kref
+
+    # end to end through the C ABI with pinned host buffers
+    e2e_n = n
+    host_ll = torch.empty((e2e_n, 2), dtype=torch.float64, pin_memory=True)
+    host_ll.copy_(pts[:e2e_n])
+    host_lab = torch.empty(e2e_n, dtype=torch.uint8, pin_memory=True)
+    L = G._lib.lib()
+    hp, hl = ctypes.c_void_p(host_ll.data_ptr()), ctypes.c_void_p(host_lab.data_ptr())
+    G.check(L.gahhg_query(g._h, hp, e2e_n, hl, G.QUERY_FP32_FILTER))
+    torch.cuda.synchronize()
+    te = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        G.check(L.gahhg_query(g._h, hp, e2e_n, hl, G.QUERY_FP32_FILTER))
+    te = (time.perf_counter() - te) / args.e2e_steps
+    if world > 1:
+        tt = torch.tensor([te], device="cuda:%d" % local, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te = float(tt.item())
+    e2e_rate = world * e2e_n / te / 1e6
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from gahhg_b200 import synth
+        sample = synth.uniform_points(args.ref_sample, np.random.default_rng(0))
+        threads = os.cpu_count()
+        v, info = cpu_reference_rate(rings, sample, threads, args.cpu_budget)
+        if v is not None:
+            cpu = {"value": round(v, 3), "unit": "Mpts/s", "cores": threads, "kind": "reference",
+                   "sample": "reference GAHHG kernels built for the CPU, maxDepth %d, OpenMP %d threads; "
+                             "%d uniform C1 points per pass for %.0f s (%s)" % (
+                                 REF_DEPTH_C1, threads, len(sample), args.cpu_budget, json.dumps(info))}
+        else:
+            cpu = {"value": None, "unit": "Mpts/s", "cores": 0, "kind": "reference", "sample": info}
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    peak, peak_kind = _peaks()
+    achieved = BYTES_PER_POINT * n / per_launch / 1e9
+    out = {
+        "metric": METRIC, "value": round(rate, 1), "unit": "Mpts/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(per_launch * 1e3, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "C1: 1,000,000-vertex outer ring + 10 x 10,000-vertex holes (1.1M edges), "
+                               "1e8 uniform FP64 lon/lat points per GPU; exact labels, FP32 certified filter",
+                   "points_per_step": n, "edges": int(P.num_edges), "inputs": "1.6 GB per GPU, larger than L2",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": args.traffic,
+                     "bytes_per_point": BYTES_PER_POINT, "peak_source": peak_kind},
+        "cpu_baseline": cpu,
+        "e2e": {"value": round(e2e_rate, 1), "unit": "Mpts/s", "h2d_bytes_per_step": 16 * e2e_n,
+                "d2h_bytes_per_step": e2e_n},
+        "gpu_launches": args.steps,
+        "clocks": clk,
+        "comparison": {
+            "fp64_filter_exact_mpts": round(world * n / t64 / 1e6, 1),
+            "reference_fp64_descent_mpts": round(world * n / tref / 1e6, 1),
+            "speedup_vs_reference_fp64": round(tref / per_launch, 2),
+            "reference_fp64_max_depth": REF_DEPTH_C1,
+        },
+        "build_ms": {"exact_total_wall": round(build_wall * 1e3, 1),
+                     "hierarchy_create": round(st_build["create_s"] * 1e3, 2),
+                     "hierarchy_classify": round(st_build["classify_s"] * 1e3, 2),
+                     "lattice": round(st_build["lattice_s"] * 1e3, 2),
+                     "hierarchy_depth": st_build["depth"],
+                     "walk_limit_hits": st_build["walk_limit_hits"],
+                     "reference_semantics_total_wall": round(ref_build_wall * 1e3, 1),
+                     "reference_semantics_create": round(st_ref["create_s"] * 1e3, 2)},
+        "escalation": {"boundary_points": esc["boundary_points"], "fp64_tests": esc["esc_fp64"],
+                       "exact_tests": esc["esc_exact"],
+                       "boundary_fraction": round(esc["boundary_points"] / n, 6)},
+        "inside_fraction": round(inside / n, 6),
+        "lattice_bytes": st_build["lattice_bytes"],
+    }
+    print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

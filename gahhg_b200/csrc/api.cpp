@@ -246,7 +246,7 @@ static gahhg_status run_query(Grid* g, const double* d_lonlat, size_t n, uint8_t
     }
     if (precision == GAHHG_QUERY_AUTO)
         precision = g->lattice ? GAHHG_QUERY_FP32_FILTER : GAHHG_QUERY_REFERENCE_FP64;
-    if (precision == GAHHG_QUERY_REFERENCE_FP64) return grid_query_ref(g, d_lonlat, n, d_labels, s);
+    if (precision == GAHHG_QUERY_REFERENCE_FP64) return grid_query_ref(g, d_lonlat, n, d_labels, s, d_counters);
     if (precision == GAHHG_QUERY_FP32_FILTER || precision == GAHHG_QUERY_FP64_FILTER) {
         if (!g->lattice) {
             set_error("exact precision needs a grid built with GAHHG_SEMANTICS_EXACT");
@@ -294,6 +294,7 @@ gahhg_status gahhg_query_device(gahhg_grid* G, const double* d_lonlat, size_t n,
     g->stats.esc_fp64 = (long long)cnt[0];
     g->stats.esc_exact = (long long)cnt[1];
     g->stats.boundary_points = (long long)cnt[2];
+    g->stats.in_count = (long long)cnt[3];
     return GAHHG_OK;
 }
 
@@ -322,11 +323,6 @@ gahhg_status gahhg_query(gahhg_grid* G, const double* lonlat, size_t n, uint8_t*
     if (d_ll) cudaFreeAsync(d_ll, s);
     if (d_lab) cudaFreeAsync(d_lab, s);
     cudaStreamSynchronize(s);
-    if (st == GAHHG_OK) {
-        long long in = 0;
-        for (size_t i = 0; i < n; i++) in += labels[i] == CELL_IN;
-        g->stats.in_count = in;
-    }
     return st;
 }
 

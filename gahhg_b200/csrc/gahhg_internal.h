@@ -145,7 +145,8 @@ struct Grid {
 
 gahhg_status grid_build(Grid* g);
 gahhg_status grid_classify(Grid* g);
-gahhg_status grid_query_ref(Grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels, cudaStream_t s);
+gahhg_status grid_query_ref(Grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels, cudaStream_t s,
+                            uint64_t* d_counters);
 gahhg_status grid_prepare_query(Grid* g);
 gahhg_status check_device_errors(Grid* g, const char* phase);
 

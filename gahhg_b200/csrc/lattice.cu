@@ -704,16 +704,32 @@ __device__ __forceinline__ uint8_t lattice_point(const QueryView& Q, double lon,
     return leaf_label(Q, w & INDEX_MASK, P, fp32, ctr);
 }
 
+// block-reduced count of inside labels (statistics only)
+__device__ __forceinline__ void count_inside(int v, unsigned long long* dst)
+{
+    __shared__ int s_sum;
+    if (threadIdx.x == 0) s_sum = 0;
+    __syncthreads();
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(&s_sum, v);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_sum) atomicAdd(dst, (unsigned long long)s_sum);
+}
+
 template <bool FP32>
 __global__ void __launch_bounds__(TPB) k_lattice_query(const double2* __restrict__ ll, long long n,
                                                        uint8_t* __restrict__ out, QueryView Q,
                                                        unsigned long long* ctr)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
+    int inside = 0;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const double2 p = ll[i];
-        out[i] = lattice_point(Q, p.x, p.y, FP32, ctr);
+        const uint8_t lab = lattice_point(Q, p.x, p.y, FP32, ctr);
+        out[i] = lab;
+        inside += lab == CELL_IN;
     }
+    if (ctr) count_inside(inside, ctr + 3);
 }
 
 }  // namespace

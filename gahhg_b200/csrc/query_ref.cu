@@ -150,14 +150,27 @@ __device__ __forceinline__ uint8_t classify_point(D3 p, const QueryView& q)
 }
 
 __global__ void __launch_bounds__(TPB) k_query_ref(const double2* __restrict__ lonlat, long long n,
-                                                   uint8_t* __restrict__ out, QueryView q)
+                                                   uint8_t* __restrict__ out, QueryView q,
+                                                   unsigned long long* inside_count)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
+    int inside = 0;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const double2 ll = lonlat[i];
         double xyz[3];
         gahhg_canon_query_xyz(ll.x, ll.y, xyz);
-        out[i] = classify_point(d3(xyz[0], xyz[1], xyz[2]), q);
+        const uint8_t lab = classify_point(d3(xyz[0], xyz[1], xyz[2]), q);
+        out[i] = lab;
+        inside += lab == CELL_IN;
+    }
+    if (inside_count) {
+        __shared__ int s_sum;
+        if (threadIdx.x == 0) s_sum = 0;
+        __syncthreads();
+        for (int d = 16; d > 0; d >>= 1) inside += __shfl_down_sync(0xffffffffu, inside, d);
+        if ((threadIdx.x & 31) == 0 && inside) atomicAdd(&s_sum, inside);
+        __syncthreads();
+        if (threadIdx.x == 0 && s_sum) atomicAdd(inside_count, (unsigned long long)s_sum);
     }
 }
 
@@ -204,7 +217,8 @@ size_t query_layout_bytes(const void* p)
            L->E.cap * sizeof(QEdge);
 }
 
-gahhg_status grid_query_ref(Grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels, cudaStream_t s)
+gahhg_status grid_query_ref(Grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels, cudaStream_t s,
+                            uint64_t* d_counters)
 {
     GAHHG_TRY(grid_prepare_query(g));
     if (n == 0) return GAHHG_OK;
@@ -214,7 +228,8 @@ gahhg_status grid_query_ref(Grid* g, const double* d_lonlat, size_t n, uint8_t* 
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
     long long want = ((long long)n + TPB - 1) / TPB;
     int grid = (int)(want < (long long)sms * 16 ? want : (long long)sms * 16);
-    k_query_ref<<<grid, TPB, 0, s>>>((const double2*)d_lonlat, (long long)n, d_labels, q);
+    k_query_ref<<<grid, TPB, 0, s>>>((const double2*)d_lonlat, (long long)n, d_labels, q,
+                                     d_counters ? (unsigned long long*)d_counters + 3 : nullptr);
     GAHHG_CUDA_TRY(cudaGetLastError());
     return GAHHG_OK;
 }

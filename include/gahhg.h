@@ -85,6 +85,7 @@ typedef struct {
     long long esc_fp64;        /* exact query: (point, edge) tests escalated to FP64 */
     long long esc_exact;       /* exact query: tests escalated to expansion arithmetic */
     long long boundary_points; /* exact query: points that ran crossing tests */
+    long long walk_limit_hits; /* edge walks stopped at the step limit (the reference would not terminate) */
 } gahhg_stats;
 
 /* Defaults as in GPISPParam::GPISPParam (source/GPISPParam.h:64-77). */
