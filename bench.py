@@ -340,7 +340,7 @@ def main():
         "cpu_baseline": cpu,
         "e2e": {"value": round(e2e_rate, 1), "unit": "Mpts/s", "h2d_bytes_per_step": 16 * e2e_n,
                 "d2h_bytes_per_step": e2e_n},
-        "gpu_launches": args.steps,
+        "gpu_launches": 2 * args.steps * ((n + (1 << 27) - 1) // (1 << 27)),
         "clocks": clk,
         "comparison": {
             "fp64_filter_exact_mpts": round(world * n / t64 / 1e6, 1),

@@ -665,43 +665,37 @@ __device__ uint8_t leaf_label(const QueryView& Q, uint32_t leaf, PointCtx& P, bo
     return (uint8_t)(par ? 3 - L.label : L.label);
 }
 
-__device__ __forceinline__ uint8_t lattice_point(const QueryView& Q, double lon, double lat, bool fp32,
-                                                 unsigned long long* ctr)
+// Top-level index of a point given its (range-reduced) degrees.
+struct Loc {
+    int ix, iy;
+    double fu, fv;
+};
+
+__device__ __forceinline__ Loc top_locate(const QueryView& Q, double lo, double la)
 {
-    PointCtx P;
-    P.lat = gahhg_canon_query_lat(lat);
-    P.lon = lon;
-    P.have64 = false;
-    double lo = lon, la = P.lat;
-    if (!(fabs(lo) <= 540.0 && fabs(la) <= 90.0)) {
-        if (!(isfinite(lo) && isfinite(la))) return CELL_UNDEFINED;
-        // unusual input: locate from the canonical XYZ itself
-        P.need64();
-        la = asin(fmin(1.0, fmax(-1.0, P.q[1]))) / RAD;
-        lo = atan2(P.q[0], P.q[2]) / RAD;
-    }
     double u = (lo + 180.0) * Q.su;
     if (u >= Q.W) u -= Q.W;
     if (u < 0) u += Q.W;
     const double v = (la + 90.0) * Q.su;
-    P.lon_r = fmin(180.0, fmax(-180.0, u / Q.su - 180.0));
-    P.lat_r = la;
-    int ix = (int)u, iy = (int)v;
-    ix = min(max(ix, 0), Q.W - 1);
-    iy = min(max(iy, 0), Q.H - 1);
-    double fu = u - ix, fv = v - iy;
-    uint32_t w = __ldg(Q.nodes + (size_t)iy * Q.W + ix);
+    Loc L;
+    L.ix = min(max((int)u, 0), Q.W - 1);
+    L.iy = min(max((int)v, 0), Q.H - 1);
+    L.fu = u - L.ix;
+    L.fv = v - L.iy;
+    return L;
+}
+
+__device__ __forceinline__ uint32_t descend(const QueryView& Q, uint32_t w, double fu, double fv)
+{
     while ((w & KIND_MASK) == KIND_INNER) {
         fu *= FAN;
         fv *= FAN;
-        int cx = min(max((int)fu, 0), FAN - 1), cy = min(max((int)fv, 0), FAN - 1);
+        const int cx = min(max((int)fu, 0), FAN - 1), cy = min(max((int)fv, 0), FAN - 1);
         fu -= cx;
         fv -= cy;
         w = __ldg(Q.nodes + (w & INDEX_MASK) + cy * FAN + cx);
     }
-    if ((w & KIND_MASK) == KIND_PURE) return (uint8_t)(w & 3u);
-    if (ctr) atomicAdd(ctr + 2, 1ull);
-    return leaf_label(Q, w & INDEX_MASK, P, fp32, ctr);
+    return w;
 }
 
 // block-reduced count of inside labels (statistics only)
@@ -716,16 +710,103 @@ __device__ __forceinline__ void count_inside(int v, unsigned long long* dst)
     if (threadIdx.x == 0 && s_sum) atomicAdd(dst, (unsigned long long)s_sum);
 }
 
-template <bool FP32>
-__global__ void __launch_bounds__(TPB) k_lattice_query(const double2* __restrict__ ll, long long n,
-                                                       uint8_t* __restrict__ out, QueryView Q,
-                                                       unsigned long long* ctr)
+constexpr int LOC_UNROLL = 4;
+constexpr uint8_t LABEL_PENDING = 0;
+
+// Pass 1: every point whose cell has no edges gets its label; the others are
+// queued (index within this chunk) for pass 2.  Lean on registers so that
+// many warps keep loads in flight; lon/lat and labels stream with an
+// evict-first policy so the node table stays in L2.
+__global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, int n, uint8_t* __restrict__ out,
+                                               QueryView Q, uint32_t* __restrict__ queue,
+                                               unsigned int* __restrict__ qcount, unsigned long long* ctr)
 {
-    const long long stride = (long long)gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
     int inside = 0;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    for (long long base = (long long)blockIdx.x * TPB * LOC_UNROLL; base < n;
+         base += (long long)gridDim.x * TPB * LOC_UNROLL) {
+        double2 p[LOC_UNROLL];
+#pragma unroll
+        for (int k = 0; k < LOC_UNROLL; k++) {
+            const long long i = base + k * TPB + threadIdx.x;
+            p[k] = i < n ? __ldcs(ll + i) : make_double2(0.0, 0.0);
+        }
+        uint32_t w[LOC_UNROLL];
+        Loc L[LOC_UNROLL];
+        bool slow[LOC_UNROLL];
+#pragma unroll
+        for (int k = 0; k < LOC_UNROLL; k++) {
+            const double la = gahhg_canon_query_lat(p[k].y);
+            const double lo = p[k].x;
+            slow[k] = !(fabs(lo) <= 540.0 && fabs(la) <= 90.0);
+            L[k] = top_locate(Q, slow[k] ? 0.0 : lo, slow[k] ? 0.0 : la);
+            w[k] = __ldg(Q.nodes + (size_t)L[k].iy * Q.W + L[k].ix);
+        }
+#pragma unroll
+        for (int k = 0; k < LOC_UNROLL; k++) {
+            const long long i = base + k * TPB + threadIdx.x;
+            const bool valid = i < n;
+            uint8_t lab = LABEL_PENDING;
+            bool push = false;
+            if (valid) {
+                if (slow[k]) {
+                    push = isfinite(p[k].x) && isfinite(p[k].y);  // non-finite input stays undefined
+                } else {
+                    const uint32_t d = descend(Q, w[k], L[k].fu, L[k].fv);
+                    if ((d & KIND_MASK) == KIND_PURE)
+                        lab = (uint8_t)(d & 3u);
+                    else
+                        push = true;
+                }
+            }
+            const unsigned int mask = __ballot_sync(0xffffffffu, push);
+            if (mask) {
+                unsigned int pos = 0;
+                const int leader = __ffs(mask) - 1;
+                if (lane == leader) pos = atomicAdd(qcount, (unsigned int)__popc(mask));
+                pos = __shfl_sync(0xffffffffu, pos, leader);
+                if (push) queue[pos + __popc(mask & ((1u << lane) - 1u))] = (uint32_t)i;
+            }
+            if (valid) __stcs(out + i, lab);
+            inside += lab == CELL_IN;
+        }
+    }
+    if (ctr) count_inside(inside, ctr + 3);
+}
+
+// Pass 2: exact crossing tests for the queued points.
+template <bool FP32>
+__global__ void __launch_bounds__(TPB) k_leaf(const double2* __restrict__ ll, uint8_t* __restrict__ out,
+                                             QueryView Q, const uint32_t* __restrict__ queue,
+                                             const unsigned int* __restrict__ qcount, unsigned long long* ctr)
+{
+    const unsigned int m = *qcount;
+    int inside = 0;
+    for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+        const uint32_t i = queue[t];
         const double2 p = ll[i];
-        const uint8_t lab = lattice_point(Q, p.x, p.y, FP32, ctr);
+        PointCtx P;
+        P.lat = gahhg_canon_query_lat(p.y);
+        P.lon = p.x;
+        P.have64 = false;
+        double lo = P.lon, la = P.lat;
+        if (!(fabs(lo) <= 540.0 && fabs(la) <= 90.0)) {
+            // unusual input: locate from the canonical XYZ itself
+            P.need64();
+            la = asin(fmin(1.0, fmax(-1.0, P.q[1]))) / RAD;
+            lo = atan2(P.q[0], P.q[2]) / RAD;
+        }
+        const Loc L = top_locate(Q, lo, la);
+        P.lon_r = fmin(180.0, fmax(-180.0, (L.ix + L.fu) / Q.su - 180.0));
+        P.lat_r = la;
+        const uint32_t w = descend(Q, __ldg(Q.nodes + (size_t)L.iy * Q.W + L.ix), L.fu, L.fv);
+        uint8_t lab;
+        if ((w & KIND_MASK) == KIND_PURE) {
+            lab = (uint8_t)(w & 3u);
+        } else {
+            if (ctr) atomicAdd(ctr + 2, 1ull);
+            lab = leaf_label(Q, w & INDEX_MASK, P, FP32, ctr);
+        }
         out[i] = lab;
         inside += lab == CELL_IN;
     }
@@ -1094,6 +1175,13 @@ gahhg_status lattice_build(Grid* g)
     return GAHHG_OK;
 }
 
+gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long long n, uint8_t* d_labels,
+                                int precision, cudaStream_t s, uint64_t* d_counters, uint32_t* queue,
+                                unsigned int* qcount, long long chunk, int device);
+
+// Points per pass; the pass-2 queue holds one 4-byte index per point.
+constexpr long long QUERY_CHUNK = 1LL << 27;
+
 gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels, int precision,
                            cudaStream_t s, uint64_t* d_counters)
 {
@@ -1108,16 +1196,36 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
     Q.recs = L->recs.ptr;
     Q.pv = g->poly->d_pv;
     Q.pe = g->poly->d_pe;
+    const long long chunk = std::min<long long>((long long)n, QUERY_CHUNK);
+    uint32_t* queue = nullptr;
+    GAHHG_CUDA_TRY(cudaMallocAsync(&queue, sizeof(uint32_t) * (chunk + 64), s));
+    unsigned int* qcount = (unsigned int*)(queue + chunk + 32);
+    const gahhg_status st = lattice_query_with(Q, d_lonlat, (long long)n, d_labels, precision, s, d_counters,
+                                               queue, qcount, chunk, g->device);
+    cudaFreeAsync(queue, s);
+    return st;
+}
+
+gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long long n, uint8_t* d_labels,
+                                int precision, cudaStream_t s, uint64_t* d_counters, uint32_t* queue,
+                                unsigned int* qcount, long long chunk, int device)
+{
     int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
-    long long want = ((long long)n + TPB - 1) / TPB;
-    int grid = (int)std::min<long long>(want, (long long)sms * 16);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     unsigned long long* ctr = (unsigned long long*)d_counters;
-    if (precision == GAHHG_QUERY_FP64_FILTER)
-        k_lattice_query<false><<<grid, TPB, 0, s>>>((const double2*)d_lonlat, (long long)n, d_labels, Q, ctr);
-    else
-        k_lattice_query<true><<<grid, TPB, 0, s>>>((const double2*)d_lonlat, (long long)n, d_labels, Q, ctr);
-    GAHHG_CUDA_TRY(cudaGetLastError());
+    for (long long off = 0; off < n; off += chunk) {
+        const int m = (int)std::min<long long>(chunk, n - off);
+        const double2* ll = (const double2*)d_lonlat + off;
+        GAHHG_CUDA_TRY(cudaMemsetAsync(qcount, 0, sizeof(unsigned int), s));
+        const long long tiles = ((long long)m + TPB * LOC_UNROLL - 1) / (TPB * LOC_UNROLL);
+        const int grid = (int)std::min<long long>(tiles, (long long)sms * 8);
+        k_locate<<<grid, TPB, 0, s>>>(ll, m, d_labels + off, Q, queue, qcount, ctr);
+        if (precision == GAHHG_QUERY_FP64_FILTER)
+            k_leaf<false><<<sms * 4, TPB, 0, s>>>(ll, d_labels + off, Q, queue, qcount, ctr);
+        else
+            k_leaf<true><<<sms * 4, TPB, 0, s>>>(ll, d_labels + off, Q, queue, qcount, ctr);
+        GAHHG_CUDA_TRY(cudaGetLastError());
+    }
     return GAHHG_OK;
 }
 
