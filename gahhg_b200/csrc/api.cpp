@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstring>
 #include <ctime>
+#include <mutex>
 
 #include "gahhg_internal.h"
 
@@ -20,6 +21,32 @@ void set_error(const char* fmt, ...)
 }
 
 const char* last_error() { return g_err; }
+
+gahhg_status pool_alloc(void** p, size_t bytes, int device, cudaStream_t s)
+{
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    if (device < 0 || device >= 64) {
+        set_error("device ordinal %d out of range", device);
+        return GAHHG_ERR_ARG;
+    }
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!pools[device]) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = device;
+            GAHHG_CUDA_TRY(cudaMemPoolCreate(&pools[device], &props));
+            uint64_t keep = 4ull << 30;  // keep up to 4 GB cached between calls
+            GAHHG_CUDA_TRY(cudaMemPoolSetAttribute(pools[device], cudaMemPoolAttrReleaseThreshold, &keep));
+        }
+        pool = pools[device];
+    }
+    GAHHG_CUDA_TRY(cudaMallocFromPoolAsync(p, bytes, pool, s));
+    return GAHHG_OK;
+}
 
 double now_seconds()
 {
@@ -266,7 +293,7 @@ gahhg_status gahhg_query_device(gahhg_grid* G, const double* d_lonlat, size_t n,
     cudaStream_t s = (cudaStream_t)stream;
     if (!sync) return run_query(g, d_lonlat, n, d_labels, precision, s, nullptr);
     uint64_t* d_cnt = nullptr;
-    GAHHG_CUDA_TRY(cudaMallocAsync(&d_cnt, 4 * sizeof(uint64_t), s));
+    GAHHG_TRY(pool_alloc((void**)&d_cnt, 4 * sizeof(uint64_t), g->device, s));
     GAHHG_CUDA_TRY(cudaMemsetAsync(d_cnt, 0, 4 * sizeof(uint64_t), s));
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -307,8 +334,8 @@ gahhg_status gahhg_query(gahhg_grid* G, const double* lonlat, size_t n, uint8_t*
     double* d_ll = nullptr;
     uint8_t* d_lab = nullptr;
     if (n) {
-        GAHHG_CUDA_TRY(cudaMallocAsync(&d_ll, n * 2 * sizeof(double), s));
-        GAHHG_CUDA_TRY(cudaMallocAsync(&d_lab, n, s));
+        GAHHG_TRY(pool_alloc((void**)&d_ll, n * 2 * sizeof(double), g->device, s));
+        GAHHG_TRY(pool_alloc((void**)&d_lab, n, g->device, s));
         GAHHG_CUDA_TRY(cudaMemcpyAsync(d_ll, lonlat, n * 2 * sizeof(double), cudaMemcpyHostToDevice, s));
     }
     gahhg_status st = gahhg_query_device(G, d_ll, n, d_lab, precision, s, 1);

@@ -166,6 +166,11 @@ gahhg_status scan_exclusive(const int* d_in, int* d_out, int n, int* d_total, vo
 
 double now_seconds();
 
+// Stream-ordered scratch from a library-owned pool per device that keeps
+// freed memory cached (the default pool returns it to the driver at every
+// synchronisation, which made each query pay for a fresh mapping).
+gahhg_status pool_alloc(void** p, size_t bytes, int device, cudaStream_t s);
+
 }  // namespace gahhg
 
 struct gahhg_polygon { gahhg::Polygon p; };

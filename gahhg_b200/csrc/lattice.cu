@@ -544,6 +544,27 @@ __global__ void k_leaf_records(BuildView v, int lvl, int nn, const int* is_leaf,
     }
 }
 
+// Coarse summary of the top level: a coarse cell whose top cells are all
+// edge-free with one label gets that label, otherwise "mixed".
+__global__ void k_summary(const uint32_t* nodes, int W, int H, int cshift, uint32_t* summary, int ncoarse)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncoarse) return;
+    const int CW = W >> cshift;
+    const int cx = c % CW, cy = c / CW;
+    const int f = 1 << cshift;
+    uint32_t code = 0xFFu;
+    for (int y = cy * f; y < (cy + 1) * f && code != 2u; y++)
+        for (int x = cx * f; x < (cx + 1) * f; x++) {
+            const uint32_t w = nodes[(size_t)y * W + x];
+            const uint32_t v = ((w & KIND_MASK) == KIND_PURE) ? (w & 3u) - 1u : 2u;  // 0 out, 1 in, 2 mixed
+            if (code == 0xFFu) code = v;
+            else if (code != v) code = 2u;
+            if (code == 2u) break;
+        }
+    atomicOr(&summary[c >> 4], code << ((c & 15) * 2));
+}
+
 __global__ void k_shift_leaf_words(uint32_t* nodes, int start, int nn, int add)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -557,6 +578,10 @@ __global__ void k_shift_leaf_words(uint32_t* nodes, int start, int nn, int add)
 struct QueryView {
     int W, H;
     double su;  // W / 360 (= H / 180)
+    int cshift;               // coarse cell = (1 << cshift) x (1 << cshift) top cells
+    int CW;                   // coarse columns
+    int swords;               // 32-bit words of the coarse summary
+    const uint32_t* summary;  // 2 bits per coarse cell: 0 out, 1 in, 2 mixed
     const uint32_t* nodes;
     const LeafRec* leaves;
     const EdgeRec* recs;
@@ -721,6 +746,9 @@ __global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, 
                                                QueryView Q, uint32_t* __restrict__ queue,
                                                unsigned int* __restrict__ qcount, unsigned long long* ctr)
 {
+    extern __shared__ uint32_t s_sum[];
+    for (int k = threadIdx.x; k < Q.swords; k += TPB) s_sum[k] = __ldg(Q.summary + k);
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     int inside = 0;
     for (long long base = (long long)blockIdx.x * TPB * LOC_UNROLL; base < n;
@@ -731,32 +759,29 @@ __global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, 
             const long long i = base + k * TPB + threadIdx.x;
             p[k] = i < n ? __ldcs(ll + i) : make_double2(0.0, 0.0);
         }
-        uint32_t w[LOC_UNROLL];
-        Loc L[LOC_UNROLL];
-        bool slow[LOC_UNROLL];
-#pragma unroll
-        for (int k = 0; k < LOC_UNROLL; k++) {
-            const double la = gahhg_canon_query_lat(p[k].y);
-            const double lo = p[k].x;
-            slow[k] = !(fabs(lo) <= 540.0 && fabs(la) <= 90.0);
-            L[k] = top_locate(Q, slow[k] ? 0.0 : lo, slow[k] ? 0.0 : la);
-            w[k] = __ldg(Q.nodes + (size_t)L[k].iy * Q.W + L[k].ix);
-        }
 #pragma unroll
         for (int k = 0; k < LOC_UNROLL; k++) {
             const long long i = base + k * TPB + threadIdx.x;
-            const bool valid = i < n;
             uint8_t lab = LABEL_PENDING;
             bool push = false;
-            if (valid) {
-                if (slow[k]) {
-                    push = isfinite(p[k].x) && isfinite(p[k].y);  // non-finite input stays undefined
+            if (i < n) {
+                const double la = gahhg_canon_query_lat(p[k].y);
+                const double lo = p[k].x;
+                if (!(fabs(lo) <= 540.0 && fabs(la) <= 90.0)) {
+                    push = isfinite(lo) && isfinite(la);  // non-finite input stays undefined
                 } else {
-                    const uint32_t d = descend(Q, w[k], L[k].fu, L[k].fv);
-                    if ((d & KIND_MASK) == KIND_PURE)
-                        lab = (uint8_t)(d & 3u);
-                    else
-                        push = true;
+                    const Loc L = top_locate(Q, lo, la);
+                    const int c = (L.iy >> Q.cshift) * Q.CW + (L.ix >> Q.cshift);
+                    const uint32_t code = (s_sum[c >> 4] >> ((c & 15) * 2)) & 3u;
+                    if (code < 2u) {
+                        lab = (uint8_t)(code + 1u);  // coarse cell without edges: most points end here
+                    } else {
+                        const uint32_t d = descend(Q, __ldg(Q.nodes + (size_t)L.iy * Q.W + L.ix), L.fu, L.fv);
+                        if ((d & KIND_MASK) == KIND_PURE)
+                            lab = (uint8_t)(d & 3u);
+                        else
+                            push = true;
+                    }
                 }
             }
             const unsigned int mask = __ballot_sync(0xffffffffu, push);
@@ -767,7 +792,7 @@ __global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, 
                 pos = __shfl_sync(0xffffffffu, pos, leader);
                 if (push) queue[pos + __popc(mask & ((1u << lane) - 1u))] = (uint32_t)i;
             }
-            if (valid) __stcs(out + i, lab);
+            if (i < n) __stcs(out + i, lab);
             inside += lab == CELL_IN;
         }
     }
@@ -823,6 +848,8 @@ struct Lattice {
     DevArray<uint32_t> nodes;
     DevArray<LeafRec> leaves;
     DevArray<EdgeRec> recs;
+    DevArray<uint32_t> summary;
+    int cshift = 0, swords = 0;
     long long nnodes = 0, nleaves = 0, nrecs = 0;
     int origin_label = 0;
     double x_in[3]{};
@@ -834,6 +861,7 @@ void lattice_free(Lattice* L)
     L->nodes.release();
     L->leaves.release();
     L->recs.release();
+    L->summary.release();
     delete L;
 }
 
@@ -1156,6 +1184,17 @@ gahhg_status lattice_build(Grid* g)
         if (leaf_base[lvl] == 0) continue;
         k_shift_leaf_words<<<blocks_for(lv[lvl].nn), TPB, 0, s>>>(L->nodes.ptr, lv[lvl].gstart, lv[lvl].nn, leaf_base[lvl]);
     }
+    {
+        // coarse summary: at most 256 x 128 cells (8 KB), staged in shared memory by the query
+        int cs = 0;
+        while ((W >> cs) > 256) cs++;
+        const int CW = W >> cs, CH = (W / 2) >> cs;
+        L->cshift = cs;
+        L->swords = (CW * CH + 15) / 16;
+        GAHHG_TRY(L->summary.reserve(L->swords, s, false));
+        GAHHG_CUDA_TRY(cudaMemsetAsync(L->summary.ptr, 0, sizeof(uint32_t) * L->swords, s));
+        k_summary<<<blocks_for(CW * CH), TPB, 0, s>>>(L->nodes.ptr, W, W / 2, cs, L->summary.ptr, CW * CH);
+    }
     int bad[4];
     GAHHG_CUDA_TRY(cudaMemcpyAsync(bad, d_bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
     GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1196,9 +1235,13 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
     Q.recs = L->recs.ptr;
     Q.pv = g->poly->d_pv;
     Q.pe = g->poly->d_pe;
+    Q.cshift = L->cshift;
+    Q.CW = L->geo.W >> L->cshift;
+    Q.swords = L->swords;
+    Q.summary = L->summary.ptr;
     const long long chunk = std::min<long long>((long long)n, QUERY_CHUNK);
     uint32_t* queue = nullptr;
-    GAHHG_CUDA_TRY(cudaMallocAsync(&queue, sizeof(uint32_t) * (chunk + 64), s));
+    GAHHG_TRY(pool_alloc((void**)&queue, sizeof(uint32_t) * (chunk + 64), g->device, s));
     unsigned int* qcount = (unsigned int*)(queue + chunk + 32);
     const gahhg_status st = lattice_query_with(Q, d_lonlat, (long long)n, d_labels, precision, s, d_counters,
                                                queue, qcount, chunk, g->device);
@@ -1219,7 +1262,7 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
         GAHHG_CUDA_TRY(cudaMemsetAsync(qcount, 0, sizeof(unsigned int), s));
         const long long tiles = ((long long)m + TPB * LOC_UNROLL - 1) / (TPB * LOC_UNROLL);
         const int grid = (int)std::min<long long>(tiles, (long long)sms * 8);
-        k_locate<<<grid, TPB, 0, s>>>(ll, m, d_labels + off, Q, queue, qcount, ctr);
+        k_locate<<<grid, TPB, sizeof(uint32_t) * Q.swords, s>>>(ll, m, d_labels + off, Q, queue, qcount, ctr);
         if (precision == GAHHG_QUERY_FP64_FILTER)
             k_leaf<false><<<sms * 4, TPB, 0, s>>>(ll, d_labels + off, Q, queue, qcount, ctr);
         else
