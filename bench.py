@@ -97,6 +97,27 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+class quiet_stdout:
+    """Route C-level stdout to stderr (the reference code prints progress
+    lines) so that stdout carries only the JSON result line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        try:
+            import ctypes as _c
+            _c.CDLL(None).fflush(None)
+        except Exception:
+            pass
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        return False
+
+
 def c1_polygon_cached():
     from gahhg_b200 import synth
     path = os.path.join(REPO, "_work", "bench_c1_rings.npz") if os.path.isdir(os.path.join(REPO, "_work")) else None
@@ -141,15 +162,16 @@ def cpu_reference_rate(rings, sample_points, threads, budget_s=12.0):
         return None, "oracle/_ref not built"
     tmp = os.path.join("/tmp", "gahhg_bench_c1_%d.txt" % os.getpid())
     synth.write_polygon(tmp, rings)
-    t0 = time.time()
-    r = ref.RefGPISP(tmp, maxdepth=REF_DEPTH_C1, threads=threads)
-    build_s = time.time() - t0
-    done, t1 = 0, time.time()
-    while time.time() - t1 < budget_s:
-        r.query(sample_points)
-        done += len(sample_points)
-    dt = time.time() - t1
-    r.close()
+    with quiet_stdout():
+        t0 = time.time()
+        r = ref.RefGPISP(tmp, maxdepth=REF_DEPTH_C1, threads=threads)
+        build_s = time.time() - t0
+        done, t1 = 0, time.time()
+        while time.time() - t1 < budget_s:
+            r.query(sample_points)
+            done += len(sample_points)
+        dt = time.time() - t1
+        r.close()
     os.unlink(tmp)
     return done / dt / 1e6, {"build_s": round(build_s, 3), "points": done, "seconds": round(dt, 3)}
 
@@ -167,17 +189,18 @@ def run_reference(args):
     rings = c1_polygon_cached()
     tmp = os.path.join("/tmp", "gahhg_bench_ref_%d.txt" % os.getpid())
     synth.write_polygon(tmp, rings)
-    t0 = time.time()
-    r = ref.RefGPISP(tmp, maxdepth=REF_DEPTH_C1, threads=threads)
-    build_s = time.time() - t0
-    sample = synth.uniform_points(args.ref_sample, np.random.default_rng(0))
-    for _ in range(args.warmup):
-        r.query(sample)
-    t1 = time.time()
-    for _ in range(args.steps):
-        r.query(sample)
-    dt = time.time() - t1
-    r.close()
+    with quiet_stdout():
+        t0 = time.time()
+        r = ref.RefGPISP(tmp, maxdepth=REF_DEPTH_C1, threads=threads)
+        build_s = time.time() - t0
+        sample = synth.uniform_points(args.ref_sample, np.random.default_rng(0))
+        for _ in range(args.warmup):
+            r.query(sample)
+        t1 = time.time()
+        for _ in range(args.steps):
+            r.query(sample)
+        dt = time.time() - t1
+        r.close()
     os.unlink(tmp)
     rate = args.steps * len(sample) / dt / 1e6
     desc = ("reference GAHHG kernels built for the CPU (oracle/_ref), OpenMP over %d threads, maxDepth %d; "
