@@ -81,6 +81,8 @@ _SIGS = {
     "gahhg_grid_free": (None, [_P]),
     "gahhg_query_device": (ctypes.c_int, [_P, _P, ctypes.c_size_t, _P, ctypes.c_int, _P, ctypes.c_int]),
     "gahhg_query": (ctypes.c_int, [_P, _P, ctypes.c_size_t, _P, ctypes.c_int]),
+    "gahhg_query_device_noalloc": (ctypes.c_int, [_P, _P, ctypes.c_size_t, _P, ctypes.c_int, _P]),
+    "gahhg_query_noalloc_max_points": (ctypes.c_longlong, []),
     "gahhg_stats_get": (ctypes.c_int, [_P, ctypes.POINTER(Stats)]),
     "gahhg_grid_depth": (ctypes.c_int, [_P]),
     "gahhg_grid_export": (ctypes.c_int, [_P, _P, _P, _P, _P, _P]),

@@ -325,6 +325,33 @@ gahhg_status gahhg_query_device(gahhg_grid* G, const double* d_lonlat, size_t n,
     return GAHHG_OK;
 }
 
+gahhg_status gahhg_query_device_noalloc(gahhg_grid* G, const double* d_lonlat, size_t n, uint8_t* d_labels,
+                                        int precision, void* stream)
+{
+    if (!G || (n && (!d_lonlat || !d_labels))) {
+        set_error("gahhg_query_device_noalloc: null argument");
+        return GAHHG_ERR_ARG;
+    }
+    Grid* g = &G->g;
+    if (!g->classified) {
+        set_error("query before classify");
+        return GAHHG_ERR_STATE;
+    }
+    if (!g->lattice) {
+        set_error("gahhg_query_device_noalloc needs a grid built with GAHHG_SEMANTICS_EXACT");
+        return GAHHG_ERR_STATE;
+    }
+    if (precision == GAHHG_QUERY_AUTO) precision = GAHHG_QUERY_FP32_FILTER;
+    if (precision != GAHHG_QUERY_FP32_FILTER && precision != GAHHG_QUERY_FP64_FILTER) {
+        set_error("gahhg_query_device_noalloc supports the exact precisions only");
+        return GAHHG_ERR_ARG;
+    }
+    GAHHG_CUDA_TRY(cudaSetDevice(g->device));
+    return lattice_query_noalloc(g, d_lonlat, n, d_labels, precision, (cudaStream_t)stream);
+}
+
+long long gahhg_query_noalloc_max_points(void) { return lattice_noalloc_max_points(); }
+
 gahhg_status gahhg_query(gahhg_grid* G, const double* lonlat, size_t n, uint8_t* labels, int precision)
 {
     if (!G || (n && (!lonlat || !labels))) return GAHHG_ERR_ARG;

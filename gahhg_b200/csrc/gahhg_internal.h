@@ -154,6 +154,9 @@ gahhg_status check_device_errors(Grid* g, const char* phase);
 gahhg_status lattice_build(Grid* g);
 gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels, int precision,
                            cudaStream_t s, uint64_t* d_counters);
+gahhg_status lattice_query_noalloc(Grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels, int precision,
+                                   cudaStream_t s);
+long long lattice_noalloc_max_points();
 void lattice_free(Lattice* L);
 size_t lattice_bytes(const Lattice* L);
 

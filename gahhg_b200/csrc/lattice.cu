@@ -35,6 +35,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "exact_pred.cuh"
 #include "gahhg_canon.h"
@@ -1270,6 +1271,75 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
         GAHHG_CUDA_TRY(cudaGetLastError());
     }
     return GAHHG_OK;
+}
+
+// ------------------------------------------------- allocation-free query --
+//
+// The same two passes as lattice_query, with the pass-2 queue in a fixed
+// array in device memory instead of memory taken from the pool, for callers
+// that must not allocate (see gahhg_query_device_noalloc in include/gahhg.h).
+// Every device that loads this library reserves the array until the process
+// exits.  All calls share it: calls that overlap on the GPU race.
+
+constexpr long long NOALLOC_MAX_POINTS = 1LL << 21;  // 2,097,152 points per call
+static __device__ __align__(256) uint32_t g_noalloc_queue[NOALLOC_MAX_POINTS + 64];
+
+static std::mutex g_noalloc_mu;
+static uint32_t* g_noalloc_addr[64] = {};
+
+long long lattice_noalloc_max_points() { return NOALLOC_MAX_POINTS; }
+
+// Device address of the array on the current device, looked up once per
+// device (the caller has made g->device current).
+static gahhg_status noalloc_queue_address(int device, uint32_t** out)
+{
+    if (device < 0 || device >= 64) {
+        set_error("device ordinal %d out of range", device);
+        return GAHHG_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_queue);
+        if (e != cudaSuccess || !p) {
+            set_error("cudaGetSymbolAddress(g_noalloc_queue) on device %d: %s", device, cudaGetErrorString(e));
+            return GAHHG_ERR_CUDA;
+        }
+        g_noalloc_addr[device] = (uint32_t*)p;
+    }
+    *out = g_noalloc_addr[device];
+    return GAHHG_OK;
+}
+
+gahhg_status lattice_query_noalloc(Grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels, int precision,
+                                   cudaStream_t s)
+{
+    if ((long long)n > NOALLOC_MAX_POINTS) {
+        set_error("gahhg_query_device_noalloc: %zu points exceed the fixed maximum of %lld per call", n,
+                  NOALLOC_MAX_POINTS);
+        return GAHHG_ERR_CAPACITY;
+    }
+    uint32_t* queue = nullptr;
+    GAHHG_TRY(noalloc_queue_address(g->device, &queue));
+    if (n == 0) return GAHHG_OK;
+    Lattice* L = g->lattice;
+    QueryView Q;
+    Q.W = L->geo.W;
+    Q.H = L->geo.H;
+    Q.su = (double)L->geo.W / 360.0;
+    Q.nodes = L->nodes.ptr;
+    Q.leaves = L->leaves.ptr;
+    Q.recs = L->recs.ptr;
+    Q.pv = g->poly->d_pv;
+    Q.pe = g->poly->d_pe;
+    Q.cshift = L->cshift;
+    Q.CW = L->geo.W >> L->cshift;
+    Q.swords = L->swords;
+    Q.summary = L->summary.ptr;
+    // the queue count lives after the queue; lattice_query_with zeroes it before each pass
+    unsigned int* qcount = (unsigned int*)(queue + NOALLOC_MAX_POINTS + 32);
+    return lattice_query_with(Q, d_lonlat, (long long)n, d_labels, precision, s, nullptr, queue, qcount,
+                              NOALLOC_MAX_POINTS, g->device);
 }
 
 }  // namespace gahhg

@@ -135,6 +135,29 @@ gahhg_status gahhg_query_device(gahhg_grid* g, const double* d_lonlat, size_t n,
  * PISPTime does.  Synchronous. */
 gahhg_status gahhg_query(gahhg_grid* g, const double* lonlat, size_t n, uint8_t* labels, int precision);
 
+/* Same labels as gahhg_query_device, without allocating anything.  No
+ * counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory at query time: an
+ * application that hands the whole device to its own allocator, a serving
+ * loop that reserves all memory up front so a request can never fail on an
+ * allocation, or code that must not hit the implicit synchronisation of
+ * cudaMalloc/cudaFree.  gahhg_query_device takes its pass-2 scratch from a
+ * stream-ordered pool; this variant uses a fixed 8 MB array in device memory
+ * that the library reserves on every GPU that loads it, for as long as the
+ * process lives.  Inputs and outputs are still the caller's device buffers.
+ *
+ * Limits: at most gahhg_query_noalloc_max_points() points per call (2,097,152;
+ * more returns GAHHG_ERR_CAPACITY); exact grids only (GAHHG_QUERY_AUTO,
+ * _FP32_FILTER or _FP64_FILTER); no statistics are collected.  The first call
+ * on a device looks up the array's device address, so make that first call
+ * before any stream capture.  All calls share the one array and it keeps the
+ * last call's contents: calls whose work overlaps on the GPU (two streams,
+ * two host threads) race, so order them on one stream or serialise them. */
+gahhg_status gahhg_query_device_noalloc(gahhg_grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels,
+                                        int precision, void* stream);
+long long gahhg_query_noalloc_max_points(void);
+
 /* ---- statistics / report ------------------------------------------------ */
 
 gahhg_status gahhg_stats_get(const gahhg_grid* g, gahhg_stats* s);
