@@ -740,9 +740,12 @@ constexpr int LOC_UNROLL = 4;
 constexpr uint8_t LABEL_PENDING = 0;
 
 // Pass 1: every point whose cell has no edges gets its label; the others are
-// queued (index within this chunk) for pass 2.  Lean on registers so that
-// many warps keep loads in flight; lon/lat and labels stream with an
-// evict-first policy so the node table stays in L2.
+// queued (index within this chunk) for pass 2.  Lean on registers and
+// instructions so that many warps keep loads in flight; lon/lat and labels
+// stream with an evict-first policy so the node table stays in L2.  The index
+// arithmetic need not match the canonical conversion bit for bit: every cap
+// carries a margin far above its rounding (see LOC_MARGIN).
+template <bool STATS>
 __global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, int n, uint8_t* __restrict__ out,
                                                QueryView Q, uint32_t* __restrict__ queue,
                                                unsigned int* __restrict__ qcount, unsigned long long* ctr)
@@ -751,53 +754,73 @@ __global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, 
     for (int k = threadIdx.x; k < Q.swords; k += TPB) s_sum[k] = __ldg(Q.summary + k);
     __syncthreads();
     const int lane = threadIdx.x & 31;
+    const double su = Q.su, u0 = 180.0 * Q.su, Wd = (double)Q.W;
+    const int wmax = Q.W - 1, hmax = Q.H - 1, cs = Q.cshift, cw = Q.CW;
     int inside = 0;
-    for (long long base = (long long)blockIdx.x * TPB * LOC_UNROLL; base < n;
-         base += (long long)gridDim.x * TPB * LOC_UNROLL) {
+    constexpr int TILE = TPB * LOC_UNROLL;
+    for (int base = blockIdx.x * TILE; base < n; base += gridDim.x * TILE) {
+        const bool full = base + TILE <= n;
         double2 p[LOC_UNROLL];
 #pragma unroll
         for (int k = 0; k < LOC_UNROLL; k++) {
-            const long long i = base + k * TPB + threadIdx.x;
-            p[k] = i < n ? __ldcs(ll + i) : make_double2(0.0, 0.0);
+            const int i = base + k * TPB + threadIdx.x;
+            p[k] = (full || i < n) ? __ldcs(ll + i) : make_double2(0.0, 0.0);
         }
+        uint8_t lab[LOC_UNROLL];
+        bool push[LOC_UNROLL];
+        bool any = false;
 #pragma unroll
         for (int k = 0; k < LOC_UNROLL; k++) {
-            const long long i = base + k * TPB + threadIdx.x;
-            uint8_t lab = LABEL_PENDING;
-            bool push = false;
-            if (i < n) {
-                const double la = gahhg_canon_query_lat(p[k].y);
-                const double lo = p[k].x;
-                if (!(fabs(lo) <= 540.0 && fabs(la) <= 90.0)) {
-                    push = isfinite(lo) && isfinite(la);  // non-finite input stays undefined
-                } else {
-                    const Loc L = top_locate(Q, lo, la);
-                    const int c = (L.iy >> Q.cshift) * Q.CW + (L.ix >> Q.cshift);
-                    const uint32_t code = (s_sum[c >> 4] >> ((c & 15) * 2)) & 3u;
+            const int i = base + k * TPB + threadIdx.x;
+            const double lo = p[k].x;
+            const double laf = p[k].y + 90.0;  // the reference's FakeLL latitude + 90
+            lab[k] = LABEL_PENDING;
+            push[k] = false;
+            if (full || i < n) {
+                if (laf >= 0.0 && laf <= 180.0 && fabs(lo) <= 540.0) {
+                    double u = fma(lo, su, u0);
+                    if (u >= Wd) u -= Wd;
+                    else if (u < 0.0) u += Wd;
+                    const double v = laf * su;
+                    const int ix = min((int)u, wmax), iy = min((int)v, hmax);
+                    const int c = (iy >> cs) * cw + (ix >> cs);
+                    const uint32_t code = (s_sum[c >> 4] >> ((c & 15) << 1)) & 3u;
                     if (code < 2u) {
-                        lab = (uint8_t)(code + 1u);  // coarse cell without edges: most points end here
+                        lab[k] = (uint8_t)(code + 1u);  // coarse cell without edges: most points end here
                     } else {
-                        const uint32_t d = descend(Q, __ldg(Q.nodes + (size_t)L.iy * Q.W + L.ix), L.fu, L.fv);
+                        const uint32_t d = descend(Q, __ldg(Q.nodes + (size_t)iy * Q.W + ix), u - ix, v - iy);
                         if ((d & KIND_MASK) == KIND_PURE)
-                            lab = (uint8_t)(d & 3u);
+                            lab[k] = (uint8_t)(d & 3u);
                         else
-                            push = true;
+                            push[k] = true;
                     }
+                } else {
+                    // unusual coordinates go to pass 2; non-finite input stays undefined
+                    push[k] = isfinite(lo) && isfinite(laf);
                 }
             }
-            const unsigned int mask = __ballot_sync(0xffffffffu, push);
-            if (mask) {
+            any |= push[k];
+        }
+        if (__any_sync(0xffffffffu, any)) {
+#pragma unroll
+            for (int k = 0; k < LOC_UNROLL; k++) {
+                const unsigned int mask = __ballot_sync(0xffffffffu, push[k]);
+                if (!mask) continue;
                 unsigned int pos = 0;
                 const int leader = __ffs(mask) - 1;
                 if (lane == leader) pos = atomicAdd(qcount, (unsigned int)__popc(mask));
                 pos = __shfl_sync(0xffffffffu, pos, leader);
-                if (push) queue[pos + __popc(mask & ((1u << lane) - 1u))] = (uint32_t)i;
+                if (push[k]) queue[pos + __popc(mask & ((1u << lane) - 1u))] = (uint32_t)(base + k * TPB + threadIdx.x);
             }
-            if (i < n) __stcs(out + i, lab);
-            inside += lab == CELL_IN;
+        }
+#pragma unroll
+        for (int k = 0; k < LOC_UNROLL; k++) {
+            const int i = base + k * TPB + threadIdx.x;
+            if (full || i < n) __stcs(out + i, lab[k]);
+            if (STATS) inside += lab[k] == CELL_IN;
         }
     }
-    if (ctr) count_inside(inside, ctr + 3);
+    if (STATS && ctr) count_inside(inside, ctr + 3);
 }
 
 // Pass 2: exact crossing tests for the queued points.
@@ -1263,7 +1286,10 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
         GAHHG_CUDA_TRY(cudaMemsetAsync(qcount, 0, sizeof(unsigned int), s));
         const long long tiles = ((long long)m + TPB * LOC_UNROLL - 1) / (TPB * LOC_UNROLL);
         const int grid = (int)std::min<long long>(tiles, (long long)sms * 8);
-        k_locate<<<grid, TPB, sizeof(uint32_t) * Q.swords, s>>>(ll, m, d_labels + off, Q, queue, qcount, ctr);
+        if (ctr)
+            k_locate<true><<<grid, TPB, sizeof(uint32_t) * Q.swords, s>>>(ll, m, d_labels + off, Q, queue, qcount, ctr);
+        else
+            k_locate<false><<<grid, TPB, sizeof(uint32_t) * Q.swords, s>>>(ll, m, d_labels + off, Q, queue, qcount, ctr);
         if (precision == GAHHG_QUERY_FP64_FILTER)
             k_leaf<false><<<sms * 4, TPB, 0, s>>>(ll, d_labels + off, Q, queue, qcount, ctr);
         else
