@@ -35,6 +35,15 @@ BYTES_PER_POINT = 17  # 16 B lon/lat in + 1 B label out
 REF_DEPTH_C1 = 11     # deepest level at which the reference's edge walks terminate on C1
 
 
+def _traffic_per_point():
+    """DRAM bytes per point of the query kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(REPO, "profiles", "locate_traffic.json")) as f:
+            return float(json.load(f)["bytes_per_point"])
+    except Exception:
+        return None
+
+
 def _peaks():
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -358,7 +367,9 @@ def main():
                    "points_per_step": n, "edges": int(P.num_edges), "inputs": "1.6 GB per GPU, larger than L2",
                    "parallelism": "replicas" if world > 1 else "single"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": args.traffic,
+                     "frac": round(achieved / peak, 4),
+                     "traffic": args.traffic if args.traffic is not None else (
+                         round(_traffic_per_point() * n) if _traffic_per_point() else None),
                      "bytes_per_point": BYTES_PER_POINT, "peak_source": peak_kind},
         "cpu_baseline": cpu,
         "e2e": {"value": round(e2e_rate, 1), "unit": "Mpts/s", "h2d_bytes_per_step": 16 * e2e_n,
