@@ -46,33 +46,43 @@ struct DeviceErrors {
     int first_tid;
 };
 
-// Growable device array (explicit capacity, reallocated with a copy).
+// Stream-ordered scratch from a library-owned pool per device that keeps
+// freed memory cached (the default pool returns it to the driver at every
+// synchronisation).  Allocation and release are ordered on the given stream,
+// so builds on different streams never synchronise the whole device.
+gahhg_status pool_alloc(void** p, size_t bytes, int device, cudaStream_t s);
+
+// Growable device array (explicit capacity, reallocated with a copy), backed
+// by the pool and ordered on the stream it was last reserved on.
 template <class T> struct DevArray {
     T* ptr = nullptr;
     size_t cap = 0;
+    cudaStream_t stream = nullptr;
     gahhg_status reserve(size_t n, cudaStream_t s, bool keep = true)
     {
         if (n <= cap) return GAHHG_OK;
         size_t ncap = cap ? cap : 1024;
         while (ncap < n) ncap *= 2;
+        int dev = 0;
+        cudaGetDevice(&dev);
         T* np = nullptr;
-        if (cudaMalloc(&np, ncap * sizeof(T)) != cudaSuccess) {
+        if (pool_alloc((void**)&np, ncap * sizeof(T), dev, s) != GAHHG_OK) {
             cudaGetLastError();
             set_error("device allocation of %zu bytes failed", ncap * sizeof(T));
             return GAHHG_ERR_NOMEM;
         }
         if (ptr) {
             if (keep) GAHHG_CUDA_TRY(cudaMemcpyAsync(np, ptr, cap * sizeof(T), cudaMemcpyDeviceToDevice, s));
-            GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
-            cudaFree(ptr);
+            cudaFreeAsync(ptr, s);
         }
         ptr = np;
         cap = ncap;
+        stream = s;
         return GAHHG_OK;
     }
     void release()
     {
-        if (ptr) cudaFree(ptr);
+        if (ptr) cudaFreeAsync(ptr, stream);
         ptr = nullptr;
         cap = 0;
     }
@@ -168,11 +178,6 @@ gahhg_status scan_exclusive(const int* d_in, int* d_out, int n, int* d_total, vo
                             cudaStream_t s);
 
 double now_seconds();
-
-// Stream-ordered scratch from a library-owned pool per device that keeps
-// freed memory cached (the default pool returns it to the driver at every
-// synchronisation, which made each query pay for a fresh mapping).
-gahhg_status pool_alloc(void** p, size_t bytes, int device, cudaStream_t s);
 
 }  // namespace gahhg
 

@@ -83,9 +83,14 @@ struct EdgeRec {
 };
 static_assert(sizeof(EdgeRec) == 40, "EdgeRec");
 
+// Level-0 grid over a lon/lat domain: W x H cells of dlon0 x dlat0 degrees
+// starting at (lon0, lat0).  full_lon: the domain spans all longitudes
+// (W * dlon0 = 360); to_north / to_south: it reaches the pole.
 struct Geo {
     int W, H;
-    double dlon0, dlat0;  // degrees at level 0
+    double lon0, lat0;
+    double dlon0, dlat0;
+    bool full_lon, to_north, to_south;
 };
 
 // Node geometry from (level, ix, iy): center (degrees, exact), cap radius.
@@ -107,8 +112,8 @@ __host__ __device__ inline NodeCap node_cap(const Geo& g, int lvl, long long ix,
     const double sc = level_scale(lvl);
     const double dlon = g.dlon0 / sc, dlat = g.dlat0 / sc;
     NodeCap c;
-    c.lonc = -180.0 + ((double)ix + 0.5) * dlon;
-    c.latc = -90.0 + ((double)iy + 0.5) * dlat;
+    c.lonc = g.lon0 + ((double)ix + 0.5) * dlon;
+    c.latc = g.lat0 + ((double)iy + 0.5) * dlat;
     gahhg_canon_vertex_xyz(c.lonc, c.latc, c.R);
     double sa, ca;
     gahhg_canon_sincos(gahhg_canon_rad(c.latc), &sa, &ca);
@@ -158,11 +163,11 @@ __host__ __device__ inline bool edge_hits_cap(const D3& A, const D3& B, const do
     return t1 >= -tol && t2 >= -tol;
 }
 
-__device__ inline double lat_of(const D3& p) { return asin(fmin(1.0, fmax(-1.0, p.y))) / RAD; }
-__device__ inline double lon_of(const D3& p) { return atan2(p.x, p.z) / RAD; }
+__host__ __device__ inline double lat_of(const D3& p) { return asin(fmin(1.0, fmax(-1.0, p.y))) / RAD; }
+__host__ __device__ inline double lon_of(const D3& p) { return atan2(p.x, p.z) / RAD; }
 
 // Latitude/longitude box (degrees) of arc AB; full_lon when it may cross a pole.
-__device__ inline void arc_box(const D3& A, const D3& B, double& la0, double& la1, double& lo0, double& lo1,
+__host__ __device__ inline void arc_box(const D3& A, const D3& B, double& la0, double& la1, double& lo0, double& lo1,
                                bool& full_lon)
 {
     double a = lat_of(A), b = lat_of(B);
@@ -231,36 +236,53 @@ __global__ void k_l0_pairs(BuildView v, int* cnt, const int* off, int* cursor, i
     const double rdeg = rmax / RAD + 1e-9;
     la0 -= rdeg;
     la1 += rdeg;
-    int iy0 = (int)floor((la0 + 90.0) / v.g.dlat0), iy1 = (int)floor((la1 + 90.0) / v.g.dlat0);
+    int iy0 = (int)floor((la0 - v.g.lat0) / v.g.dlat0), iy1 = (int)floor((la1 - v.g.lat0) / v.g.dlat0);
     iy0 = max(iy0, 0);
     iy1 = min(iy1, H - 1);
     const double maxlat = fmax(fabs(la0), fabs(la1));
-    long long ix0, ix1;
-    if (full || maxlat >= 89.0) {
-        ix0 = 0;
-        ix1 = W - 1;
-    } else {
+    // candidate columns: up to two ranges (the inflated lon interval may wrap
+    // past 360 degrees relative to the domain's west edge)
+    long long r0a = 0, r0b = W - 1, r1a = 1, r1b = 0;
+    bool all_cols = full || maxlat >= 89.0;
+    if (!all_cols) {
         const double c = cos(maxlat * RAD);
         const double wdeg = rdeg / c;
-        if (lo1 - lo0 + 2 * wdeg >= 360.0) {
-            ix0 = 0;
-            ix1 = W - 1;
+        const double len = (lo1 - lo0) + 2 * wdeg;
+        if (len >= 360.0) {
+            all_cols = true;
         } else {
-            ix0 = (long long)floor((lo0 - wdeg + 180.0) / v.g.dlon0);
-            ix1 = (long long)floor((lo1 + wdeg + 180.0) / v.g.dlon0);
+            double a = lo0 - wdeg - v.g.lon0;
+            a -= 360.0 * floor(a / 360.0);  // [0, 360)
+            r0a = (long long)floor(a / v.g.dlon0);
+            r0b = (long long)floor((a + len) / v.g.dlon0);
+            if (a + len >= 360.0) {
+                r1a = 0;
+                r1b = (long long)floor((a + len - 360.0) / v.g.dlon0);
+            }
         }
     }
+    if (all_cols) {
+        r0a = 0;
+        r0b = W - 1;
+        r1a = 1;
+        r1b = 0;
+    }
+    r0a = max(r0a, 0LL);
+    r0b = min(r0b, (long long)W - 1);
+    r1b = min(r1b, (long long)W - 1);
     for (int iy = iy0; iy <= iy1; iy++) {
-        for (long long xx = ix0; xx <= ix1; xx++) {
-            const int ix = (int)(((xx % W) + W) % W);
+        for (int range = 0; range < 2; range++) {
+            const long long xa = range ? r1a : r0a, xb = range ? r1b : r0b;
+            for (long long ix = xa; ix <= xb; ix++) {
             const NodeCap c = node_cap(v.g, 0, ix, iy);
             if (!edge_hits_cap(A, B, c.R, c.r)) continue;
-            const int node = iy * W + ix;
+            const int node = iy * W + (int)ix;
             if (PASS == 0) {
                 atomicAdd(&cnt[node], 1);
             } else {
                 const int pos = off[node] + atomicAdd(&cursor[node], 1);
                 list[pos] = t;
+            }
             }
         }
     }
@@ -551,12 +573,12 @@ __global__ void k_summary(const uint32_t* nodes, int W, int H, int cshift, uint3
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncoarse) return;
-    const int CW = W >> cshift;
-    const int cx = c % CW, cy = c / CW;
     const int f = 1 << cshift;
+    const int CW = (W + f - 1) >> cshift;
+    const int cx = c % CW, cy = c / CW;
     uint32_t code = 0xFFu;
-    for (int y = cy * f; y < (cy + 1) * f && code != 2u; y++)
-        for (int x = cx * f; x < (cx + 1) * f; x++) {
+    for (int y = cy * f; y < min((cy + 1) * f, H) && code != 2u; y++)
+        for (int x = cx * f; x < min((cx + 1) * f, W); x++) {
             const uint32_t w = nodes[(size_t)y * W + x];
             const uint32_t v = ((w & KIND_MASK) == KIND_PURE) ? (w & 3u) - 1u : 2u;  // 0 out, 1 in, 2 mixed
             if (code == 0xFFu) code = v;
@@ -564,6 +586,21 @@ __global__ void k_summary(const uint32_t* nodes, int W, int H, int cshift, uint3
             if (code == 2u) break;
         }
     atomicOr(&summary[c >> 4], code << ((c & 15) * 2));
+}
+
+// Label of the region outside the domain: parity of the arc from a border
+// cell's center to the center of the virtual cell just beyond the border
+// (both inside the border cell's cap), against that cell's edges.
+__global__ void k_outside_label(BuildView v, int ix, int iy, int ox, int oy, const int* cnt, const int* off,
+                                const int* list, const uint8_t* label, uint8_t* out, int* bad)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const int p = iy * v.g.W + ix;
+    NodeCap a = node_cap(v.g, 0, ix, iy);
+    nudge_center(v.g, 0, a, v.pv, v.pe, list + off[p], cnt[p]);
+    const NodeCap b = node_cap(v.g, 0, ox, oy);
+    const int par = arc_parity_lists(v.pv, v.pe, a.R, b.R, list + off[p], cnt[p], nullptr, 0, bad);
+    *out = (uint8_t)(par ? 3 - label[p] : label[p]);
 }
 
 __global__ void k_shift_leaf_words(uint32_t* nodes, int start, int nn, int add)
@@ -578,7 +615,12 @@ __global__ void k_shift_leaf_words(uint32_t* nodes, int start, int nn, int add)
 
 struct QueryView {
     int W, H;
-    double su;  // W / 360 (= H / 180)
+    double Wd, Hd;            // W, H as doubles
+    double su_lon, su_lat;    // level-0 cells per degree
+    double u0, v0;            // column = lon * su_lon + u0; row = (lat + 90) * su_lat + v0
+    double U360;              // cells per 360 degrees of longitude
+    int full_lon, to_north, to_south;
+    uint32_t outside;         // label outside the domain (pure node word)
     int cshift;               // coarse cell = (1 << cshift) x (1 << cshift) top cells
     int CW;                   // coarse columns
     int swords;               // 32-bit words of the coarse summary
@@ -691,24 +733,44 @@ __device__ uint8_t leaf_label(const QueryView& Q, uint32_t leaf, PointCtx& P, bo
     return (uint8_t)(par ? 3 - L.label : L.label);
 }
 
-// Top-level index of a point given its (range-reduced) degrees.
+// Level-0 cell of a point from its longitude and FakeLL latitude + 90
+// (`laf`); false when the point lies outside the domain.
 struct Loc {
     int ix, iy;
     double fu, fv;
 };
 
-__device__ __forceinline__ Loc top_locate(const QueryView& Q, double lo, double la)
+// Level-0 cell of a point from its longitude and FakeLL latitude + 90
+// (`laf`); false when the point lies outside the domain.  Inside the domain
+// this costs two multiply-adds, two conversions and two unsigned compares;
+// points beyond a non-polar latitude edge are rejected with one more compare.
+__device__ __forceinline__ bool domain_locate(const QueryView& Q, double lo, double laf, Loc& L)
 {
-    double u = (lo + 180.0) * Q.su;
-    if (u >= Q.W) u -= Q.W;
-    if (u < 0) u += Q.W;
-    const double v = (la + 90.0) * Q.su;
-    Loc L;
-    L.ix = min(max((int)u, 0), Q.W - 1);
-    L.iy = min(max((int)v, 0), Q.H - 1);
-    L.fu = u - L.ix;
-    L.fv = v - L.iy;
-    return L;
+    double u = fma(lo, Q.su_lon, Q.u0), v = fma(laf, Q.su_lat, Q.v0);
+    int ix = __double2int_rd(u), iy = __double2int_rd(v);
+    if ((unsigned)iy >= (unsigned)Q.H) {
+        if (iy < 0 ? !Q.to_south : !Q.to_north) return false;
+        // a domain that reaches the pole keeps the pole in its first/last row
+        const bool below = iy < 0;
+        iy = below ? 0 : Q.H - 1;
+        v = below ? 0.0 : fmin(v, Q.Hd);
+    }
+    if ((unsigned)ix >= (unsigned)Q.W) {
+        if (u < 0.0) u += Q.U360;
+        if (u < 0.0) u += Q.U360;
+        if (u >= Q.U360) u -= Q.U360;
+        if (u >= Q.U360) u -= Q.U360;
+        ix = __double2int_rd(u);
+        if ((unsigned)ix >= (unsigned)Q.W) {
+            if (!Q.full_lon) return false;
+            ix = ix < 0 ? 0 : Q.W - 1;
+        }
+    }
+    L.ix = ix;
+    L.iy = iy;
+    L.fu = u - ix;
+    L.fv = v - iy;
+    return true;
 }
 
 __device__ __forceinline__ uint32_t descend(const QueryView& Q, uint32_t w, double fu, double fv)
@@ -754,8 +816,7 @@ __global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, 
     for (int k = threadIdx.x; k < Q.swords; k += TPB) s_sum[k] = __ldg(Q.summary + k);
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    const double su = Q.su, u0 = 180.0 * Q.su, Wd = (double)Q.W;
-    const int wmax = Q.W - 1, hmax = Q.H - 1, cs = Q.cshift, cw = Q.CW;
+    const int cs = Q.cshift, cw = Q.CW;
     int inside = 0;
     constexpr int TILE = TPB * LOC_UNROLL;
     for (int base = blockIdx.x * TILE; base < n; base += gridDim.x * TILE) {
@@ -778,21 +839,21 @@ __global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, 
             push[k] = false;
             if (full || i < n) {
                 if (laf >= 0.0 && laf <= 180.0 && fabs(lo) <= 540.0) {
-                    double u = fma(lo, su, u0);
-                    if (u >= Wd) u -= Wd;
-                    else if (u < 0.0) u += Wd;
-                    const double v = laf * su;
-                    const int ix = min((int)u, wmax), iy = min((int)v, hmax);
-                    const int c = (iy >> cs) * cw + (ix >> cs);
-                    const uint32_t code = (s_sum[c >> 4] >> ((c & 15) << 1)) & 3u;
-                    if (code < 2u) {
-                        lab[k] = (uint8_t)(code + 1u);  // coarse cell without edges: most points end here
+                    Loc L;
+                    if (!domain_locate(Q, lo, laf, L)) {
+                        lab[k] = (uint8_t)Q.outside;
                     } else {
-                        const uint32_t d = descend(Q, __ldg(Q.nodes + (size_t)iy * Q.W + ix), u - ix, v - iy);
-                        if ((d & KIND_MASK) == KIND_PURE)
-                            lab[k] = (uint8_t)(d & 3u);
-                        else
-                            push[k] = true;
+                        const int c = (L.iy >> cs) * cw + (L.ix >> cs);
+                        const uint32_t code = (s_sum[c >> 4] >> ((c & 15) << 1)) & 3u;
+                        if (code < 2u) {
+                            lab[k] = (uint8_t)(code + 1u);  // coarse cell without edges: most points end here
+                        } else {
+                            const uint32_t d = descend(Q, __ldg(Q.nodes + (size_t)L.iy * Q.W + L.ix), L.fu, L.fv);
+                            if ((d & KIND_MASK) == KIND_PURE)
+                                lab[k] = (uint8_t)(d & 3u);
+                            else
+                                push[k] = true;
+                        }
                     }
                 } else {
                     // unusual coordinates go to pass 2; non-finite input stays undefined
@@ -845,10 +906,16 @@ __global__ void __launch_bounds__(TPB) k_leaf(const double2* __restrict__ ll, ui
             la = asin(fmin(1.0, fmax(-1.0, P.q[1]))) / RAD;
             lo = atan2(P.q[0], P.q[2]) / RAD;
         }
-        const Loc L = top_locate(Q, lo, la);
-        P.lon_r = fmin(180.0, fmax(-180.0, (L.ix + L.fu) / Q.su - 180.0));
+        Loc L;
+        double lr = lo;
+        if (lr > 180.0) lr -= 360.0;
+        if (lr > 180.0) lr -= 360.0;
+        if (lr < -180.0) lr += 360.0;
+        if (lr < -180.0) lr += 360.0;
+        P.lon_r = lr;
         P.lat_r = la;
-        const uint32_t w = descend(Q, __ldg(Q.nodes + (size_t)L.iy * Q.W + L.ix), L.fu, L.fv);
+        const bool in = domain_locate(Q, lo, la + 90.0, L);
+        const uint32_t w = in ? descend(Q, __ldg(Q.nodes + (size_t)L.iy * Q.W + L.ix), L.fu, L.fv) : Q.outside;
         uint8_t lab;
         if ((w & KIND_MASK) == KIND_PURE) {
             lab = (uint8_t)(w & 3u);
@@ -874,6 +941,7 @@ struct Lattice {
     DevArray<EdgeRec> recs;
     DevArray<uint32_t> summary;
     int cshift = 0, swords = 0;
+    int outside_label = 0;
     long long nnodes = 0, nleaves = 0, nrecs = 0;
     int origin_label = 0;
     double x_in[3]{};
@@ -997,6 +1065,140 @@ int nearest_hub(const double* q)
 
 }  // namespace
 
+
+// Longitude/latitude domain of the polygon's edges, padded by one cell, with
+// cells of near-equal size in degrees whose count is about `target`.  A
+// domain that reaches within a degree of a pole takes in the whole polar cap
+// (all longitudes), so that points outside it are never close to an edge.
+gahhg_status compute_domain(const Polygon* P, long long target, Geo* G)
+{
+    double latmin = 90.0, latmax = -90.0;
+    bool full = false;
+    std::vector<uint8_t> bins(3600, 0);  // 0.1-degree longitude bins touched by some arc
+    for (int e = 0; e < P->pv_num; e++) {
+        const int ia = P->pe[2 * e], ib = P->pe[2 * e + 1];
+        const D3 a = P->pv[ia], b = P->pv[ib];
+        if (a.x == b.x && a.y == b.y && a.z == b.z) continue;
+        double la0, la1, lo0, lo1;
+        bool fl = false;
+        const double dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+        if (dx * dx + dy * dy + dz * dz > 1e-4) {
+            arc_box(a, b, la0, la1, lo0, lo1, fl);  // long edge: its great circle may bulge
+        } else {
+            // short edge: the input degrees of its ends (the bulge is below 1e-4 deg, far
+            // inside the one-cell padding)
+            double oa = P->lonlat[2 * ia], ob = P->lonlat[2 * ib];
+            const double ta = P->lonlat[2 * ia + 1], tb = P->lonlat[2 * ib + 1];
+            la0 = std::min(ta, tb) - 1e-4;
+            la1 = std::max(ta, tb) + 1e-4;
+            oa -= 360.0 * floor((oa + 180.0) / 360.0);
+            ob -= 360.0 * floor((ob + 180.0) / 360.0);
+            if (oa > ob) std::swap(oa, ob);
+            if (ob - oa <= 180.0) {
+                lo0 = oa;
+                lo1 = ob;
+            } else {
+                lo0 = ob;
+                lo1 = oa + 360.0;
+            }
+            if (fabs(ta) > 89.9 || fabs(tb) > 89.9) fl = true;
+        }
+        latmin = std::min(latmin, la0);
+        latmax = std::max(latmax, la1);
+        if (fl) {
+            full = true;
+            continue;
+        }
+        const long long b0 = (long long)floor((lo0 + 180.0) * 10.0) - 1, b1 = (long long)floor((lo1 + 180.0) * 10.0) + 1;
+        for (long long k = b0; k <= b1; k++) bins[((k % 3600) + 3600) % 3600] = 1;
+    }
+    if (latmin > latmax) {
+        set_error("exact index: polygon has no edges of positive length");
+        return GAHHG_ERR_ARG;
+    }
+    // largest circular run of untouched bins = the longitude gap left outside
+    int gstart = 0, glen = 0;
+    if (!full) {
+        int best = 0, bs = 0;
+        for (int st = 0; st < 3600; st++) {
+            if (bins[st] || bins[(st + 3599) % 3600] == 0) continue;  // runs start after a touched bin
+            int len = 0;
+            while (len < 3600 && !bins[(st + len) % 3600]) len++;
+            if (len > best) {
+                best = len;
+                bs = st;
+            }
+        }
+        gstart = bs;
+        glen = best;
+        if (glen == 0) full = true;
+    }
+    double lon0 = -180.0, lon_span = 360.0;
+    if (!full) {
+        lon0 = ((gstart + glen) % 3600) * 0.1 - 180.0;
+        lon_span = (3600 - glen) * 0.1;
+    }
+    double lat0 = latmin, lat_span = std::max(latmax - latmin, 1e-6);
+    // cell size (degrees) for about `target` cells, with the padding included
+    double cell = sqrt(std::max(lon_span, 1e-6) * lat_span / (double)std::max(target, 1LL));
+    bool full_lon = full, north = false, south = false;
+    for (int it = 0; it < 3; it++) {
+        const double pad = cell * 1.5;
+        double la = latmin - pad, lb = latmax + pad;
+        north = lb >= 89.0;
+        south = la <= -89.0;
+        bool fl = full || north || south;
+        double lspan = 360.0, l0 = -180.0;
+        if (!fl) {
+            const double maxabs = std::min(89.0, std::max(fabs(la), fabs(lb)));
+            const double padlon = pad / cos(maxabs * RAD);
+            lspan = lon_span + 2.0 * padlon;
+            l0 = lon0 - padlon;
+            if (lspan >= 359.0) fl = true;
+        }
+        if (fl) {
+            lspan = 360.0;
+            l0 = -180.0;
+            if (!north && !south) {
+                if (latmin + latmax >= 0.0)
+                    north = true;
+                else
+                    south = true;
+            }
+        }
+        if (north) lb = 90.0;
+        if (south) la = -90.0;
+        la = std::max(la, -90.0);
+        lb = std::min(lb, 90.0);
+        full_lon = fl;
+        G->lon0 = l0;
+        G->lat0 = la;
+        lon_span = fl ? 360.0 : lon_span;
+        const double ncell = sqrt(lspan * (lb - la) / (double)std::max(target, 1LL));
+        if (it < 2 && fabs(ncell - cell) > 1e-3 * cell) {
+            cell = ncell;
+            if (!fl) lon0 = lon0;  // unchanged: padding recomputed from the unpadded span
+            continue;
+        }
+        long long W = std::max(1LL, (long long)ceil(lspan / cell)), H = std::max(1LL, (long long)ceil((lb - la) / cell));
+        W = std::min(W, 16384LL);
+        H = std::min(H, 16384LL);
+        if ((long long)W * H >= (long long)INDEX_MASK / 4) {
+            set_error("exact index: top level too large");
+            return GAHHG_ERR_CAPACITY;
+        }
+        G->W = (int)W;
+        G->H = (int)H;
+        G->dlon0 = lspan / (double)W;
+        G->dlat0 = (lb - la) / (double)H;
+        G->full_lon = full_lon;
+        G->to_north = north;
+        G->to_south = south;
+        break;
+    }
+    return GAHHG_OK;
+}
+
 gahhg_status lattice_build(Grid* g)
 {
     cudaStream_t s = g->stream;
@@ -1005,38 +1207,32 @@ gahhg_status lattice_build(Grid* g)
     Lattice* L = new Lattice();
     g->lattice = L;
 
-    int W = 64;
-    if (g->opts.lattice_top > 0) {
-        W = g->opts.lattice_top;
-    } else {
-        while (W < 4096 && (long long)W * W / 2 < 8LL * n) W *= 2;
-    }
-    if (W < 8 || W > 16384 || (W & (W - 1))) {
-        set_error("lattice_top must be a power of two in [8, 16384]");
-        return GAHHG_ERR_ARG;
-    }
+    long long target = g->opts.lattice_top > 0 ? (long long)g->opts.lattice_top
+                                                : std::min<long long>(std::max<long long>(8LL * n, 1024), 8LL << 20);
+    GAHHG_TRY(compute_domain(P, target, &L->geo));
+    const int W = L->geo.W, H = L->geo.H;
     L->K = g->opts.lattice_leaf > 0 ? g->opts.lattice_leaf : 8;
     L->maxlev = 9;
-    L->geo.W = W;
-    L->geo.H = W / 2;
-    L->geo.dlon0 = 360.0 / W;
-    L->geo.dlat0 = 180.0 / (W / 2);
     BuildView bv{L->geo, P->d_pv, P->d_pe, n};
 
-    // exact label of the first level-0 center, through the hubs
+    // exact label of the first level-0 center: from a point just left of an
+    // outer edge, through the hubs whenever an arc would exceed ~84 degrees
     GAHHG_TRY(reference_point(g, L->x_in));
     int label = CELL_IN;
     {
-        const int h0 = nearest_hub(L->x_in);
-        const int south = 3;  // hub near -y
+        const NodeCap c00 = node_cap(L->geo, 0, 0, 0);
         std::vector<const double*> path;
         path.push_back(L->x_in);
-        path.push_back(HUBS[h0]);
-        if (h0 == 2) path.push_back(HUBS[0]);  // +y -> +x -> -y
-        if (h0 != south) path.push_back(HUBS[south]);
-        NodeCap c00 = node_cap(L->geo, 0, 0, 0);
-        // the origin center gets nudged like every other center (its list is
-        // not known yet; a vertex exactly at the center is rejected below)
+        auto unit_dot = [](const double* a, const double* b) {
+            return (a[0] * b[0] + a[1] * b[1] + a[2] * b[2]) /
+                   sqrt((a[0] * a[0] + a[1] * a[1] + a[2] * a[2]) * (b[0] * b[0] + b[1] * b[1] + b[2] * b[2]));
+        };
+        if (unit_dot(L->x_in, c00.R) < 0.1) {
+            const int ha = nearest_hub(L->x_in), hb = nearest_hub(c00.R);
+            path.push_back(HUBS[ha]);
+            if ((ha ^ 1) == hb) path.push_back(HUBS[(ha + 2) % 6]);  // opposite hubs: go round
+            if (hb != ha) path.push_back(HUBS[hb]);
+        }
         path.push_back(c00.R);
         for (size_t k = 0; k + 1 < path.size(); k++) {
             int par;
@@ -1053,7 +1249,7 @@ gahhg_status lattice_build(Grid* g)
     std::vector<LevelBuf> lv(1);
     // ---------------- level 0 ----------------
     LevelBuf& l0 = lv[0];
-    l0.nn = W * (W / 2);
+    l0.nn = W * H;
     l0.gstart = 0;
     GAHHG_TRY(l0.cnt.reserve(l0.nn, s, false));
     GAHHG_TRY(l0.off.reserve(l0.nn, s, false));
@@ -1079,15 +1275,40 @@ gahhg_status lattice_build(Grid* g)
     GAHHG_CUDA_TRY(cudaMemsetAsync(d_bad, 0, 4 * sizeof(int), s));
     {
         DevArray<uint8_t> vpar, hpar;
-        GAHHG_TRY(vpar.reserve((size_t)W * (W / 2 - 1) + 1, s, false));
+        GAHHG_TRY(vpar.reserve((size_t)W * (H > 1 ? H - 1 : 1) + 1, s, false));
         GAHHG_TRY(hpar.reserve(W, s, false));
         GAHHG_TRY(l0.label.reserve(l0.nn, s, false));
-        const long long nthreads = (long long)W * (W / 2 - 1) + W - 1;
+        const long long nthreads = (long long)W * (H - 1) + W - 1;
         k_l0_neighbour_parity<<<blocks_for(nthreads), TPB, 0, s>>>(bv, l0.cnt.ptr, l0.off.ptr, l0.list.ptr, vpar.ptr,
                                                                    hpar.ptr, d_bad);
         int* d_origin = g->d_counts + 12;
         GAHHG_CUDA_TRY(cudaMemcpyAsync(d_origin, &L->origin_label, sizeof(int), cudaMemcpyHostToDevice, s));
-        k_l0_labels<<<blocks_for(W), TPB, 0, s>>>(W, W / 2, vpar.ptr, hpar.ptr, d_origin, l0.label.ptr);
+        k_l0_labels<<<blocks_for(W), TPB, 0, s>>>(W, H, vpar.ptr, hpar.ptr, d_origin, l0.label.ptr);
+        // label of the region outside the domain, from the nearest border cell
+        const Geo& G0 = L->geo;
+        int ix = 0, iy = 0, ox = 0, oy = 0;
+        bool has_outside = true;
+        if (!G0.full_lon) {
+            ox = -1;
+        } else if (!G0.to_south) {
+            oy = -1;
+        } else if (!G0.to_north) {
+            iy = H - 1;
+            oy = H;
+        } else {
+            has_outside = false;
+        }
+        uint8_t* d_out = reinterpret_cast<uint8_t*>(g->d_counts + 13);
+        if (has_outside) {
+            k_outside_label<<<1, 1, 0, s>>>(bv, ix, iy, ox, oy, l0.cnt.ptr, l0.off.ptr, l0.list.ptr, l0.label.ptr,
+                                            d_out, d_bad);
+            uint8_t ol = 0;
+            GAHHG_CUDA_TRY(cudaMemcpyAsync(&ol, d_out, 1, cudaMemcpyDeviceToHost, s));
+            GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+            L->outside_label = ol;
+        } else {
+            L->outside_label = CELL_UNDEFINED;
+        }
         GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
         vpar.release();
         hpar.release();
@@ -1211,13 +1432,14 @@ gahhg_status lattice_build(Grid* g)
     {
         // coarse summary: at most 256 x 128 cells (8 KB), staged in shared memory by the query
         int cs = 0;
-        while ((W >> cs) > 256) cs++;
-        const int CW = W >> cs, CH = (W / 2) >> cs;
+        auto blocks = [&](int c) { return (long long)((W + (1 << c) - 1) >> c) * ((H + (1 << c) - 1) >> c); };
+        while (blocks(cs) > 65536) cs++;
+        const int CW = (W + (1 << cs) - 1) >> cs, CH = (H + (1 << cs) - 1) >> cs;
         L->cshift = cs;
         L->swords = (CW * CH + 15) / 16;
         GAHHG_TRY(L->summary.reserve(L->swords, s, false));
         GAHHG_CUDA_TRY(cudaMemsetAsync(L->summary.ptr, 0, sizeof(uint32_t) * L->swords, s));
-        k_summary<<<blocks_for(CW * CH), TPB, 0, s>>>(L->nodes.ptr, W, W / 2, cs, L->summary.ptr, CW * CH);
+        k_summary<<<blocks_for(CW * CH), TPB, 0, s>>>(L->nodes.ptr, W, H, cs, L->summary.ptr, CW * CH);
     }
     int bad[4];
     GAHHG_CUDA_TRY(cudaMemcpyAsync(bad, d_bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
@@ -1242,27 +1464,43 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
                                 int precision, cudaStream_t s, uint64_t* d_counters, uint32_t* queue,
                                 unsigned int* qcount, long long chunk, int device);
 
-// Points per pass; the pass-2 queue holds one 4-byte index per point.
-constexpr long long QUERY_CHUNK = 1LL << 27;
-
-gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels, int precision,
-                           cudaStream_t s, uint64_t* d_counters)
+QueryView make_view(const Grid* g)
 {
-    Lattice* L = g->lattice;
-    if (n == 0) return GAHHG_OK;
+    const Lattice* L = g->lattice;
     QueryView Q;
     Q.W = L->geo.W;
     Q.H = L->geo.H;
-    Q.su = (double)L->geo.W / 360.0;
+    Q.Wd = (double)L->geo.W;
+    Q.Hd = (double)L->geo.H;
+    Q.su_lon = 1.0 / L->geo.dlon0;
+    Q.su_lat = 1.0 / L->geo.dlat0;
+    Q.u0 = -L->geo.lon0 * Q.su_lon;
+    Q.v0 = -(L->geo.lat0 + 90.0) * Q.su_lat;
+    Q.U360 = 360.0 * Q.su_lon;
+    Q.full_lon = L->geo.full_lon;
+    Q.to_north = L->geo.to_north;
+    Q.to_south = L->geo.to_south;
+    Q.outside = KIND_PURE | (uint32_t)L->outside_label;
     Q.nodes = L->nodes.ptr;
     Q.leaves = L->leaves.ptr;
     Q.recs = L->recs.ptr;
     Q.pv = g->poly->d_pv;
     Q.pe = g->poly->d_pe;
     Q.cshift = L->cshift;
-    Q.CW = L->geo.W >> L->cshift;
+    Q.CW = (L->geo.W + (1 << L->cshift) - 1) >> L->cshift;
     Q.swords = L->swords;
     Q.summary = L->summary.ptr;
+    return Q;
+}
+
+// Points per pass; the pass-2 queue holds one 4-byte index per point.
+constexpr long long QUERY_CHUNK = 1LL << 27;
+
+gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels, int precision,
+                           cudaStream_t s, uint64_t* d_counters)
+{
+    if (n == 0) return GAHHG_OK;
+    const QueryView Q = make_view(g);
     const long long chunk = std::min<long long>((long long)n, QUERY_CHUNK);
     uint32_t* queue = nullptr;
     GAHHG_TRY(pool_alloc((void**)&queue, sizeof(uint32_t) * (chunk + 64), g->device, s));
@@ -1348,20 +1586,7 @@ gahhg_status lattice_query_noalloc(Grid* g, const double* d_lonlat, size_t n, ui
     uint32_t* queue = nullptr;
     GAHHG_TRY(noalloc_queue_address(g->device, &queue));
     if (n == 0) return GAHHG_OK;
-    Lattice* L = g->lattice;
-    QueryView Q;
-    Q.W = L->geo.W;
-    Q.H = L->geo.H;
-    Q.su = (double)L->geo.W / 360.0;
-    Q.nodes = L->nodes.ptr;
-    Q.leaves = L->leaves.ptr;
-    Q.recs = L->recs.ptr;
-    Q.pv = g->poly->d_pv;
-    Q.pe = g->poly->d_pe;
-    Q.cshift = L->cshift;
-    Q.CW = L->geo.W >> L->cshift;
-    Q.swords = L->swords;
-    Q.summary = L->summary.ptr;
+    const QueryView Q = make_view(g);
     // the queue count lives after the queue; lattice_query_with zeroes it before each pass
     unsigned int* qcount = (unsigned int*)(queue + NOALLOC_MAX_POINTS + 32);
     return lattice_query_with(Q, d_lonlat, (long long)n, d_labels, precision, s, nullptr, queue, qcount,

@@ -61,7 +61,7 @@ typedef struct {
     int max_depth;      /* GPISPParam::maxDepth (source/GPISPParam.h:67), default 15 */
     int auto_depth;     /* GPISPParam::autoDepth (:68), default 1 */
     int semantics;      /* gahhg_semantics; GAHHG_SEMANTICS_EXACT builds both indexes */
-    int lattice_top;    /* exact index: top lattice columns (0 = automatic) */
+    int lattice_top;    /* exact index: target number of top-level cells (0 = automatic, 8 per edge) */
     int lattice_leaf;   /* exact index: max edges per leaf before refining (0 = automatic) */
     int device;         /* CUDA device ordinal */
     int verbose;        /* print the reference's progress lines */
