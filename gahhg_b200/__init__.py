@@ -148,6 +148,51 @@ class Grid:
             self._h = None
 
 
+class Batch:
+    """Exact indexes of many polygons, queried together (see gahhg_batch_* in
+    include/gahhg.h)."""
+
+    def __init__(self, polygons, device=0, top_cells=None, leaf_edges=None, workers=0, chunk_points=None):
+        L = _lib.lib()
+        o = _lib.BuildOpts()
+        L.gahhg_build_opts_init(ctypes.byref(o))
+        o.device = device
+        self.polygons = list(polygons)
+        arr = (ctypes.c_void_p * len(self.polygons))(*[p._h.value for p in self.polygons])
+        tc = np.ascontiguousarray(top_cells, dtype=np.int32) if top_cells is not None else None
+        le = np.ascontiguousarray(leaf_edges, dtype=np.int32) if leaf_edges is not None else None
+        h = ctypes.c_void_p()
+        check(L.gahhg_batch_build(arr, len(self.polygons), ctypes.byref(o), _lib.ptr(tc), _lib.ptr(le), workers,
+                                  ctypes.byref(h)))
+        self._h = h
+        if chunk_points:
+            check(L.gahhg_batch_set_chunk(h, chunk_points))
+
+    def query_device(self, d_lonlat, offsets, d_labels, precision=QUERY_AUTO, stream=0, sync=False, graph=False):
+        """d_lonlat / d_labels: device pointers; offsets: host int64 array (count+1)."""
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        assert len(off) == len(self.polygons) + 1
+        self._off = off  # keep alive for the call
+        L = _lib.lib()
+        if graph:
+            check(L.gahhg_batch_query_graph(self._h, ctypes.c_void_p(d_lonlat), _lib.ptr(off),
+                                            ctypes.c_void_p(d_labels), precision, ctypes.c_void_p(stream)))
+        else:
+            check(L.gahhg_batch_query_device(self._h, ctypes.c_void_p(d_lonlat), _lib.ptr(off),
+                                             ctypes.c_void_p(d_labels), precision, ctypes.c_void_p(stream),
+                                             1 if sync else 0))
+
+    def stats(self):
+        s = _lib.BatchStats()
+        check(_lib.lib().gahhg_batch_stats_get(self._h, ctypes.byref(s)))
+        return s.as_dict()
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _lib.lib().gahhg_batch_free(self._h)
+            self._h = None
+
+
 def write_result(path, labels):
     labels = np.ascontiguousarray(labels, dtype=np.uint8)
     check(_lib.lib().gahhg_result_write(str(path).encode(), _lib.ptr(labels), len(labels)))

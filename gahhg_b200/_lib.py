@@ -61,6 +61,16 @@ class Stats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BatchStats(ctypes.Structure):
+    _fields_ = [("polygons", ctypes.c_int), ("workers", ctypes.c_int), ("edges", ctypes.c_longlong),
+                ("lattice_bytes", ctypes.c_longlong), ("build_s", ctypes.c_double), ("query_s", ctypes.c_double),
+                ("query_points", ctypes.c_longlong), ("boundary_points", ctypes.c_longlong),
+                ("esc_fp64", ctypes.c_longlong), ("esc_exact", ctypes.c_longlong), ("in_count", ctypes.c_longlong)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 # name: (restype, argtypes)
 _P = ctypes.c_void_p
 _SIGS = {
@@ -90,6 +100,14 @@ _SIGS = {
                                            ctypes.c_char_p, ctypes.c_int]),
     "gahhg_result_write": (ctypes.c_int, [ctypes.c_char_p, _P, ctypes.c_size_t]),
     "gahhg_grid0_export": (ctypes.c_int, [_P, _P, _P]),
+    "gahhg_batch_build": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(BuildOpts), _P, _P, ctypes.c_int,
+                                         ctypes.POINTER(_P)]),
+    "gahhg_batch_size": (ctypes.c_int, [_P]),
+    "gahhg_batch_set_chunk": (ctypes.c_int, [_P, ctypes.c_int]),
+    "gahhg_batch_query_device": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int, _P, ctypes.c_int]),
+    "gahhg_batch_query_graph": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int, _P]),
+    "gahhg_batch_stats_get": (ctypes.c_int, [_P, ctypes.POINTER(BatchStats)]),
+    "gahhg_batch_free": (None, [_P]),
 }
 
 _lib = None

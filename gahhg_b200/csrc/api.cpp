@@ -101,10 +101,12 @@ Grid::~Grid()
     if (d_err) cudaFree(d_err);
     if (d_counts) cudaFree(d_counts);
     if (h_counts) cudaFreeHost(h_counts);
-    scan_state_destroy(scan_state);
     free_query_layout(qlayout);
     lattice_free(lattice);
-    if (stream) cudaStreamDestroy(stream);
+    if (!borrowed) {
+        scan_state_destroy(scan_state);
+        if (stream) cudaStreamDestroy(stream);
+    }
 }
 
 static void fill_stats(Grid* g)

@@ -149,6 +149,7 @@ struct Grid {
 
     gahhg_stats stats{};
     bool classified = false;
+    bool borrowed = false;        // stream and scan state belong to a batch worker
 
     ~Grid();
 };
@@ -168,6 +169,17 @@ gahhg_status lattice_query_noalloc(Grid* g, const double* d_lonlat, size_t n, ui
                                    cudaStream_t s);
 long long lattice_noalloc_max_points();
 void lattice_free(Lattice* L);
+// batches (lattice.cu)
+size_t lattice_view_bytes();
+size_t batch_chunk_bytes();
+void lattice_view_write(const Grid* g, void* dst);
+long long lattice_summary_words(const Grid* g);
+void batch_make_chunks(const long long* offsets, int npoly, int chunk_points, std::vector<uint8_t>& out,
+                       int* nchunks);
+gahhg_status batch_query_launch(const void* d_views, int npoly, const long long* d_offsets, const void* d_chunks,
+                                int nchunks, const double* d_lonlat, uint8_t* d_labels, int precision,
+                                uint32_t* queue, unsigned int* counters, uint64_t* d_stats, cudaStream_t s,
+                                int device);
 size_t lattice_bytes(const Lattice* L);
 
 // scans (scan.cu)

@@ -807,25 +807,30 @@ constexpr uint8_t LABEL_PENDING = 0;
 // stream with an evict-first policy so the node table stays in L2.  The index
 // arithmetic need not match the canonical conversion bit for bit: every cap
 // carries a margin far above its rounding (see LOC_MARGIN).
+// Pass 1 over points [first, first + count) of one polygon, in tiles of
+// TPB * LOC_UNROLL points (tiles tile0, tile0 + tstride, ...): every point
+// whose cell has no edges gets its label; the others are queued (their index
+// `first + local`) for pass 2.  Lean on registers and instructions so that
+// many warps keep loads in flight; lon/lat and labels stream with an
+// evict-first policy so the node table stays in L2.  The index arithmetic
+// need not match the canonical conversion bit for bit: every cap carries a
+// margin far above its rounding (see LOC_MARGIN).
 template <bool STATS>
-__global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, int n, uint8_t* __restrict__ out,
-                                               QueryView Q, uint32_t* __restrict__ queue,
-                                               unsigned int* __restrict__ qcount, unsigned long long* ctr)
+__device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t* s_sum,
+                                             const double2* __restrict__ ll, uint8_t* __restrict__ out,
+                                             uint32_t* __restrict__ queue, unsigned int* __restrict__ qcount,
+                                             long long first, int count, int tile0, int tstride, int& inside)
 {
-    extern __shared__ uint32_t s_sum[];
-    for (int k = threadIdx.x; k < Q.swords; k += TPB) s_sum[k] = __ldg(Q.summary + k);
-    __syncthreads();
     const int lane = threadIdx.x & 31;
     const int cs = Q.cshift, cw = Q.CW;
-    int inside = 0;
     constexpr int TILE = TPB * LOC_UNROLL;
-    for (int base = blockIdx.x * TILE; base < n; base += gridDim.x * TILE) {
-        const bool full = base + TILE <= n;
+    for (int base = tile0 * TILE; base < count; base += tstride * TILE) {
+        const bool full = base + TILE <= count;
         double2 p[LOC_UNROLL];
 #pragma unroll
         for (int k = 0; k < LOC_UNROLL; k++) {
             const int i = base + k * TPB + threadIdx.x;
-            p[k] = (full || i < n) ? __ldcs(ll + i) : make_double2(0.0, 0.0);
+            p[k] = (full || i < count) ? __ldcs(ll + first + i) : make_double2(0.0, 0.0);
         }
         uint8_t lab[LOC_UNROLL];
         bool push[LOC_UNROLL];
@@ -837,7 +842,7 @@ __global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, 
             const double laf = p[k].y + 90.0;  // the reference's FakeLL latitude + 90
             lab[k] = LABEL_PENDING;
             push[k] = false;
-            if (full || i < n) {
+            if (full || i < count) {
                 if (laf >= 0.0 && laf <= 180.0 && fabs(lo) <= 540.0) {
                     Loc L;
                     if (!domain_locate(Q, lo, laf, L)) {
@@ -871,17 +876,60 @@ __global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, 
                 const int leader = __ffs(mask) - 1;
                 if (lane == leader) pos = atomicAdd(qcount, (unsigned int)__popc(mask));
                 pos = __shfl_sync(0xffffffffu, pos, leader);
-                if (push[k]) queue[pos + __popc(mask & ((1u << lane) - 1u))] = (uint32_t)(base + k * TPB + threadIdx.x);
+                if (push[k])
+                    queue[pos + __popc(mask & ((1u << lane) - 1u))] = (uint32_t)(first + base + k * TPB + threadIdx.x);
             }
         }
 #pragma unroll
         for (int k = 0; k < LOC_UNROLL; k++) {
             const int i = base + k * TPB + threadIdx.x;
-            if (full || i < n) __stcs(out + i, lab[k]);
+            if (full || i < count) __stcs(out + first + i, lab[k]);
             if (STATS) inside += lab[k] == CELL_IN;
         }
     }
+}
+
+template <bool STATS>
+__global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, int n, uint8_t* __restrict__ out,
+                                               QueryView Q, uint32_t* __restrict__ queue,
+                                               unsigned int* __restrict__ qcount, unsigned long long* ctr)
+{
+    extern __shared__ uint32_t s_sum[];
+    for (int k = threadIdx.x; k < Q.swords; k += TPB) s_sum[k] = __ldg(Q.summary + k);
+    __syncthreads();
+    int inside = 0;
+    locate_range<STATS>(Q, s_sum, ll, out, queue, qcount, 0, n, blockIdx.x, gridDim.x, inside);
     if (STATS && ctr) count_inside(inside, ctr + 3);
+}
+
+// Pass 2 for one queued point.
+template <bool FP32>
+__device__ __forceinline__ uint8_t leaf_point(const QueryView& Q, double2 p, unsigned long long* ctr)
+{
+    PointCtx P;
+    P.lat = gahhg_canon_query_lat(p.y);
+    P.lon = p.x;
+    P.have64 = false;
+    double lo = P.lon, la = P.lat;
+    if (!(fabs(lo) <= 540.0 && fabs(la) <= 90.0)) {
+        // unusual input: locate from the canonical XYZ itself
+        P.need64();
+        la = asin(fmin(1.0, fmax(-1.0, P.q[1]))) / RAD;
+        lo = atan2(P.q[0], P.q[2]) / RAD;
+    }
+    Loc L;
+    double lr = lo;
+    if (lr > 180.0) lr -= 360.0;
+    if (lr > 180.0) lr -= 360.0;
+    if (lr < -180.0) lr += 360.0;
+    if (lr < -180.0) lr += 360.0;
+    P.lon_r = lr;
+    P.lat_r = la;
+    const bool in = domain_locate(Q, lo, la + 90.0, L);
+    const uint32_t w = in ? descend(Q, __ldg(Q.nodes + (size_t)L.iy * Q.W + L.ix), L.fu, L.fv) : Q.outside;
+    if ((w & KIND_MASK) == KIND_PURE) return (uint8_t)(w & 3u);
+    if (ctr) atomicAdd(ctr + 2, 1ull);
+    return leaf_label(Q, w & INDEX_MASK, P, FP32, ctr);
 }
 
 // Pass 2: exact crossing tests for the queued points.
@@ -894,35 +942,73 @@ __global__ void __launch_bounds__(TPB) k_leaf(const double2* __restrict__ ll, ui
     int inside = 0;
     for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
         const uint32_t i = queue[t];
-        const double2 p = ll[i];
-        PointCtx P;
-        P.lat = gahhg_canon_query_lat(p.y);
-        P.lon = p.x;
-        P.have64 = false;
-        double lo = P.lon, la = P.lat;
-        if (!(fabs(lo) <= 540.0 && fabs(la) <= 90.0)) {
-            // unusual input: locate from the canonical XYZ itself
-            P.need64();
-            la = asin(fmin(1.0, fmax(-1.0, P.q[1]))) / RAD;
-            lo = atan2(P.q[0], P.q[2]) / RAD;
+        const uint8_t lab = leaf_point<FP32>(Q, ll[i], ctr);
+        out[i] = lab;
+        inside += lab == CELL_IN;
+    }
+    if (ctr) count_inside(inside, ctr + 3);
+}
+
+// ------------------------------------------------------------- batches --
+
+// A run of points of one polygon (points are stored polygon after polygon).
+struct BatchChunk {
+    int poly;
+    int count;
+    long long start;
+};
+
+constexpr int BATCH_SUMMARY_WORDS = 4096;  // 16 KB of shared memory
+
+// Pass 1 over a batch: a persistent grid takes chunks in order from an atomic
+// counter (polygons of very different sizes balance themselves), stages the
+// chunk's polygon summary in shared memory and runs the single-polygon tile
+// loop on it.
+template <bool STATS>
+__global__ void __launch_bounds__(TPB) k_batch_locate(const QueryView* __restrict__ views,
+                                                     const BatchChunk* __restrict__ chunks, int nchunks,
+                                                     unsigned int* next_chunk, const double2* __restrict__ ll,
+                                                     uint8_t* __restrict__ out, uint32_t* __restrict__ queue,
+                                                     unsigned int* __restrict__ qcount, unsigned long long* ctr)
+{
+    __shared__ uint32_t s_sum[BATCH_SUMMARY_WORDS];
+    __shared__ int s_chunk;
+    int inside = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_chunk = (int)atomicAdd(next_chunk, 1u);
+        __syncthreads();
+        const int ci = s_chunk;
+        if (ci >= nchunks) break;
+        const BatchChunk c = chunks[ci];
+        const QueryView Q = views[c.poly];
+        for (int k = threadIdx.x; k < Q.swords; k += TPB) s_sum[k] = __ldg(Q.summary + k);
+        __syncthreads();
+        locate_range<STATS>(Q, s_sum, ll, out, queue, qcount, c.start, c.count, 0, 1, inside);
+        __syncthreads();
+    }
+    if (STATS && ctr) count_inside(inside, ctr + 3);
+}
+
+// Pass 2 over a batch: the polygon of a queued point by binary search of the
+// per-polygon point offsets.
+template <bool FP32>
+__global__ void __launch_bounds__(TPB) k_batch_leaf(const QueryView* __restrict__ views,
+                                                   const long long* __restrict__ offsets, int npoly,
+                                                   const double2* __restrict__ ll, uint8_t* __restrict__ out,
+                                                   const uint32_t* __restrict__ queue,
+                                                   const unsigned int* __restrict__ qcount, unsigned long long* ctr)
+{
+    const unsigned int m = *qcount;
+    int inside = 0;
+    for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+        const uint32_t i = queue[t];
+        int lo = 0, hi = npoly;  // offsets[lo] <= i < offsets[hi]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (offsets[mid] <= (long long)i) lo = mid;
+            else hi = mid;
         }
-        Loc L;
-        double lr = lo;
-        if (lr > 180.0) lr -= 360.0;
-        if (lr > 180.0) lr -= 360.0;
-        if (lr < -180.0) lr += 360.0;
-        if (lr < -180.0) lr += 360.0;
-        P.lon_r = lr;
-        P.lat_r = la;
-        const bool in = domain_locate(Q, lo, la + 90.0, L);
-        const uint32_t w = in ? descend(Q, __ldg(Q.nodes + (size_t)L.iy * Q.W + L.ix), L.fu, L.fv) : Q.outside;
-        uint8_t lab;
-        if ((w & KIND_MASK) == KIND_PURE) {
-            lab = (uint8_t)(w & 3u);
-        } else {
-            if (ctr) atomicAdd(ctr + 2, 1ull);
-            lab = leaf_label(Q, w & INDEX_MASK, P, FP32, ctr);
-        }
+        const uint8_t lab = leaf_point<FP32>(views[lo], ll[i], ctr);
         out[i] = lab;
         inside += lab == CELL_IN;
     }
@@ -1591,6 +1677,67 @@ gahhg_status lattice_query_noalloc(Grid* g, const double* d_lonlat, size_t n, ui
     unsigned int* qcount = (unsigned int*)(queue + NOALLOC_MAX_POINTS + 32);
     return lattice_query_with(Q, d_lonlat, (long long)n, d_labels, precision, s, nullptr, queue, qcount,
                               NOALLOC_MAX_POINTS, g->device);
+}
+
+// ------------------------------------------------------- batch launcher --
+
+size_t lattice_view_bytes() { return sizeof(QueryView); }
+size_t batch_chunk_bytes() { return sizeof(BatchChunk); }
+
+void lattice_view_write(const Grid* g, void* dst)
+{
+    const QueryView q = make_view(g);
+    memcpy(dst, &q, sizeof(q));
+}
+
+long long lattice_summary_words(const Grid* g) { return g->lattice ? g->lattice->swords : 0; }
+
+// Chunks of at most `chunk_points` points, polygon after polygon.
+void batch_make_chunks(const long long* offsets, int npoly, int chunk_points, std::vector<uint8_t>& out, int* nchunks)
+{
+    std::vector<BatchChunk> v;
+    for (int p = 0; p < npoly; p++)
+        for (long long a = offsets[p]; a < offsets[p + 1]; a += chunk_points) {
+            BatchChunk c;
+            c.poly = p;
+            c.start = a;
+            c.count = (int)std::min<long long>(chunk_points, offsets[p + 1] - a);
+            v.push_back(c);
+        }
+    out.resize(v.size() * sizeof(BatchChunk));
+    if (!v.empty()) memcpy(out.data(), v.data(), out.size());
+    *nchunks = (int)v.size();
+}
+
+// counters: [0] queue count, [1] next chunk.  Everything is enqueued on `s`
+// (no allocation, no host synchronisation), so it can be captured in a graph.
+gahhg_status batch_query_launch(const void* d_views, int npoly, const long long* d_offsets, const void* d_chunks,
+                                int nchunks, const double* d_lonlat, uint8_t* d_labels, int precision,
+                                uint32_t* queue, unsigned int* counters, uint64_t* d_stats, cudaStream_t s,
+                                int device)
+{
+    if (nchunks == 0) return GAHHG_OK;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const QueryView* views = (const QueryView*)d_views;
+    const BatchChunk* chunks = (const BatchChunk*)d_chunks;
+    unsigned long long* ctr = (unsigned long long*)d_stats;
+    GAHHG_CUDA_TRY(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned int), s));
+    const int grid = std::min(nchunks, sms * 8);
+    if (ctr)
+        k_batch_locate<true><<<grid, TPB, 0, s>>>(views, chunks, nchunks, counters + 1, (const double2*)d_lonlat,
+                                                  d_labels, queue, counters, ctr);
+    else
+        k_batch_locate<false><<<grid, TPB, 0, s>>>(views, chunks, nchunks, counters + 1, (const double2*)d_lonlat,
+                                                   d_labels, queue, counters, ctr);
+    if (precision == GAHHG_QUERY_FP64_FILTER)
+        k_batch_leaf<false><<<sms * 4, TPB, 0, s>>>(views, d_offsets, npoly, (const double2*)d_lonlat, d_labels,
+                                                    queue, counters, ctr);
+    else
+        k_batch_leaf<true><<<sms * 4, TPB, 0, s>>>(views, d_offsets, npoly, (const double2*)d_lonlat, d_labels,
+                                                   queue, counters, ctr);
+    GAHHG_CUDA_TRY(cudaGetLastError());
+    return GAHHG_OK;
 }
 
 }  // namespace gahhg

@@ -158,6 +158,51 @@ gahhg_status gahhg_query_device_noalloc(gahhg_grid* g, const double* d_lonlat, s
                                         int precision, void* stream);
 long long gahhg_query_noalloc_max_points(void);
 
+/* ---- batches: many polygons (no counterpart in the reference) ----------- */
+
+typedef struct gahhg_batch gahhg_batch;
+
+typedef struct {
+    int polygons;
+    int workers;               /* host threads that built the lattices */
+    long long edges;
+    long long lattice_bytes;   /* device bytes of all exact indexes */
+    double build_s;            /* wall time of gahhg_batch_build */
+    double query_s;            /* device time of the last synchronous batch query */
+    long long query_points;
+    long long boundary_points;
+    long long esc_fp64;
+    long long esc_exact;
+    long long in_count;
+} gahhg_batch_stats;
+
+/* Builds the exact index of every polygon (exact semantics only; the hexagon
+ * hierarchy is not built).  Builds run concurrently on `workers` host threads
+ * (0 = up to 16), each with its own stream.  top_cells / leaf_edges, when not
+ * NULL, set each polygon's lattice_top / lattice_leaf (e.g. from the
+ * autotuner); 0 entries mean automatic.  The polygons must outlive the batch. */
+gahhg_status gahhg_batch_build(const gahhg_polygon* const* polys, int count, const gahhg_build_opts* opts,
+                               const int* top_cells, const int* leaf_edges, int workers, gahhg_batch** out);
+int gahhg_batch_size(const gahhg_batch* b);
+/* Points per work chunk of the persistent query launch (default 4096). */
+gahhg_status gahhg_batch_set_chunk(gahhg_batch* b, int chunk_points);
+/* Labels for all polygons at once.  d_lonlat holds the points polygon after
+ * polygon: polygon p owns points [offsets[p], offsets[p+1]) (host array of
+ * count+1 entries, offsets[0] = 0, fewer than 2^32 points in all).  Exact
+ * labels (GAHHG_QUERY_AUTO, _FP32_FILTER, _FP64_FILTER).  Scratch comes from
+ * the library's stream-ordered pool; with sync != 0 the call waits and
+ * records statistics. */
+gahhg_status gahhg_batch_query_device(gahhg_batch* b, const double* d_lonlat, const int64_t* offsets,
+                                      uint8_t* d_labels, int precision, void* stream, int sync);
+/* The same query as a CUDA graph: the first call with a given set of
+ * pointers, offsets and precision captures the launch sequence (with its own
+ * persistent scratch); later calls with the same arguments only launch the
+ * graph on `stream`.  Replays of one batch's graph must not overlap. */
+gahhg_status gahhg_batch_query_graph(gahhg_batch* b, const double* d_lonlat, const int64_t* offsets,
+                                     uint8_t* d_labels, int precision, void* stream);
+gahhg_status gahhg_batch_stats_get(const gahhg_batch* b, gahhg_batch_stats* s);
+void gahhg_batch_free(gahhg_batch* b);
+
 /* ---- statistics / report ------------------------------------------------ */
 
 gahhg_status gahhg_stats_get(const gahhg_grid* g, gahhg_stats* s);
