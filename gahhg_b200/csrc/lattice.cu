@@ -61,6 +61,16 @@ constexpr uint32_t INDEX_MASK = 0x3FFFFFFFu;
 constexpr double LOC_MARGIN = 2.0e-8;
 constexpr double RAD = GAHHG_PI_TRUNC / 180.0;  // degrees -> canonical radians (approx., bounds only)
 
+// Cap radius = CAP_FACTOR x (half-height + half-width x cos(center lat)).
+// hlat + hlon cos(lat) bounds the distance from the center to any point of
+// the cell (along a parallel, then a meridian).  Children of a 4 x 4 split
+// have their centers within 3/4 of that bound from the parent's center and
+// bounds of about a quarter of it, so a factor of 1.25 keeps every child cap
+// inside its parent's cap with room for the distortion near the poles (the
+// build checks every child), and the arc between two neighbouring top-level
+// centers stays inside the union of their caps.
+constexpr double CAP_FACTOR = 1.25;
+
 // Bound on |q32 - q| per component for q32 from __sincosf (documented error
 // 2^-21.41 on [-pi, pi]) of FP32-rounded canonical radians; see DESIGN.
 constexpr float E_Q32 = 2.0e-6f;
@@ -118,7 +128,7 @@ __host__ __device__ inline NodeCap node_cap(const Geo& g, int lvl, long long ix,
     double sa, ca;
     gahhg_canon_sincos(gahhg_canon_rad(c.latc), &sa, &ca);
     const double hlat = 0.5 * dlat * RAD, hlon = 0.5 * dlon * RAD;
-    c.r = 2.0 * (hlat + hlon * fabs(ca)) * (1.0 + 1e-9) + LOC_MARGIN + 1e-12;
+    c.r = CAP_FACTOR * (hlat + hlon * fabs(ca)) * (1.0 + 1e-9) + LOC_MARGIN + 1e-12;
     return c;
 }
 
@@ -232,7 +242,7 @@ __global__ void k_l0_pairs(BuildView v, int* cnt, const int* off, int* cursor, i
     double la0, la1, lo0, lo1;
     bool full;
     arc_box(A, B, la0, la1, lo0, lo1, full);
-    const double rmax = (2.0 * (0.5 * v.g.dlat0 + 0.5 * v.g.dlon0) * RAD) * (1.0 + 1e-6) + LOC_MARGIN;
+    const double rmax = (CAP_FACTOR * (0.5 * v.g.dlat0 + 0.5 * v.g.dlon0) * RAD) * (1.0 + 1e-6) + LOC_MARGIN;
     const double rdeg = rmax / RAD + 1e-9;
     la0 -= rdeg;
     la1 += rdeg;
