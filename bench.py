@@ -228,6 +228,123 @@ def run_reference(args):
     return 0
 
 
+def device_cap_points(lons, lats, radii_deg, counts, seed, device):
+    """Points uniform by area inside each polygon's cap (1.5 x the bounding
+    radius 1.2 r of a star polygon of radius r), generated on the device."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    counts = np.asarray(counts, dtype=np.int64)
+    n = int(counts.sum())
+    pts = torch.empty((n, 2), dtype=torch.float64, device=device)
+    lon_all = torch.as_tensor(lons, dtype=torch.float64, device=device) * (np.pi / 180)
+    lat_all = torch.as_tensor(lats, dtype=torch.float64, device=device) * (np.pi / 180)
+    R_all = torch.clamp(torch.as_tensor(radii_deg, dtype=torch.float64, device=device) * (1.5 * 1.2 * np.pi / 180),
+                        max=np.pi)
+    starts = np.concatenate([[0], np.cumsum(counts)])
+    p0 = 0
+    while p0 < len(counts):  # polygon ranges of about 32M points keep the temporaries small
+        p1 = p0
+        while p1 < len(counts) and (p1 == p0 or starts[p1 + 1] - starts[p0] <= (1 << 25)):
+            p1 += 1
+        cnt = torch.as_tensor(counts[p0:p1], dtype=torch.int64, device=device)
+        idx = torch.repeat_interleave(torch.arange(p0, p1, device=device), cnt)
+        m = int(starts[p1] - starts[p0])
+        lon0, lat0, R = lon_all[idx], lat_all[idx], R_all[idx]
+        u = torch.rand((m, 2), generator=g, device=device, dtype=torch.float64)
+        c = torch.cos(R) + (1.0 - torch.cos(R)) * u[:, 0]
+        d = torch.arccos(torch.clamp(c, -1.0, 1.0))
+        b = u[:, 1] * 2 * np.pi
+        sl = torch.sin(lat0) * torch.cos(d) + torch.cos(lat0) * torch.sin(d) * torch.cos(b)
+        la2 = torch.asin(torch.clamp(sl, -1.0, 1.0))
+        lo2 = lon0 + torch.atan2(torch.sin(b) * torch.sin(d) * torch.cos(lat0), torch.cos(d) - torch.sin(lat0) * sl)
+        out = pts[starts[p0]:starts[p1]]
+        out[:, 0] = torch.remainder(lo2 * (180 / np.pi) + 180.0, 360.0) - 180.0
+        out[:, 1] = la2 * (180 / np.pi)
+        del idx, lon0, lat0, R, u, c, d, b, sl, la2, lo2
+        p0 = p1
+    return pts
+
+
+def run_c3(args):
+    """Batch configuration: 4,096 star polygons (16-200,000 vertices, 0-8
+    holes, radius 0.5-40 deg, ~5 % around a pole), each with 1e3-1e6 points
+    inside its 1.5x bounding cap; autotuned lattices; one CUDA-graph query
+    over all points per step."""
+    import torch
+    import gahhg_b200 as G
+    from gahhg_b200 import autotune, synth
+    dev = "cuda:0"
+    t0 = time.time()
+    polys = synth.c3_polygons(args.c3_polygons, seed=3)
+    P = [G.Polygon.from_rings(r) for r, _c, _r in polys]
+    gen_s = time.time() - t0
+    rng = np.random.default_rng(4)
+    counts = np.maximum(1, np.round(np.exp(rng.uniform(np.log(1e3), np.log(1e6), len(polys))) *
+                                    args.c3_scale)).astype(np.int64)
+    offsets = np.zeros(len(polys) + 1, dtype=np.int64)
+    offsets[1:] = np.cumsum(counts)
+    lons = [c[0] for _r, c, _ in polys]
+    lats = [c[1] for _r, c, _ in polys]
+    radii = [r for _p, _c, r in polys]
+    t0 = time.time()
+
+    def sample(i):
+        return synth.cap_points(lons[i], lats[i], 1.5 * 1.2 * radii[i], 20000, np.random.default_rng(100 + i))
+
+    tuning = autotune.tune(P, sample, per_class=2, reps=3, budget_s=args.tune_budget)
+    tune_s = time.time() - t0
+    tc, le = tuning.for_polygons(P)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    B = G.Batch(P, top_cells=tc, leaf_edges=le)
+    build_wall = time.time() - t0
+    bst = B.stats()
+    d_pts = device_cap_points(lons, lats, radii, counts, 5, dev)
+    n = int(offsets[-1])
+    d_lab = torch.empty(n, dtype=torch.uint8, device=dev)
+    chunk = autotune.tune_chunk(B, d_pts, offsets, d_lab, reps=2)
+    stream = torch.cuda.current_stream()
+    B.query_device(d_pts.data_ptr(), offsets, d_lab.data_ptr(), G.QUERY_FP32_FILTER, stream.cuda_stream, sync=True)
+    esc = B.stats()
+
+    def step():
+        B.query_device(d_pts.data_ptr(), offsets, d_lab.data_ptr(), G.QUERY_FP32_FILTER, stream.cuda_stream,
+                       graph=True)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    time.sleep(0.3)
+    steps = max(3, args.steps // 20)
+    t = timed_loop(step, steps, stream)
+    clk = clocks.stop()
+    per = t / steps
+    peak, peak_kind = _peaks()
+    achieved = BYTES_PER_POINT * n / per / 1e9
+    print(json.dumps({
+        "metric": METRIC, "value": round(n / per / 1e6, 1), "unit": "Mpts/s", "n_gpus": 1, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": round(per * 1e3, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "C3: %d star polygons (16-200,000 vertices, 0-8 holes, radius 0.5-40 deg), "
+                               "%d FP64 points inside the polygons' 1.5x bounding caps; exact labels; one CUDA-graph "
+                               "query launch per step" % (len(P), n),
+                   "polygons": len(P), "edges": bst["edges"], "points_per_step": n},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None, "bytes_per_point": BYTES_PER_POINT,
+                     "peak_source": peak_kind},
+        "gpu_launches": 2 * steps, "clocks": clk,
+        "build_ms": {"batch_build_wall": round(build_wall * 1e3, 1), "workers": bst["workers"],
+                     "generate_s": round(gen_s, 1), "autotune_s": round(tune_s, 1)},
+        "lattice_bytes": bst["lattice_bytes"], "tuning": tuning.as_dict(), "chunk_points": chunk,
+        "escalation": {"boundary_points": esc["boundary_points"], "fp64_tests": esc["esc_fp64"],
+                       "exact_tests": esc["esc_exact"], "boundary_fraction": round(esc["boundary_points"] / n, 6)},
+    }))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -241,9 +358,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per launch of the query kernel from an ncu capture (profiles/)")
+    ap.add_argument("--config", default="c1", choices=["c1", "c3"])
+    ap.add_argument("--c3-polygons", type=int, default=4096)
+    ap.add_argument("--c3-scale", type=float, default=1.0, help="scale the C3 point counts")
+    ap.add_argument("--tune-budget", type=float, default=60.0)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.config == "c3":
+        return run_c3(args)
 
     import torch
     import torch.distributed as dist

@@ -24,6 +24,7 @@ struct gahhg_batch {
     int chunk_points = 4096;
     std::vector<Polygon*> polys;
     std::vector<Grid*> grids;
+    std::vector<int> swords;  // summary words per polygon (chunk sizing)
     DevArray<uint8_t> views;
     std::vector<cudaStream_t> streams;
     std::vector<void*> scans;
@@ -175,6 +176,7 @@ gahhg_status gahhg_batch_build(const gahhg_polygon* const* polys, int count, con
     long long bytes = 0, edges = 0;
     for (int i = 0; i < count; i++) {
         lattice_view_write(B->grids[i], host.data() + vb * i);
+        B->swords.push_back((int)lattice_summary_words(B->grids[i]));
         bytes += (long long)lattice_bytes(B->grids[i]->lattice);
         edges += B->polys[i]->pv_num;
         if (lattice_summary_words(B->grids[i]) > 4096) {
@@ -241,7 +243,7 @@ gahhg_status gahhg_batch_query_device(gahhg_batch* b, const double* d_lonlat, co
     const long long total = offsets[b->count];
     std::vector<uint8_t> chunks;
     int nchunks = 0;
-    batch_make_chunks((const long long*)offsets, b->count, b->chunk_points, chunks, &nchunks);
+    batch_make_chunks((const long long*)offsets, b->count, b->chunk_points, b->swords.data(), chunks, &nchunks);
     long long* d_off = nullptr;
     void* d_chunks = nullptr;
     uint32_t* queue = nullptr;
@@ -319,7 +321,8 @@ gahhg_status gahhg_batch_query_graph(gahhg_batch* b, const double* d_lonlat, con
         cudaStream_t ws = b->owner_stream;
         const long long total = offsets[b->count];
         std::vector<uint8_t> chunks;
-        batch_make_chunks((const long long*)offsets, b->count, b->chunk_points, chunks, &b->g_nchunks);
+        batch_make_chunks((const long long*)offsets, b->count, b->chunk_points, b->swords.data(), chunks,
+                          &b->g_nchunks);
         GAHHG_TRY(b->g_doff.reserve(b->count + 1, ws, false));
         GAHHG_TRY(b->g_chunks.reserve(std::max<size_t>(chunks.size(), 16), ws, false));
         GAHHG_TRY(b->g_queue.reserve(std::max<long long>(total, 1), ws, false));

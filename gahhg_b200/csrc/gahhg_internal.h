@@ -58,6 +58,29 @@ template <class T> struct DevArray {
     T* ptr = nullptr;
     size_t cap = 0;
     cudaStream_t stream = nullptr;
+    DevArray() = default;
+    DevArray(const DevArray&) = delete;
+    DevArray& operator=(const DevArray&) = delete;
+    DevArray(DevArray&& o) noexcept : ptr(o.ptr), cap(o.cap), stream(o.stream)
+    {
+        o.ptr = nullptr;
+        o.cap = 0;
+    }
+    DevArray& operator=(DevArray&& o) noexcept
+    {
+        if (this != &o) {
+            release();
+            ptr = o.ptr;
+            cap = o.cap;
+            stream = o.stream;
+            o.ptr = nullptr;
+            o.cap = 0;
+        }
+        return *this;
+    }
+    // owners release explicitly before destroying the stream; this only
+    // catches early returns
+    ~DevArray() { release(); }
     gahhg_status reserve(size_t n, cudaStream_t s, bool keep = true)
     {
         if (n <= cap) return GAHHG_OK;
@@ -174,8 +197,8 @@ size_t lattice_view_bytes();
 size_t batch_chunk_bytes();
 void lattice_view_write(const Grid* g, void* dst);
 long long lattice_summary_words(const Grid* g);
-void batch_make_chunks(const long long* offsets, int npoly, int chunk_points, std::vector<uint8_t>& out,
-                       int* nchunks);
+void batch_make_chunks(const long long* offsets, int npoly, int chunk_points, const int* swords,
+                       std::vector<uint8_t>& out, int* nchunks);
 gahhg_status batch_query_launch(const void* d_views, int npoly, const long long* d_offsets, const void* d_chunks,
                                 int nchunks, const double* d_lonlat, uint8_t* d_labels, int precision,
                                 uint32_t* queue, unsigned int* counters, uint64_t* d_stats, cudaStream_t s,

@@ -33,6 +33,7 @@
 //     then exactly (exact_pred.cuh).  Labels are therefore those of the exact
 //     oracle; the FP32 stage only decides when its bound proves the sign.
 #include <algorithm>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -70,6 +71,10 @@ constexpr double RAD = GAHHG_PI_TRUNC / 180.0;  // degrees -> canonical radians 
 // build checks every child), and the arc between two neighbouring top-level
 // centers stays inside the union of their caps.
 constexpr double CAP_FACTOR = 1.25;
+
+// Refinement limits: node words (4 B each) and edge entries of one level.
+constexpr long long NODE_BUDGET = 1LL << 27;
+constexpr long long PAIR_BUDGET = 1LL << 30;
 
 // Bound on |q32 - q| per component for q32 from __sincosf (documented error
 // 2^-21.41 on [-pi, pi]) of FP32-rounded canonical radians; see DESIGN.
@@ -1422,10 +1427,18 @@ gahhg_status lattice_build(Grid* g)
         int nref = 0;
         GAHHG_CUDA_TRY(cudaMemcpyAsync(&nref, g->d_counts + 9, sizeof(int), cudaMemcpyDeviceToHost, s));
         GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+        if (getenv("GAHHG_DEBUG"))
+            fprintf(stderr, "lattice level %d: %d cells, %d edge entries, %d split (W=%d H=%d K=%d)\n", lvl, pl.nn,
+                    pl.npairs, nref, L->geo.W, L->geo.H, L->K);
         if (nref == 0) break;
-        if ((long long)gnext + (long long)nref * FAN * FAN >= (long long)INDEX_MASK) {
-            set_error("exact index: node count exceeds 2^30");
-            return GAHHG_ERR_CAPACITY;
+        // Bounded refinement: a polygon whose edges fill an area densely (not
+        // a curve) would need cells below the edge spacing everywhere.  Past
+        // the budget the remaining cells stay leaves with more edges: the
+        // labels are the same, the crossing loops longer.
+        if ((long long)gnext + (long long)nref * FAN * FAN > NODE_BUDGET || 4LL * pl.npairs > PAIR_BUDGET) {
+            if (getenv("GAHHG_DEBUG"))
+                fprintf(stderr, "lattice level %d: refinement stopped at the node/entry budget\n", lvl);
+            break;
         }
         lv.emplace_back();
         LevelBuf& cl = lv.back();
@@ -1703,17 +1716,22 @@ void lattice_view_write(const Grid* g, void* dst)
 long long lattice_summary_words(const Grid* g) { return g->lattice ? g->lattice->swords : 0; }
 
 // Chunks of at most `chunk_points` points, polygon after polygon.
-void batch_make_chunks(const long long* offsets, int npoly, int chunk_points, std::vector<uint8_t>& out, int* nchunks)
+// A polygon's chunks hold at least 16 points per word of its summary, so
+// staging the summary costs at most a quarter byte per point.
+void batch_make_chunks(const long long* offsets, int npoly, int chunk_points, const int* swords,
+                       std::vector<uint8_t>& out, int* nchunks)
 {
     std::vector<BatchChunk> v;
-    for (int p = 0; p < npoly; p++)
-        for (long long a = offsets[p]; a < offsets[p + 1]; a += chunk_points) {
+    for (int p = 0; p < npoly; p++) {
+        const long long step = std::max<long long>(chunk_points, 16LL * (swords ? swords[p] : 0));
+        for (long long a = offsets[p]; a < offsets[p + 1]; a += step) {
             BatchChunk c;
             c.poly = p;
             c.start = a;
-            c.count = (int)std::min<long long>(chunk_points, offsets[p + 1] - a);
+            c.count = (int)std::min<long long>(step, offsets[p + 1] - a);
             v.push_back(c);
         }
+    }
     out.resize(v.size() * sizeof(BatchChunk));
     if (!v.empty()) memcpy(out.data(), v.data(), out.size());
     *nchunks = (int)v.size();

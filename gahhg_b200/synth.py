@@ -11,11 +11,13 @@ C1  1,000,000-vertex outer ring by midpoint displacement of a 64-gon of
     pole; ten 10,000-vertex holes of radius U[1, 4] deg; 1e8 points uniform.
 C2  the C1 polygon; half the points uniform, half on random edges offset
     along the edge normal by +-10^u rad, u ~ U[-15, -3].
-C3  batch of star polygons: vertex count log-uniform in [16, 200000], 0-8
-    holes (about 1/20 of the outer vertex count each, radius 5-15 % of the
-    outer radius), radius log-uniform in [0.5, 40] deg, centers uniform on the
-    sphere with about 5 % moved onto a pole; per polygon a log-uniform 1e3-1e6
-    points inside the 1.5x bounding cap.
+C3  batch of polygons: vertex count log-uniform in [16, 200000] (fractal
+    outer rings by midpoint displacement of a 16-gon with amplitude 10 % of
+    the radius, star rings below 64 vertices), 0-8 holes (about 1/20 of the
+    outer vertex count each, radius 5-15 % of the outer radius), radius
+    log-uniform in [0.5, 40] deg, centers uniform on the sphere with about 5 %
+    moved onto a pole; per polygon a log-uniform 1e3-1e6 points inside the
+    1.5x bounding cap.
 
 Rings are star-shaped around their center with monotonic bearings and radius
 below 85 deg, so in the gnomonic projection at the center they are simple
@@ -154,7 +156,12 @@ def c3_polygons(count=4096, seed=3, vmin=16, vmax=200_000):
             lon = rng.uniform(-180, 180)
         else:
             lon, lat = uniform_points(1, rng)[0]
-        outer = star_ring(lon, lat, nv, radius, 0.2, rng)
+        if nv < 64:
+            outer = star_ring(lon, lat, nv, radius, 0.2, rng)
+        else:
+            # a fractal boundary like C1's: midpoint displacement of a 16-gon,
+            # amplitude 10 % of the radius halving per level
+            outer, _r = displaced_ring(lon, lat, nv, radius, base=16, amp_deg=0.1 * radius, rng=rng)
         rings = [outer]
         nh = int(rng.integers(0, 9))
         placed = []
