@@ -345,6 +345,173 @@ def run_c3(args):
     return 0
 
 
+def run_c4(args):
+    """Serving configuration: 1,024 resident C3-style polygons (built through
+    the server, pinned); open-loop Poisson arrivals at `--c4-rate` requests/s
+    for `--c4-seconds`: 95 % queries (polygon uniform over the residents,
+    log-uniform 1-1e6 points inside its 1.5x bounding cap, from pageable host
+    memory), 5 % builds of new C3-style polygons admitted by HBM footprint
+    (the budget leaves `--c4-headroom` GB above the residents; the least
+    recently used unpinned indexes are evicted).  Latency is submission to
+    labels in host memory."""
+    import torch
+    import gahhg_b200 as G
+    from gahhg_b200 import autotune, synth
+    dev = "cuda:0"
+    t0 = time.time()
+    polys = synth.c3_polygons(args.c4_polygons, seed=41)
+    fresh = synth.c3_polygons(args.c4_new, seed=42)
+    P = [G.Polygon.from_rings(r) for r, _c, _r in polys]
+    NP = [G.Polygon.from_rings(r) for r, _c, _r in fresh]
+    gen_s = time.time() - t0
+    lons = [c[0] for _r, c, _ in polys]
+    lats = [c[1] for _r, c, _ in polys]
+    radii = [r for _p, _c, r in polys]
+
+    def sample(i):
+        return synth.cap_points(lons[i], lats[i], 1.5 * 1.2 * radii[i], 20000, np.random.default_rng(200 + i))
+
+    t0 = time.time()
+    tuning = autotune.tune(P, sample, per_class=1, reps=2, budget_s=args.tune_budget)
+    tune_s = time.time() - t0
+    tc, le = tuning.for_polygons(P)
+    ntc, nle = tuning.for_polygons(NP)
+
+    def serve(budget):
+        srv = G.Server(slots=args.c4_slots, slot_points=args.c4_slot_points, build_workers=args.c4_workers,
+                       evict_lru=True, hbm_budget=int(budget))
+        t0 = time.time()
+        built = [srv.build(p, tc[i], le[i], pinned=True) for i, p in enumerate(P)]
+        for _pid, tk in built:
+            srv.wait(tk, 600.0)
+        return srv, [pid for pid, _tk in built], time.time() - t0
+
+    # the resident set's footprint, then the served configuration with a
+    # budget of the residents plus the headroom
+    srv, ids, resident_build_s = serve(150e9)
+    resident = srv.stats()["resident_bytes"]
+    srv.close()
+    srv, ids, _ = serve(resident * 1.02 + args.c4_headroom * 1e9)
+    # point pools: pool_n points per polygon inside its cap, pageable host memory
+    pool_n = args.c4_pool
+    d_pool = device_cap_points(lons, lats, radii, [pool_n] * len(P), 43, dev)
+    pool = d_pool.cpu().numpy()
+    del d_pool
+    torch.cuda.empty_cache()
+    lab_pool = np.zeros(len(pool), dtype=np.uint8)
+    total = len(pool)
+    # the arrival schedule
+    rng = np.random.default_rng(44)
+    nev = int(args.c4_rate * args.c4_seconds * 1.1) + 16
+    times = np.cumsum(rng.exponential(1.0 / args.c4_rate, nev))
+    times = times[times < args.c4_seconds]
+    nev = len(times)
+    is_build = rng.random(nev) < args.c4_build_frac
+    qpoly = rng.integers(0, len(P), nev)
+    qn = np.maximum(1, np.round(np.exp(rng.uniform(0.0, np.log(1e6), nev)))).astype(np.int64)
+    qoff = np.empty(nev, dtype=np.int64)
+    for k in range(nev):
+        n = qn[k]
+        if n <= pool_n:
+            qoff[k] = qpoly[k] * pool_n + rng.integers(0, pool_n - n + 1)
+        else:  # a request longer than one pool continues into the next polygons' pools
+            qoff[k] = min(qpoly[k] * pool_n, total - n)
+    q_idx = np.nonzero(~is_build)[0]
+    b_idx = np.nonzero(is_build)[0]
+    offered_pts = int(qn[q_idx].sum())
+    pool_ptr, lab_ptr = pool.ctypes.data, lab_pool.ctypes.data
+    lags = np.zeros(len(q_idx))
+    build_lag = []
+
+    def builds(t_start):
+        for j, k in enumerate(b_idx):
+            target = t_start + times[k]
+            d = target - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            build_lag.append(time.perf_counter() - target)
+            m = j % len(NP)
+            srv.build(NP[m], ntc[m], nle[m], detached=True)
+
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    time.sleep(0.3)
+    srv.reset_stats()
+    t_start = time.perf_counter() + 0.02
+    bt = threading.Thread(target=builds, args=(t_start,))
+    bt.start()
+    for j, k in enumerate(q_idx):
+        target = t_start + times[k]
+        while True:
+            now = time.perf_counter()
+            d = target - now
+            if d <= 0:
+                break
+            if d > 0.0006:
+                time.sleep(d - 0.0005)
+        lags[j] = now - target
+        off = int(qoff[k])
+        srv.query_raw(ids[qpoly[k]], pool_ptr + 16 * off, int(qn[k]), lab_ptr + off, detached=True)
+    t_submit_end = time.perf_counter()
+    bt.join()
+    srv.drain(300.0)
+    t_end = time.perf_counter()
+    st = srv.stats()
+    clk = clocks.stop()
+    lat = srv.latencies(0)
+    tr = srv.trace()
+    if args.c4_trace:
+        np.savez(args.c4_trace, trace=tr, latencies=lat, builds=srv.latencies(1))
+    window = t_end - t_start
+    srv.close()
+    sustained = st["query_points"] / window
+
+    def pct(a, q):
+        return round(float(np.percentile(a, q)), 4) if len(a) else None
+
+    print(json.dumps({
+        "metric": METRIC, "value": round(st["p99_ms"], 3), "unit": "ms (query p99)", "n_gpus": 1,
+        "steps": int(st["queries_done"]), "warmup": 0,
+        "ms_per_step": round(float(lat.mean()), 4) if len(lat) else None,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "C4: %d resident C3-style polygons; Poisson arrivals at %g req/s for %g s: %d %% "
+                               "queries (uniform polygon, log-uniform 1-1e6 points from pageable host memory), %d %% "
+                               "builds of new C3-style polygons admitted by HBM footprint with LRU eviction"
+                               % (len(P), args.c4_rate, args.c4_seconds, round(100 * (1 - args.c4_build_frac)),
+                                  round(100 * args.c4_build_frac)),
+                   "polygons": len(P), "slots": args.c4_slots, "slot_points": args.c4_slot_points,
+                   "build_workers": args.c4_workers, "pool_points_per_polygon": pool_n,
+                   "hbm_budget_gb": round(st["hbm_budget"] / 1e9, 2)},
+        "latency_ms": {"p50": round(st["p50_ms"], 3), "p90": round(st["p90_ms"], 3), "p99": round(st["p99_ms"], 3),
+                       "max": round(st["max_ms"], 3), "build_p50": round(st["build_p50_ms"], 2),
+                       "build_p99": round(st["build_p99_ms"], 2)},
+        "throughput": {"sustained_mpts_s": round(sustained / 1e6, 3),
+                       "offered_mpts_s": round(offered_pts / args.c4_seconds / 1e6, 3),
+                       "queries": int(st["queries_done"]), "builds_done": int(st["builds_done"]),
+                       "builds_failed": int(st["builds_failed"]), "evictions": int(st["evictions"]),
+                       "batches": int(st["batches"]), "mean_batch_pieces": round(st["mean_batch_pieces"], 2),
+                       "mean_batch_points": round(st["mean_batch_points"], 1),
+                       "drain_s": round(t_end - t_submit_end, 4)},
+        "batch_trace_ms": {"enqueue_p99": pct(tr[:, 1], 99), "device_p50": pct(tr[:, 2], 50),
+                           "device_p99": pct(tr[:, 2], 99), "device_max": pct(tr[:, 2], 100),
+                           "complete_p99": pct(tr[:, 3], 99)},
+        "e2e": {"value": round(sustained / 1e6, 3), "unit": "Mpts/s",
+                "h2d_bytes_per_step": int(16 * st["query_points"] / max(st["queries_done"], 1)),
+                "d2h_bytes_per_step": int(st["query_points"] / max(st["queries_done"], 1))},
+        "arrival_lag_ms": {"p50": round(float(np.median(lags)) * 1e3, 4),
+                           "p99": round(float(np.percentile(lags, 99)) * 1e3, 4),
+                           "build_p99": round(float(np.percentile(build_lag, 99)) * 1e3, 4) if build_lag else None},
+        "escalation": {"boundary_points": st["boundary_points"], "fp64_tests": st["esc_fp64"],
+                       "exact_tests": st["esc_exact"]},
+        "gpu_launches": 2 * int(st["batches"]), "clocks": clk,
+        "build_ms": {"resident_set_wall": round(resident_build_s * 1e3, 1), "resident_bytes": resident,
+                     "generate_s": round(gen_s, 1), "autotune_s": round(tune_s, 1)},
+        "tuning": tuning.as_dict(),
+    }))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -358,15 +525,28 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per launch of the query kernel from an ncu capture (profiles/)")
-    ap.add_argument("--config", default="c1", choices=["c1", "c3"])
+    ap.add_argument("--config", default="c1", choices=["c1", "c3", "c4"])
     ap.add_argument("--c3-polygons", type=int, default=4096)
     ap.add_argument("--c3-scale", type=float, default=1.0, help="scale the C3 point counts")
     ap.add_argument("--tune-budget", type=float, default=60.0)
+    ap.add_argument("--c4-polygons", type=int, default=1024)
+    ap.add_argument("--c4-new", type=int, default=256, help="distinct new polygons the build requests cycle over")
+    ap.add_argument("--c4-rate", type=float, default=2000.0, help="requests per second (Poisson)")
+    ap.add_argument("--c4-seconds", type=float, default=20.0)
+    ap.add_argument("--c4-build-frac", type=float, default=0.05)
+    ap.add_argument("--c4-slots", type=int, default=4)
+    ap.add_argument("--c4-slot-points", type=int, default=1 << 22)
+    ap.add_argument("--c4-workers", type=int, default=4)
+    ap.add_argument("--c4-pool", type=int, default=1 << 19, help="host points per resident polygon")
+    ap.add_argument("--c4-headroom", type=float, default=8.0, help="GB of budget above the resident set")
+    ap.add_argument("--c4-trace", default=None, help="save the per-batch trace and latencies (.npz)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.config == "c3":
         return run_c3(args)
+    if args.config == "c4":
+        return run_c4(args)
 
     import torch
     import torch.distributed as dist

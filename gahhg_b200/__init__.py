@@ -193,6 +193,114 @@ class Batch:
             self._h = None
 
 
+class Server:
+    """A request loop over resident exact indexes (gahhg_server_* in
+    include/gahhg.h): builds admitted by HBM footprint, queries batched
+    continuously into in-flight slots, latency percentiles.
+
+    Query buffers must stay alive and unmoved until the request completes;
+    `query` keeps references to the numpy arrays it was given until then.
+    """
+
+    def __init__(self, device=0, slots=4, slot_points=1 << 22, max_pieces=4096, chunk_points=4096,
+                 build_workers=4, max_polygons=65536, hbm_budget=0, evict_lru=False,
+                 precision=QUERY_FP32_FILTER, direct_min_points=65536):
+        L = _lib.lib()
+        o = _lib.ServerOpts()
+        L.gahhg_server_opts_init(ctypes.byref(o))
+        o.device, o.slots, o.slot_points, o.max_pieces = device, slots, slot_points, max_pieces
+        o.chunk_points, o.build_workers, o.max_polygons = chunk_points, build_workers, max_polygons
+        o.hbm_budget, o.evict_lru, o.precision = int(hbm_budget), 1 if evict_lru else 0, precision
+        o.direct_min_points = direct_min_points
+        h = ctypes.c_void_p()
+        check(L.gahhg_server_create(ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def build(self, polygon, top_cells=0, leaf_edges=0, pinned=False, detached=False):
+        """Queues a build; returns (polygon id, ticket)."""
+        pid, tk = ctypes.c_int(), ctypes.c_int64()
+        flags = (_lib.SERVE_PINNED if pinned else 0) | (_lib.SERVE_DETACHED if detached else 0)
+        check(_lib.lib().gahhg_server_submit_build(self._h, polygon._h, int(top_cells), int(leaf_edges), flags,
+                                                   ctypes.byref(pid), ctypes.byref(tk)))
+        return pid.value, tk.value
+
+    def query(self, pid, lonlat, labels=None, detached=False):
+        """Queues a query of (n, 2) float64 lon/lat; returns (ticket, labels array)."""
+        ll = np.asarray(lonlat)
+        assert ll.dtype == np.float64 and ll.flags.c_contiguous and ll.ndim == 2 and ll.shape[1] == 2
+        if labels is None:
+            labels = np.empty(len(ll), dtype=np.uint8)
+        assert labels.dtype == np.uint8 and labels.flags.c_contiguous and len(labels) >= len(ll)
+        tk = ctypes.c_int64()
+        check(_lib.lib().gahhg_server_submit_query(self._h, int(pid), ctypes.c_void_p(ll.ctypes.data), len(ll),
+                                                   ctypes.c_void_p(labels.ctypes.data),
+                                                   _lib.SERVE_DETACHED if detached else 0, ctypes.byref(tk)))
+        if not detached:
+            self._keep[tk.value] = (ll, labels)
+        return tk.value, labels
+
+    def query_raw(self, pid, ll_ptr, n, labels_ptr, detached=True):
+        """Pointer form (the caller keeps the buffers alive); returns the ticket."""
+        tk = ctypes.c_int64()
+        check(_lib.lib().gahhg_server_submit_query(self._h, int(pid), ctypes.c_void_p(ll_ptr), int(n),
+                                                   ctypes.c_void_p(labels_ptr),
+                                                   _lib.SERVE_DETACHED if detached else 0, ctypes.byref(tk)))
+        return tk.value
+
+    def wait(self, ticket, timeout_s=60.0):
+        st = _lib.lib().gahhg_server_wait(self._h, int(ticket), float(timeout_s))
+        if st != _lib.ERR_STATE:
+            self._keep.pop(ticket, None)
+        check(st)
+
+    def drain(self, timeout_s=120.0):
+        check(_lib.lib().gahhg_server_drain(self._h, float(timeout_s)))
+
+    def evict(self, pid):
+        check(_lib.lib().gahhg_server_evict(self._h, int(pid)))
+
+    def state(self, pid):
+        st, b = ctypes.c_int(), ctypes.c_longlong()
+        check(_lib.lib().gahhg_server_polygon_state(self._h, int(pid), ctypes.byref(st), ctypes.byref(b)))
+        return st.value, b.value
+
+    def stats(self):
+        s = _lib.ServerStats()
+        check(_lib.lib().gahhg_server_stats_get(self._h, ctypes.byref(s)))
+        return s.as_dict()
+
+    def reset_stats(self):
+        check(_lib.lib().gahhg_server_stats_reset(self._h))
+
+    def latencies(self, kind=0):
+        L = _lib.lib()
+        n = L.gahhg_server_latencies(self._h, kind, None, 0)
+        out = np.zeros(n, dtype=np.float64)
+        if n:
+            L.gahhg_server_latencies(self._h, kind, _lib.ptr(out), n)
+        return out
+
+    def trace(self):
+        """Per query batch: formed (s), host enqueue ms, device ms, completion
+        ms after forming, points, pieces."""
+        L = _lib.lib()
+        n = L.gahhg_server_trace(self._h, None, 0)
+        out = np.zeros((n, 6), dtype=np.float64)
+        if n:
+            L.gahhg_server_trace(self._h, _lib.ptr(out), n)
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().gahhg_server_free(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        self.close()
+
+
 def write_result(path, labels):
     labels = np.ascontiguousarray(labels, dtype=np.uint8)
     check(_lib.lib().gahhg_result_write(str(path).encode(), _lib.ptr(labels), len(labels)))

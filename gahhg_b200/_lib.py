@@ -71,6 +71,35 @@ class BatchStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_int), ("slot_points", ctypes.c_longlong),
+                ("max_pieces", ctypes.c_int), ("chunk_points", ctypes.c_int), ("build_workers", ctypes.c_int),
+                ("max_polygons", ctypes.c_int), ("hbm_budget", ctypes.c_longlong), ("evict_lru", ctypes.c_int),
+                ("precision", ctypes.c_int), ("direct_min_points", ctypes.c_int)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("queries_done", ctypes.c_longlong), ("query_points", ctypes.c_longlong),
+                ("builds_done", ctypes.c_longlong), ("builds_failed", ctypes.c_longlong),
+                ("evictions", ctypes.c_longlong), ("batches", ctypes.c_longlong), ("pieces", ctypes.c_longlong),
+                ("resident_polygons", ctypes.c_int), ("pending_queries", ctypes.c_int),
+                ("pending_builds", ctypes.c_int), ("inflight_batches", ctypes.c_int),
+                ("resident_bytes", ctypes.c_longlong), ("hbm_budget", ctypes.c_longlong),
+                ("window_s", ctypes.c_double), ("points_per_s", ctypes.c_double),
+                ("p50_ms", ctypes.c_double), ("p90_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("max_ms", ctypes.c_double), ("build_p50_ms", ctypes.c_double), ("build_p99_ms", ctypes.c_double),
+                ("mean_batch_points", ctypes.c_double), ("mean_batch_pieces", ctypes.c_double),
+                ("boundary_points", ctypes.c_longlong), ("esc_fp64", ctypes.c_longlong),
+                ("esc_exact", ctypes.c_longlong), ("in_count", ctypes.c_longlong)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+SERVE_PINNED = 1
+SERVE_DETACHED = 2
+POLY_FREE, POLY_QUEUED, POLY_BUILDING, POLY_READY, POLY_FAILED, POLY_EVICTING = range(6)
+
 # name: (restype, argtypes)
 _P = ctypes.c_void_p
 _SIGS = {
@@ -108,6 +137,22 @@ _SIGS = {
     "gahhg_batch_query_graph": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int, _P]),
     "gahhg_batch_stats_get": (ctypes.c_int, [_P, ctypes.POINTER(BatchStats)]),
     "gahhg_batch_free": (None, [_P]),
+    "gahhg_server_opts_init": (None, [ctypes.POINTER(ServerOpts)]),
+    "gahhg_server_create": (ctypes.c_int, [ctypes.POINTER(ServerOpts), ctypes.POINTER(_P)]),
+    "gahhg_server_submit_build": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64)]),
+    "gahhg_server_submit_query": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int64, _P, ctypes.c_int,
+                                                 ctypes.POINTER(ctypes.c_int64)]),
+    "gahhg_server_wait": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_double]),
+    "gahhg_server_drain": (ctypes.c_int, [_P, ctypes.c_double]),
+    "gahhg_server_evict": (ctypes.c_int, [_P, ctypes.c_int]),
+    "gahhg_server_polygon_state": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                                  ctypes.POINTER(ctypes.c_longlong)]),
+    "gahhg_server_stats_get": (ctypes.c_int, [_P, ctypes.POINTER(ServerStats)]),
+    "gahhg_server_stats_reset": (ctypes.c_int, [_P]),
+    "gahhg_server_latencies": (ctypes.c_longlong, [_P, ctypes.c_int, _P, ctypes.c_longlong]),
+    "gahhg_server_trace": (ctypes.c_longlong, [_P, _P, ctypes.c_longlong]),
+    "gahhg_server_free": (None, [_P]),
 }
 
 _lib = None

@@ -22,29 +22,48 @@ void set_error(const char* fmt, ...)
 
 const char* last_error() { return g_err; }
 
-gahhg_status pool_alloc(void** p, size_t bytes, int device, cudaStream_t s)
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pools[64] = {};
+
+static gahhg_status device_pool(int device, cudaMemPool_t* out)
 {
-    static std::mutex mu;
-    static cudaMemPool_t pools[64] = {};
     if (device < 0 || device >= 64) {
         set_error("device ordinal %d out of range", device);
         return GAHHG_ERR_ARG;
     }
-    cudaMemPool_t pool;
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        if (!pools[device]) {
-            cudaMemPoolProps props = {};
-            props.allocType = cudaMemAllocationTypePinned;
-            props.location.type = cudaMemLocationTypeDevice;
-            props.location.id = device;
-            GAHHG_CUDA_TRY(cudaMemPoolCreate(&pools[device], &props));
-            uint64_t keep = 4ull << 30;  // keep up to 4 GB cached between calls
-            GAHHG_CUDA_TRY(cudaMemPoolSetAttribute(pools[device], cudaMemPoolAttrReleaseThreshold, &keep));
-        }
-        pool = pools[device];
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (!g_pools[device]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        GAHHG_CUDA_TRY(cudaMemPoolCreate(&g_pools[device], &props));
+        uint64_t keep = 4ull << 30;  // keep up to 4 GB cached between calls
+        GAHHG_CUDA_TRY(cudaMemPoolSetAttribute(g_pools[device], cudaMemPoolAttrReleaseThreshold, &keep));
     }
+    *out = g_pools[device];
+    return GAHHG_OK;
+}
+
+gahhg_status pool_alloc(void** p, size_t bytes, int device, cudaStream_t s)
+{
+    cudaMemPool_t pool;
+    GAHHG_TRY(device_pool(device, &pool));
     GAHHG_CUDA_TRY(cudaMallocFromPoolAsync(p, bytes, pool, s));
+    return GAHHG_OK;
+}
+
+gahhg_status pool_keep(int device, size_t bytes)
+{
+    cudaMemPool_t pool;
+    GAHHG_TRY(device_pool(device, &pool));
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    uint64_t cur = 0;
+    GAHHG_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &cur));
+    if ((uint64_t)bytes > cur) {
+        uint64_t v = bytes;
+        GAHHG_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &v));
+    }
     return GAHHG_OK;
 }
 
@@ -54,12 +73,22 @@ double now_seconds()
     return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
 
-gahhg_status Polygon::upload()
+gahhg_status Polygon::upload(cudaStream_t s, int device)
 {
     if (d_pv) return GAHHG_OK;
     if (pv_num <= 0) {
         set_error("polygon has no edges");
         return GAHHG_ERR_ARG;
+    }
+    if (s) {
+        // stream-ordered from the library pool: neither the upload nor the
+        // release synchronises other streams
+        GAHHG_TRY(pool_alloc((void**)&d_pv, sizeof(D3) * pv_num, device, s));
+        GAHHG_TRY(pool_alloc((void**)&d_pe, sizeof(int) * 2 * pv_num, device, s));
+        pooled = true;
+        GAHHG_CUDA_TRY(cudaMemcpyAsync(d_pv, pv.data(), sizeof(D3) * pv_num, cudaMemcpyHostToDevice, s));
+        GAHHG_CUDA_TRY(cudaMemcpyAsync(d_pe, pe.data(), sizeof(int) * 2 * pv_num, cudaMemcpyHostToDevice, s));
+        return GAHHG_OK;
     }
     GAHHG_CUDA_TRY(cudaMalloc(&d_pv, sizeof(D3) * pv_num));
     GAHHG_CUDA_TRY(cudaMalloc(&d_pe, sizeof(int) * 2 * pv_num));
@@ -68,8 +97,26 @@ gahhg_status Polygon::upload()
     return GAHHG_OK;
 }
 
+void Polygon::copy_host(const Polygon& o)
+{
+    pv_num = o.pv_num;
+    num_rings = o.num_rings;
+    lonlat = o.lonlat;
+    pv = o.pv;
+    pe = o.pe;
+    ring_start = o.ring_start;
+    path = o.path;
+}
+
 Polygon::~Polygon()
 {
+    // pooled copies were last used by kernels whose completion the owner has
+    // observed; the legacy stream does not wait for non-blocking streams
+    if (pooled) {
+        if (d_pv) cudaFreeAsync(d_pv, 0);
+        if (d_pe) cudaFreeAsync(d_pe, 0);
+        return;
+    }
     if (d_pv) cudaFree(d_pv);
     if (d_pe) cudaFree(d_pe);
 }

@@ -26,8 +26,7 @@ struct gahhg_batch {
     std::vector<Grid*> grids;
     std::vector<int> swords;  // summary words per polygon (chunk sizing)
     DevArray<uint8_t> views;
-    std::vector<cudaStream_t> streams;
-    std::vector<void*> scans;
+    WorkerPool pool;
     gahhg_batch_stats stats{};
     // graph replay state
     cudaGraphExec_t exec = nullptr;
@@ -36,7 +35,6 @@ struct gahhg_batch {
     uint8_t* g_labels = nullptr;
     int g_precision = -1;
     std::vector<int64_t> g_offsets;
-    DevArray<long long> g_doff;
     DevArray<uint8_t> g_chunks;
     DevArray<uint32_t> g_queue;
     DevArray<unsigned int> g_counters;
@@ -47,16 +45,12 @@ struct gahhg_batch {
     {
         cudaSetDevice(device);
         if (exec) cudaGraphExecDestroy(exec);
-        g_doff.release();
         g_chunks.release();
         g_queue.release();
         g_counters.release();
         views.release();
         for (Grid* g : grids) delete g;
-        for (size_t i = 0; i < streams.size(); i++) {
-            scan_state_destroy(scans[i]);
-            cudaStreamDestroy(streams[i]);
-        }
+        pool.destroy();
         if (owner_stream) {
             cudaStreamSynchronize(owner_stream);
             cudaStreamDestroy(owner_stream);
@@ -64,26 +58,27 @@ struct gahhg_batch {
     }
 };
 
-namespace {
+namespace gahhg {
 
-gahhg_status build_one(gahhg_batch* B, int i, cudaStream_t s, void** scan, const gahhg_build_opts& base,
-                       int top, int leaf)
+// Builds the exact index of one polygon on stream s (the caller's worker
+// context); the grid borrows the stream and the scan state.
+gahhg_status build_exact_grid(Polygon* P, int device, cudaStream_t s, void** scan, const gahhg_build_opts& base,
+                              int top, int leaf, Grid** out)
 {
-    Polygon* P = B->polys[i];
-    GAHHG_TRY(P->upload());
+    GAHHG_TRY(P->upload(s, device));
     Grid* g = new Grid();
-    B->grids[i] = g;
+    *out = g;
     g->poly = P;
     g->opts = base;
     g->opts.semantics = GAHHG_SEMANTICS_EXACT;
     if (top > 0) g->opts.lattice_top = top;
     if (leaf > 0) g->opts.lattice_leaf = leaf;
-    g->device = B->device;
+    g->device = device;
     g->stream = s;
     g->borrowed = true;
     g->scan_state = *scan;
-    GAHHG_TRY(pool_alloc((void**)&g->d_err, sizeof(DeviceErrors), B->device, s));
-    GAHHG_TRY(pool_alloc((void**)&g->d_counts, 64 * sizeof(int), B->device, s));
+    GAHHG_TRY(pool_alloc((void**)&g->d_err, sizeof(DeviceErrors), device, s));
+    GAHHG_TRY(pool_alloc((void**)&g->d_counts, 64 * sizeof(int), device, s));
     GAHHG_CUDA_TRY(cudaMemsetAsync(g->d_err, 0, sizeof(DeviceErrors), s));
     const gahhg_status st = lattice_build(g);
     *scan = g->scan_state;  // the build may have grown it
@@ -95,7 +90,71 @@ gahhg_status build_one(gahhg_batch* B, int i, cudaStream_t s, void** scan, const
     return st;
 }
 
-}  // namespace
+gahhg_status WorkerPool::create(int device, int n, int priority)
+{
+    this->device = device;
+    streams.assign(n, nullptr);
+    scans.assign(n, nullptr);
+    for (int w = 0; w < n; w++) {
+        if (cudaStreamCreateWithPriority(&streams[w], cudaStreamNonBlocking, priority) != cudaSuccess ||
+            scan_state_reserve(&scans[w], 1u << 26) != GAHHG_OK) {
+            set_error("worker stream or scan state creation failed");
+            return GAHHG_ERR_CUDA;
+        }
+    }
+    return GAHHG_OK;
+}
+
+void WorkerPool::destroy()
+{
+    for (size_t i = 0; i < streams.size(); i++) {
+        if (scans[i]) scan_state_destroy(scans[i]);
+        if (streams[i]) cudaStreamDestroy(streams[i]);
+    }
+    streams.clear();
+    scans.clear();
+}
+
+// Builds grids[i] for every polygon with the pool's workers, one host thread
+// per worker stream.  Returns the first failure (index in *failed).
+gahhg_status WorkerPool::build_all(const std::vector<Polygon*>& polys, const gahhg_build_opts& base,
+                                   const int* top, const int* leaf, std::vector<Grid*>& grids, int* failed)
+{
+    const int count = (int)polys.size();
+    grids.assign(count, nullptr);
+    std::atomic<int> next(0);
+    std::atomic<int> bad(-1);
+    std::mutex mu;
+    std::string first_error;
+    gahhg_status first_status = GAHHG_OK;
+    auto worker = [&](int w) {
+        cudaSetDevice(device);
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= count || bad.load() >= 0) break;
+            const gahhg_status st = build_exact_grid(polys[i], device, streams[w], &scans[w], base,
+                                                     top ? top[i] : 0, leaf ? leaf[i] : 0, &grids[i]);
+            if (st != GAHHG_OK) {
+                std::lock_guard<std::mutex> lock(mu);
+                if (bad.load() < 0) {
+                    bad.store(i);
+                    first_status = st;
+                    first_error = last_error();
+                }
+            }
+        }
+        cudaStreamSynchronize(streams[w]);
+    };
+    std::vector<std::thread> th;
+    const int nw = std::min((int)streams.size(), std::max(count, 1));
+    for (int w = 0; w < nw; w++) th.emplace_back(worker, w);
+    for (auto& t : th) t.join();
+    *failed = bad.load();
+    if (*failed >= 0) set_error("polygon %d: %s", *failed, first_error.c_str());
+    return *failed >= 0 ? first_status : GAHHG_OK;
+}
+
+}  // namespace gahhg
 
 extern "C" {
 
@@ -127,48 +186,18 @@ gahhg_status gahhg_batch_build(const gahhg_polygon* const* polys, int count, con
     }
     int nw = workers > 0 ? workers : (int)std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
     nw = std::min(nw, count);
-    B->streams.resize(nw);
-    B->scans.assign(nw, nullptr);
-    for (int w = 0; w < nw; w++) {
-        if (cudaStreamCreateWithFlags(&B->streams[w], cudaStreamNonBlocking) != cudaSuccess ||
-            scan_state_reserve(&B->scans[w], 1u << 26) != GAHHG_OK) {
-            delete B;
-            set_error("gahhg_batch_build: stream or scan state creation failed");
-            return GAHHG_ERR_CUDA;
-        }
+    if (B->pool.create(B->device, nw) != GAHHG_OK) {
+        delete B;
+        return GAHHG_ERR_CUDA;
     }
     const double t0 = now_seconds();
-    std::atomic<int> next(0);
-    std::atomic<int> failed(-1);
-    std::mutex mu;
-    std::string first_error;
-    gahhg_status first_status = GAHHG_OK;
-    auto worker = [&](int w) {
-        cudaSetDevice(B->device);
-        for (;;) {
-            const int i = next.fetch_add(1);
-            if (i >= count || failed.load() >= 0) break;
-            const gahhg_status st = build_one(B, i, B->streams[w], &B->scans[w], base,
-                                              top_cells ? top_cells[i] : 0, leaf_edges ? leaf_edges[i] : 0);
-            if (st != GAHHG_OK) {
-                std::lock_guard<std::mutex> lock(mu);
-                if (failed.load() < 0) {
-                    failed.store(i);
-                    first_status = st;
-                    first_error = last_error();
-                }
-            }
-        }
-        cudaStreamSynchronize(B->streams[w]);
-    };
-    std::vector<std::thread> th;
-    for (int w = 0; w < nw; w++) th.emplace_back(worker, w);
-    for (auto& t : th) t.join();
-    if (failed.load() >= 0) {
-        const int i = failed.load();
+    int failed = -1;
+    const gahhg_status bst = B->pool.build_all(B->polys, base, top_cells, leaf_edges, B->grids, &failed);
+    if (bst != GAHHG_OK) {
+        const std::string msg = last_error();
         delete B;
-        set_error("gahhg_batch_build: polygon %d: %s", i, first_error.c_str());
-        return first_status;
+        set_error("gahhg_batch_build: %s", msg.c_str());
+        return bst;
     }
     // per-polygon query views, in one device table
     const size_t vb = lattice_view_bytes();
@@ -185,7 +214,7 @@ gahhg_status gahhg_batch_build(const gahhg_polygon* const* polys, int count, con
             return GAHHG_ERR_CAPACITY;
         }
     }
-    cudaStream_t s0 = B->streams[0];
+    cudaStream_t s0 = B->pool.streams[0];
     GAHHG_TRY(B->views.reserve(host.size(), s0, false));
     GAHHG_CUDA_TRY(cudaMemcpyAsync(B->views.ptr, host.data(), host.size(), cudaMemcpyHostToDevice, s0));
     GAHHG_CUDA_TRY(cudaStreamSynchronize(s0));
@@ -243,17 +272,15 @@ gahhg_status gahhg_batch_query_device(gahhg_batch* b, const double* d_lonlat, co
     const long long total = offsets[b->count];
     std::vector<uint8_t> chunks;
     int nchunks = 0;
-    batch_make_chunks((const long long*)offsets, b->count, b->chunk_points, b->swords.data(), chunks, &nchunks);
-    long long* d_off = nullptr;
+    batch_make_chunks((const long long*)offsets, b->count, b->chunk_points, b->swords.data(), nullptr, chunks,
+                      &nchunks);
     void* d_chunks = nullptr;
     uint32_t* queue = nullptr;
     unsigned int* counters = nullptr;
     uint64_t* d_stats = nullptr;
-    GAHHG_TRY(pool_alloc((void**)&d_off, sizeof(long long) * (b->count + 1), b->device, s));
     GAHHG_TRY(pool_alloc(&d_chunks, std::max<size_t>(chunks.size(), 16), b->device, s));
     GAHHG_TRY(pool_alloc((void**)&queue, sizeof(uint32_t) * std::max<long long>(total, 1), b->device, s));
     GAHHG_TRY(pool_alloc((void**)&counters, 4 * sizeof(unsigned int), b->device, s));
-    GAHHG_CUDA_TRY(cudaMemcpyAsync(d_off, offsets, sizeof(long long) * (b->count + 1), cudaMemcpyHostToDevice, s));
     if (!chunks.empty())
         GAHHG_CUDA_TRY(cudaMemcpyAsync(d_chunks, chunks.data(), chunks.size(), cudaMemcpyHostToDevice, s));
     if (sync) {
@@ -266,8 +293,8 @@ gahhg_status gahhg_batch_query_device(gahhg_batch* b, const double* d_lonlat, co
         cudaEventCreate(&e1);
         cudaEventRecord(e0, s);
     }
-    gahhg_status st = batch_query_launch(b->views.ptr, b->count, d_off, d_chunks, nchunks, d_lonlat, d_labels,
-                                         precision, queue, counters, d_stats, s, b->device);
+    gahhg_status st = batch_query_launch(b->views.ptr, d_chunks, nchunks, d_lonlat, d_labels, precision, queue,
+                                         counters, d_stats, s, b->device);
     if (sync && st == GAHHG_OK) {
         cudaEventRecord(e1, s);
         uint64_t c[4] = {0, 0, 0, 0};
@@ -288,7 +315,6 @@ gahhg_status gahhg_batch_query_device(gahhg_batch* b, const double* d_lonlat, co
     }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
-    cudaFreeAsync(d_off, s);
     cudaFreeAsync(d_chunks, s);
     cudaFreeAsync(queue, s);
     cudaFreeAsync(counters, s);
@@ -321,14 +347,11 @@ gahhg_status gahhg_batch_query_graph(gahhg_batch* b, const double* d_lonlat, con
         cudaStream_t ws = b->owner_stream;
         const long long total = offsets[b->count];
         std::vector<uint8_t> chunks;
-        batch_make_chunks((const long long*)offsets, b->count, b->chunk_points, b->swords.data(), chunks,
+        batch_make_chunks((const long long*)offsets, b->count, b->chunk_points, b->swords.data(), nullptr, chunks,
                           &b->g_nchunks);
-        GAHHG_TRY(b->g_doff.reserve(b->count + 1, ws, false));
         GAHHG_TRY(b->g_chunks.reserve(std::max<size_t>(chunks.size(), 16), ws, false));
         GAHHG_TRY(b->g_queue.reserve(std::max<long long>(total, 1), ws, false));
         GAHHG_TRY(b->g_counters.reserve(4, ws, false));
-        GAHHG_CUDA_TRY(cudaMemcpyAsync(b->g_doff.ptr, offsets, sizeof(long long) * (b->count + 1),
-                                       cudaMemcpyHostToDevice, ws));
         if (!chunks.empty())
             GAHHG_CUDA_TRY(cudaMemcpyAsync(b->g_chunks.ptr, chunks.data(), chunks.size(), cudaMemcpyHostToDevice, ws));
         GAHHG_CUDA_TRY(cudaStreamSynchronize(ws));
@@ -339,8 +362,8 @@ gahhg_status gahhg_batch_query_graph(gahhg_batch* b, const double* d_lonlat, con
         if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
             st = GAHHG_ERR_CUDA;
         } else {
-            st = batch_query_launch(b->views.ptr, b->count, b->g_doff.ptr, b->g_chunks.ptr, b->g_nchunks, d_lonlat,
-                                    d_labels, precision, b->g_queue.ptr, b->g_counters.ptr, nullptr, cs, b->device);
+            st = batch_query_launch(b->views.ptr, b->g_chunks.ptr, b->g_nchunks, d_lonlat, d_labels, precision,
+                                    b->g_queue.ptr, b->g_counters.ptr, nullptr, cs, b->device);
             if (cudaStreamEndCapture(cs, &graph) != cudaSuccess) st = GAHHG_ERR_CUDA;
         }
         cudaStreamDestroy(cs);

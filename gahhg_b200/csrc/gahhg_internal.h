@@ -51,6 +51,8 @@ struct DeviceErrors {
 // synchronisation).  Allocation and release are ordered on the given stream,
 // so builds on different streams never synchronise the whole device.
 gahhg_status pool_alloc(void** p, size_t bytes, int device, cudaStream_t s);
+// Raises the pool's release threshold to at least `bytes` (never lowers it).
+gahhg_status pool_keep(int device, size_t bytes);
 
 // Growable device array (explicit capacity, reallocated with a copy), backed
 // by the pool and ordered on the stream it was last reserved on.
@@ -123,7 +125,13 @@ struct Polygon {
     // device copies
     D3* d_pv = nullptr;
     int* d_pe = nullptr;
-    gahhg_status upload();
+    bool pooled = false;          // device copies come from the stream-ordered pool
+    // Device copies: synchronous cudaMalloc without a stream, else ordered on s.
+    gahhg_status upload(cudaStream_t s = nullptr, int device = 0);
+    void copy_host(const Polygon& o);  // host arrays only
+    Polygon() = default;
+    Polygon(const Polygon&) = delete;
+    Polygon& operator=(const Polygon&) = delete;
     ~Polygon();
 };
 
@@ -197,13 +205,19 @@ size_t lattice_view_bytes();
 size_t batch_chunk_bytes();
 void lattice_view_write(const Grid* g, void* dst);
 long long lattice_summary_words(const Grid* g);
-void batch_make_chunks(const long long* offsets, int npoly, int chunk_points, const int* swords,
+// Chunks over segments of points stored segment after segment; segment p's
+// points belong to view seg_view[p] (p itself when seg_view is null).
+void batch_make_chunks(const long long* offsets, int nseg, int chunk_points, const int* swords, const int* seg_view,
                        std::vector<uint8_t>& out, int* nchunks);
-gahhg_status batch_query_launch(const void* d_views, int npoly, const long long* d_offsets, const void* d_chunks,
-                                int nchunks, const double* d_lonlat, uint8_t* d_labels, int precision,
-                                uint32_t* queue, unsigned int* counters, uint64_t* d_stats, cudaStream_t s,
-                                int device);
+void batch_write_chunks(const long long* offsets, int nseg, int chunk_points, const int* swords, const int* seg_view,
+                        void* out, int* nchunks);
+size_t batch_chunk_count_bound(long long points, int nseg, int chunk_points);
+// counters[0..1] must be zero on entry unless zero_counters is set.
+gahhg_status batch_query_launch(const void* d_views, const void* d_chunks, int nchunks, const double* d_lonlat,
+                                uint8_t* d_labels, int precision, uint32_t* queue, unsigned int* counters,
+                                uint64_t* d_stats, cudaStream_t s, int device, bool zero_counters = true);
 size_t lattice_bytes(const Lattice* L);
+size_t lattice_device_bytes(const Lattice* L);  // capacity held on the device
 
 // scans (scan.cu)
 size_t scan_state_bytes(size_t n);
@@ -213,6 +227,20 @@ gahhg_status scan_exclusive(const int* d_in, int* d_out, int n, int* d_total, vo
                             cudaStream_t s);
 
 double now_seconds();
+
+// Host threads with one non-blocking stream and look-back scan state each,
+// building exact indexes concurrently (batch.cpp).
+struct WorkerPool {
+    int device = 0;
+    std::vector<cudaStream_t> streams;
+    std::vector<void*> scans;
+    gahhg_status create(int device, int n, int priority = 0);
+    void destroy();
+    gahhg_status build_all(const std::vector<Polygon*>& polys, const gahhg_build_opts& base, const int* top,
+                           const int* leaf, std::vector<Grid*>& grids, int* failed);
+};
+gahhg_status build_exact_grid(Polygon* P, int device, cudaStream_t s, void** scan, const gahhg_build_opts& base,
+                              int top, int leaf, Grid** out);
 
 }  // namespace gahhg
 

@@ -33,6 +33,7 @@
 //     then exactly (exact_pred.cuh).  Labels are therefore those of the exact
 //     oracle; the FP32 stage only decides when its bound proves the sign.
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
@@ -966,9 +967,10 @@ __global__ void __launch_bounds__(TPB) k_leaf(const double2* __restrict__ ll, ui
 
 // ------------------------------------------------------------- batches --
 
-// A run of points of one polygon (points are stored polygon after polygon).
+// A run of points of one view (points are stored segment after segment, and
+// chunks are in point order, so chunk starts are increasing).
 struct BatchChunk {
-    int poly;
+    int view;
     int count;
     long long start;
 };
@@ -995,7 +997,7 @@ __global__ void __launch_bounds__(TPB) k_batch_locate(const QueryView* __restric
         const int ci = s_chunk;
         if (ci >= nchunks) break;
         const BatchChunk c = chunks[ci];
-        const QueryView Q = views[c.poly];
+        const QueryView Q = views[c.view];
         for (int k = threadIdx.x; k < Q.swords; k += TPB) s_sum[k] = __ldg(Q.summary + k);
         __syncthreads();
         locate_range<STATS>(Q, s_sum, ll, out, queue, qcount, c.start, c.count, 0, 1, inside);
@@ -1004,11 +1006,11 @@ __global__ void __launch_bounds__(TPB) k_batch_locate(const QueryView* __restric
     if (STATS && ctr) count_inside(inside, ctr + 3);
 }
 
-// Pass 2 over a batch: the polygon of a queued point by binary search of the
-// per-polygon point offsets.
+// Pass 2 over a batch: the view of a queued point by binary search of the
+// chunk starts (the chunk table stays in L1/L2).
 template <bool FP32>
 __global__ void __launch_bounds__(TPB) k_batch_leaf(const QueryView* __restrict__ views,
-                                                   const long long* __restrict__ offsets, int npoly,
+                                                   const BatchChunk* __restrict__ chunks, int nchunks,
                                                    const double2* __restrict__ ll, uint8_t* __restrict__ out,
                                                    const uint32_t* __restrict__ queue,
                                                    const unsigned int* __restrict__ qcount, unsigned long long* ctr)
@@ -1017,13 +1019,13 @@ __global__ void __launch_bounds__(TPB) k_batch_leaf(const QueryView* __restrict_
     int inside = 0;
     for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
         const uint32_t i = queue[t];
-        int lo = 0, hi = npoly;  // offsets[lo] <= i < offsets[hi]
+        int lo = 0, hi = nchunks;  // chunks[lo].start <= i < chunks[hi].start
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
-            if (offsets[mid] <= (long long)i) lo = mid;
+            if (__ldg(&chunks[mid].start) <= (long long)i) lo = mid;
             else hi = mid;
         }
-        const uint8_t lab = leaf_point<FP32>(views[lo], ll[i], ctr);
+        const uint8_t lab = leaf_point<FP32>(views[__ldg(&chunks[lo].view)], ll[i], ctr);
         out[i] = lab;
         inside += lab == CELL_IN;
     }
@@ -1062,6 +1064,13 @@ size_t lattice_bytes(const Lattice* L)
 {
     if (!L) return 0;
     return L->nnodes * sizeof(uint32_t) + L->nleaves * sizeof(LeafRec) + L->nrecs * sizeof(EdgeRec);
+}
+
+size_t lattice_device_bytes(const Lattice* L)
+{
+    if (!L) return 0;
+    return L->nodes.cap * sizeof(uint32_t) + L->leaves.cap * sizeof(LeafRec) + L->recs.cap * sizeof(EdgeRec) +
+           L->summary.cap * sizeof(uint32_t);
 }
 
 namespace {
@@ -1715,42 +1724,60 @@ void lattice_view_write(const Grid* g, void* dst)
 
 long long lattice_summary_words(const Grid* g) { return g->lattice ? g->lattice->swords : 0; }
 
-// Chunks of at most `chunk_points` points, polygon after polygon.
-// A polygon's chunks hold at least 16 points per word of its summary, so
+// Chunks of at most `chunk_points` points, segment after segment.
+// A segment's chunks hold at least 16 points per word of its summary, so
 // staging the summary costs at most a quarter byte per point.
-void batch_make_chunks(const long long* offsets, int npoly, int chunk_points, const int* swords,
-                       std::vector<uint8_t>& out, int* nchunks)
+void batch_write_chunks(const long long* offsets, int nseg, int chunk_points, const int* swords, const int* seg_view,
+                        void* out, int* nchunks)
 {
-    std::vector<BatchChunk> v;
-    for (int p = 0; p < npoly; p++) {
+    BatchChunk* v = (BatchChunk*)out;
+    int n = 0;
+    for (int p = 0; p < nseg; p++) {
         const long long step = std::max<long long>(chunk_points, 16LL * (swords ? swords[p] : 0));
         for (long long a = offsets[p]; a < offsets[p + 1]; a += step) {
             BatchChunk c;
-            c.poly = p;
+            c.view = seg_view ? seg_view[p] : p;
             c.start = a;
             c.count = (int)std::min<long long>(step, offsets[p + 1] - a);
-            v.push_back(c);
+            if (v) v[n] = c;
+            n++;
         }
     }
-    out.resize(v.size() * sizeof(BatchChunk));
-    if (!v.empty()) memcpy(out.data(), v.data(), out.size());
-    *nchunks = (int)v.size();
+    *nchunks = n;
+}
+
+size_t batch_chunk_count_bound(long long points, int nseg, int chunk_points)
+{
+    return (size_t)(points / std::max(chunk_points, 1)) + (size_t)nseg + 1;
+}
+
+void batch_make_chunks(const long long* offsets, int nseg, int chunk_points, const int* swords, const int* seg_view,
+                       std::vector<uint8_t>& out, int* nchunks)
+{
+    int n = 0;
+    batch_write_chunks(offsets, nseg, chunk_points, swords, seg_view, nullptr, &n);
+    out.resize((size_t)n * sizeof(BatchChunk));
+    batch_write_chunks(offsets, nseg, chunk_points, swords, seg_view, out.data(), nchunks);
 }
 
 // counters: [0] queue count, [1] next chunk.  Everything is enqueued on `s`
 // (no allocation, no host synchronisation), so it can be captured in a graph.
-gahhg_status batch_query_launch(const void* d_views, int npoly, const long long* d_offsets, const void* d_chunks,
-                                int nchunks, const double* d_lonlat, uint8_t* d_labels, int precision,
-                                uint32_t* queue, unsigned int* counters, uint64_t* d_stats, cudaStream_t s,
-                                int device)
+gahhg_status batch_query_launch(const void* d_views, const void* d_chunks, int nchunks, const double* d_lonlat,
+                                uint8_t* d_labels, int precision, uint32_t* queue, unsigned int* counters,
+                                uint64_t* d_stats, cudaStream_t s, int device, bool zero_counters)
 {
     if (nchunks == 0) return GAHHG_OK;
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    static std::atomic<int> sms_cache[64];
+    int sms = (device >= 0 && device < 64) ? sms_cache[device].load(std::memory_order_relaxed) : 0;
+    if (!sms) {
+        sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (device >= 0 && device < 64) sms_cache[device].store(sms, std::memory_order_relaxed);
+    }
     const QueryView* views = (const QueryView*)d_views;
     const BatchChunk* chunks = (const BatchChunk*)d_chunks;
     unsigned long long* ctr = (unsigned long long*)d_stats;
-    GAHHG_CUDA_TRY(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned int), s));
+    if (zero_counters) GAHHG_CUDA_TRY(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned int), s));
     const int grid = std::min(nchunks, sms * 8);
     if (ctr)
         k_batch_locate<true><<<grid, TPB, 0, s>>>(views, chunks, nchunks, counters + 1, (const double2*)d_lonlat,
@@ -1759,10 +1786,10 @@ gahhg_status batch_query_launch(const void* d_views, int npoly, const long long*
         k_batch_locate<false><<<grid, TPB, 0, s>>>(views, chunks, nchunks, counters + 1, (const double2*)d_lonlat,
                                                    d_labels, queue, counters, ctr);
     if (precision == GAHHG_QUERY_FP64_FILTER)
-        k_batch_leaf<false><<<sms * 4, TPB, 0, s>>>(views, d_offsets, npoly, (const double2*)d_lonlat, d_labels,
+        k_batch_leaf<false><<<sms * 4, TPB, 0, s>>>(views, chunks, nchunks, (const double2*)d_lonlat, d_labels,
                                                     queue, counters, ctr);
     else
-        k_batch_leaf<true><<<sms * 4, TPB, 0, s>>>(views, d_offsets, npoly, (const double2*)d_lonlat, d_labels,
+        k_batch_leaf<true><<<sms * 4, TPB, 0, s>>>(views, chunks, nchunks, (const double2*)d_lonlat, d_labels,
                                                    queue, counters, ctr);
     GAHHG_CUDA_TRY(cudaGetLastError());
     return GAHHG_OK;

@@ -203,6 +203,102 @@ gahhg_status gahhg_batch_query_graph(gahhg_batch* b, const double* d_lonlat, con
 gahhg_status gahhg_batch_stats_get(const gahhg_batch* b, gahhg_batch_stats* s);
 void gahhg_batch_free(gahhg_batch* b);
 
+/* ---- serving: a request loop over resident indexes (no counterpart in the
+ * reference, which answers one query file for one polygon per process) --- */
+
+typedef struct gahhg_server gahhg_server;
+
+typedef struct gahhg_server_opts {
+    int device;
+    int slots;              /* query batches in flight, each with its own stream and buffers (4) */
+    long long slot_points;  /* points per batch; larger requests are split (4,194,304) */
+    int max_pieces;         /* requests (or request pieces) per batch (4096) */
+    int chunk_points;       /* work grain of the persistent query launch (4096) */
+    int build_workers;      /* host threads building indexes, each with a low-priority stream (4) */
+    int max_polygons;       /* polygon ids, resident or not (65536) */
+    long long hbm_budget;   /* bytes of resident indexes; 0 = half the free device memory at creation */
+    int evict_lru;          /* admit a build by evicting the least recently queried unpinned polygons */
+    int precision;          /* GAHHG_QUERY_FP32_FILTER (default) or _FP64_FILTER; labels are exact either way */
+    int direct_min_points;  /* requests in page-locked memory of at least this many points are copied
+                               without staging (65536) */
+} gahhg_server_opts;
+
+/* Submission flags. */
+#define GAHHG_SERVE_PINNED 1    /* build: never evicted to admit another build */
+#define GAHHG_SERVE_DETACHED 2  /* no ticket is kept: the request cannot be waited on (drain instead) */
+
+/* Polygon states (gahhg_server_polygon_state). */
+#define GAHHG_POLY_FREE 0
+#define GAHHG_POLY_QUEUED 1     /* waiting for HBM admission */
+#define GAHHG_POLY_BUILDING 2
+#define GAHHG_POLY_READY 3
+#define GAHHG_POLY_FAILED 4
+#define GAHHG_POLY_EVICTING 5   /* evicted; freed when its last query completes */
+
+typedef struct gahhg_server_stats {
+    long long queries_done;
+    long long query_points;     /* points of completed queries */
+    long long builds_done;
+    long long builds_failed;    /* build errors and refused admissions */
+    long long evictions;
+    long long batches;          /* query batches launched */
+    long long pieces;           /* request pieces in those batches */
+    int resident_polygons;
+    int pending_queries;
+    int pending_builds;
+    int inflight_batches;
+    long long resident_bytes;   /* device bytes of resident indexes and polygons */
+    long long hbm_budget;
+    double window_s;            /* since creation or the last stats reset */
+    double points_per_s;        /* query_points / window_s */
+    double p50_ms, p90_ms, p99_ms, max_ms;  /* query latency, submission to labels in host memory */
+    double build_p50_ms, build_p99_ms;      /* build latency, submission to ready */
+    double mean_batch_points;
+    double mean_batch_pieces;
+    long long boundary_points;  /* points answered by the crossing test */
+    long long esc_fp64;         /* crossing tests the FP32 filter could not decide */
+    long long esc_exact;        /* ... nor the FP64 filter */
+    long long in_count;
+} gahhg_server_stats;
+
+void gahhg_server_opts_init(gahhg_server_opts* o);
+gahhg_status gahhg_server_create(const gahhg_server_opts* o, gahhg_server** out);
+/* Queues the exact-index build of a copy of `poly` (the handle may be freed
+ * after the call).  *id is the polygon's id at once: queries to it are held
+ * until it is ready.  A build is admitted when its estimated footprint fits
+ * in the budget; one that cannot fit even after eviction fails with
+ * GAHHG_ERR_CAPACITY on its ticket.  Ids are reused after eviction. */
+gahhg_status gahhg_server_submit_build(gahhg_server* s, const gahhg_polygon* poly, int top_cells, int leaf_edges,
+                                       int flags, int* id, int64_t* ticket);
+/* Queues labels for n points (host lon/lat pairs) of polygon `id`, written
+ * to labels[0..n) before the request completes.  Both buffers must stay
+ * valid until then.  Requests are batched with whatever else is pending
+ * when a slot frees, so work of concurrent requests overlaps on the device;
+ * a request's labels do not depend on what it was batched with. */
+gahhg_status gahhg_server_submit_query(gahhg_server* s, int id, const double* lonlat, int64_t n, uint8_t* labels,
+                                       int flags, int64_t* ticket);
+/* Waits for a ticket: returns the request's own status (and forgets the
+ * ticket), or GAHHG_ERR_STATE if it is still pending after timeout_s. */
+gahhg_status gahhg_server_wait(gahhg_server* s, int64_t ticket, double timeout_s);
+/* Waits until no request is pending or in flight (GAHHG_ERR_STATE on timeout). */
+gahhg_status gahhg_server_drain(gahhg_server* s, double timeout_s);
+/* Frees polygon `id` once its submitted queries complete; later queries to
+ * it fail.  Also releases the id of a failed build. */
+gahhg_status gahhg_server_evict(gahhg_server* s, int id);
+gahhg_status gahhg_server_polygon_state(gahhg_server* s, int id, int* state, long long* bytes);
+gahhg_status gahhg_server_stats_get(gahhg_server* s, gahhg_server_stats* out);
+/* Clears latency samples and counters and restarts the window. */
+gahhg_status gahhg_server_stats_reset(gahhg_server* s);
+/* Copies up to `cap` latency samples (ms) of kind 0 = queries, 1 = builds;
+ * returns how many there are. */
+long long gahhg_server_latencies(gahhg_server* s, int kind, double* out, long long cap);
+/* Per-batch trace (kind 0 = query batches): up to `cap` records of 6 doubles
+ * each - formed (s since the window start), host enqueue ms, device ms,
+ * completion ms after forming, points, pieces.  Returns the record count. */
+long long gahhg_server_trace(gahhg_server* s, double* out, long long cap);
+/* Drains (up to 60 s), stops the threads and frees everything. */
+void gahhg_server_free(gahhg_server* s);
+
 /* ---- statistics / report ------------------------------------------------ */
 
 gahhg_status gahhg_stats_get(const gahhg_grid* g, gahhg_stats* s);
