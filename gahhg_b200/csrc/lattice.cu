@@ -34,6 +34,7 @@
 //     oracle; the FP32 stage only decides when its bound proves the sign.
 #include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
@@ -101,11 +102,13 @@ static_assert(sizeof(EdgeRec) == 40, "EdgeRec");
 
 // Level-0 grid over a lon/lat domain: W x H cells of dlon0 x dlat0 degrees
 // starting at (lon0, lat0).  full_lon: the domain spans all longitudes
-// (W * dlon0 = 360); to_north / to_south: it reaches the pole.
+// (W * dlon0 = 360); to_north / to_south: it reaches the pole.  cap_cos
+// bounds cos(latitude) over the domain (1 when it spans the equator).
 struct Geo {
     int W, H;
     double lon0, lat0;
     double dlon0, dlat0;
+    double cap_cos;
     bool full_lon, to_north, to_south;
 };
 
@@ -131,8 +134,14 @@ __host__ __device__ inline NodeCap node_cap(const Geo& g, int lvl, long long ix,
     c.lonc = g.lon0 + ((double)ix + 0.5) * dlon;
     c.latc = g.lat0 + ((double)iy + 0.5) * dlat;
     gahhg_canon_vertex_xyz(c.lonc, c.latc, c.R);
+    // the width term takes cos at the cell's equator-ward edge, the widest
+    // parallel of the cell: a child's center then lies within 3/4 of the
+    // parent's bound and its own bound is a quarter of it, so every child cap
+    // nests in its parent's for any cell aspect (near a pole cos changes by a
+    // large factor across one cell)
+    const double phi_eq = fmax(fabs(c.latc) - 0.5 * dlat, 0.0);
     double sa, ca;
-    gahhg_canon_sincos(gahhg_canon_rad(c.latc), &sa, &ca);
+    gahhg_canon_sincos(gahhg_canon_rad(phi_eq), &sa, &ca);
     const double hlat = 0.5 * dlat * RAD, hlon = 0.5 * dlon * RAD;
     c.r = CAP_FACTOR * (hlat + hlon * fabs(ca)) * (1.0 + 1e-9) + LOC_MARGIN + 1e-12;
     return c;
@@ -236,69 +245,131 @@ struct BuildView {
     int n;
 };
 
-// Level-0 pairs: one thread per edge, candidate cells from the edge's box.
-template <int PASS>
-__global__ void k_l0_pairs(BuildView v, int* cnt, const int* off, int* cursor, int* list)
+// Level-0 candidates of one edge: rows [iy0, iy0 + nrows) by up to two
+// column ranges [c0, c0 + n0) and [c1, c1 + n1) (the inflated longitude
+// interval may wrap past 360 degrees relative to the domain's west edge).
+struct EdgeBox {
+    int iy0, nrows, c0, n0, c1, n1;
+};
+
+// A work item is one row of one column chunk of an edge's box, so no thread
+// tests more than L0_CHUNK cells: an edge near a pole (all columns) or a
+// very long edge has a box of up to millions of cells, and one thread per
+// edge would hold its block for tens of milliseconds.
+constexpr int L0_CHUNK = 64;
+
+__device__ inline int l0_chunks(int n) { return (n + L0_CHUNK - 1) / L0_CHUNK; }
+
+// Per edge: its candidate box and number of work items; total64 accumulates
+// the 64-bit item total (the 32-bit scan of the counts must not wrap).
+__global__ void k_l0_box(BuildView v, EdgeBox* box, int* items, unsigned long long* total64)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= v.n) return;
-    const D3 A = v.pv[v.pe[2 * t]], B = v.pv[v.pe[2 * t + 1]];
-    if (A.x == B.x && A.y == B.y && A.z == B.z) return;
-    const int W = v.g.W, H = v.g.H;
-    double la0, la1, lo0, lo1;
-    bool full;
-    arc_box(A, B, la0, la1, lo0, lo1, full);
-    const double rmax = (CAP_FACTOR * (0.5 * v.g.dlat0 + 0.5 * v.g.dlon0) * RAD) * (1.0 + 1e-6) + LOC_MARGIN;
-    const double rdeg = rmax / RAD + 1e-9;
-    la0 -= rdeg;
-    la1 += rdeg;
-    int iy0 = (int)floor((la0 - v.g.lat0) / v.g.dlat0), iy1 = (int)floor((la1 - v.g.lat0) / v.g.dlat0);
-    iy0 = max(iy0, 0);
-    iy1 = min(iy1, H - 1);
-    const double maxlat = fmax(fabs(la0), fabs(la1));
-    // candidate columns: up to two ranges (the inflated lon interval may wrap
-    // past 360 degrees relative to the domain's west edge)
-    long long r0a = 0, r0b = W - 1, r1a = 1, r1b = 0;
-    bool all_cols = full || maxlat >= 89.0;
-    if (!all_cols) {
-        const double c = cos(maxlat * RAD);
-        const double wdeg = rdeg / c;
-        const double len = (lo1 - lo0) + 2 * wdeg;
-        if (len >= 360.0) {
-            all_cols = true;
-        } else {
-            double a = lo0 - wdeg - v.g.lon0;
-            a -= 360.0 * floor(a / 360.0);  // [0, 360)
-            r0a = (long long)floor(a / v.g.dlon0);
-            r0b = (long long)floor((a + len) / v.g.dlon0);
-            if (a + len >= 360.0) {
-                r1a = 0;
-                r1b = (long long)floor((a + len - 360.0) / v.g.dlon0);
+    long long nit = 0;
+    if (t < v.n) {
+        EdgeBox bx{0, 0, 0, 0, 0, 0};
+        const D3 A = v.pv[v.pe[2 * t]], B = v.pv[v.pe[2 * t + 1]];
+        if (!(A.x == B.x && A.y == B.y && A.z == B.z)) {
+            const int W = v.g.W, H = v.g.H;
+            double la0, la1, lo0, lo1;
+            bool full;
+            arc_box(A, B, la0, la1, lo0, lo1, full);
+            const double rmax =
+                (CAP_FACTOR * (0.5 * v.g.dlat0 + 0.5 * v.g.dlon0 * v.g.cap_cos) * RAD) * (1.0 + 1e-6) + LOC_MARGIN;
+            const double rdeg = rmax / RAD + 1e-9;
+            la0 -= rdeg;
+            la1 += rdeg;
+            int iy0 = (int)floor((la0 - v.g.lat0) / v.g.dlat0), iy1 = (int)floor((la1 - v.g.lat0) / v.g.dlat0);
+            iy0 = max(iy0, 0);
+            iy1 = min(iy1, H - 1);
+            const double maxlat = fmax(fabs(la0), fabs(la1));
+            long long r0a = 0, r0b = W - 1, r1a = 1, r1b = 0;
+            bool all_cols = full || maxlat >= 89.0;
+            if (!all_cols) {
+                const double c = cos(maxlat * RAD);
+                const double wdeg = rdeg / c;
+                const double len = (lo1 - lo0) + 2 * wdeg;
+                if (len >= 360.0) {
+                    all_cols = true;
+                } else {
+                    double a = lo0 - wdeg - v.g.lon0;
+                    a -= 360.0 * floor(a / 360.0);  // [0, 360)
+                    r0a = (long long)floor(a / v.g.dlon0);
+                    r0b = (long long)floor((a + len) / v.g.dlon0);
+                    if (a + len >= 360.0) {
+                        r1a = 0;
+                        r1b = (long long)floor((a + len - 360.0) / v.g.dlon0);
+                    }
+                }
             }
+            if (all_cols) {
+                r0a = 0;
+                r0b = W - 1;
+                r1a = 1;
+                r1b = 0;
+            }
+            r0a = max(r0a, 0LL);
+            r0b = min(r0b, (long long)W - 1);
+            r1b = min(r1b, (long long)W - 1);
+            bx.iy0 = iy0;
+            bx.nrows = max(0, iy1 - iy0 + 1);
+            bx.c0 = (int)r0a;
+            bx.n0 = (int)max(0LL, r0b - r0a + 1);
+            bx.c1 = (int)r1a;
+            bx.n1 = (int)max(0LL, r1b - r1a + 1);
+            nit = (long long)bx.nrows * (l0_chunks(bx.n0) + l0_chunks(bx.n1));
         }
+        box[t] = bx;
+        items[t] = (int)min(nit, (long long)INT_MAX);
     }
-    if (all_cols) {
-        r0a = 0;
-        r0b = W - 1;
-        r1a = 1;
-        r1b = 0;
-    }
-    r0a = max(r0a, 0LL);
-    r0b = min(r0b, (long long)W - 1);
-    r1b = min(r1b, (long long)W - 1);
-    for (int iy = iy0; iy <= iy1; iy++) {
-        for (int range = 0; range < 2; range++) {
-            const long long xa = range ? r1a : r0a, xb = range ? r1b : r0b;
-            for (long long ix = xa; ix <= xb; ix++) {
+    // one 64-bit atomic per warp
+    unsigned long long w = (unsigned long long)nit;
+    for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+    if ((threadIdx.x & 31) == 0 && w) atomicAdd(total64, w);
+}
+
+// Level-0 pairs over the work items (persistent grid; the item total is read
+// on the device).  PASS 0 counts per cell, PASS 1 fills the lists.
+template <int PASS>
+__global__ void k_l0_expand(BuildView v, const EdgeBox* __restrict__ box, const int* __restrict__ item_off,
+                            const int* total_items, const unsigned long long* total64, int* cnt, const int* off,
+                            int* cursor, int* list)
+{
+    if (*total64 > (unsigned long long)INT_MAX) return;  // the host reports it; the 32-bit offsets wrapped
+    const int total = *total_items;
+    const int W = v.g.W, H = v.g.H;
+    for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < total; it += gridDim.x * blockDim.x) {
+        int lo = 0, hi = v.n;  // the last edge whose first item is <= it
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (item_off[mid] <= it) lo = mid;
+            else hi = mid;
+        }
+        const int t = lo;
+        const EdgeBox b = box[t];
+        const int k0 = l0_chunks(b.n0), kk = k0 + l0_chunks(b.n1);
+        const int local = it - item_off[t];
+        const int iy = b.iy0 + local / kk;
+        const int ch = local % kk;
+        int xa, xb;
+        if (ch < k0) {
+            xa = b.c0 + ch * L0_CHUNK;
+            xb = min(b.c0 + b.n0, xa + L0_CHUNK);
+        } else {
+            xa = b.c1 + (ch - k0) * L0_CHUNK;
+            xb = min(b.c1 + b.n1, xa + L0_CHUNK);
+        }
+        if (iy < 0 || iy >= H || xa < 0 || xb > W) continue;
+        const D3 A = v.pv[v.pe[2 * t]], B = v.pv[v.pe[2 * t + 1]];
+        for (int ix = xa; ix < xb; ix++) {
             const NodeCap c = node_cap(v.g, 0, ix, iy);
             if (!edge_hits_cap(A, B, c.R, c.r)) continue;
-            const int node = iy * W + (int)ix;
+            const int node = iy * W + ix;
             if (PASS == 0) {
                 atomicAdd(&cnt[node], 1);
             } else {
                 const int pos = off[node] + atomicAdd(&cursor[node], 1);
                 list[pos] = t;
-            }
             }
         }
     }
@@ -338,12 +409,24 @@ __global__ void k_fill_pair_node(const int* cnt, const int* off, int nn, int* pa
     for (int k = 0; k < cnt[p]; k++) pair_node[off[p] + k] = p;
 }
 
-__global__ void k_sort_lists(const int* cnt, const int* off, int nn, int* list)
+// Cell lists are filled with atomics, so their order is arbitrary; sorting
+// makes the index deterministic.  Short lists are sorted by their own thread;
+// longer ones are handed to k_sort_long, where a whole block sorts each, so
+// no thread spends O(n^2) steps on one list.
+constexpr int SORT_SMALL = 64;
+constexpr int SORT_SMEM = 12256;  // ints staged in shared memory (48 KB with the block's counter)
+constexpr int SORT_TPB = 512;
+
+__global__ void k_sort_lists(const int* cnt, const int* off, int nn, int* list, int* long_ids, int* nlong)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nn) return;
-    int* L = list + off[p];
     const int n = cnt[p];
+    if (n > SORT_SMALL) {
+        long_ids[atomicAdd(nlong, 1)] = p;
+        return;
+    }
+    int* L = list + off[p];
     for (int i = 1; i < n; i++) {
         int x = L[i], j = i - 1;
         while (j >= 0 && L[j] > x) {
@@ -351,6 +434,70 @@ __global__ void k_sort_lists(const int* cnt, const int* off, int nn, int* list)
             j--;
         }
         L[j + 1] = x;
+    }
+}
+
+// Block-wide bitonic sort, ascending, of a[0..n) in the form where every
+// comparator puts the minimum at the lower index (the first step of each
+// merge compares mirrored positions).  Positions >= n act as +infinity, so
+// comparators that reach them are skipped and no padding is stored.
+__device__ void block_bitonic_sort(int* a, int n)
+{
+    int lg = 1;
+    while ((1 << lg) < n) lg++;
+    const int half = 1 << (lg - 1);  // comparators per step
+    for (int lk = 1; lk <= lg; lk++) {
+        const int k = 1 << lk;
+        for (int lj = lk - 1; lj >= 0; lj--) {
+            const int j = 1 << lj;
+            for (int t = threadIdx.x; t < half; t += blockDim.x) {
+                int i, q;
+                if (lj == lk - 1) {  // mirrored compare across the two sorted halves
+                    const int base = (t >> lj) << lk, pp = t & (j - 1);
+                    i = base + pp;
+                    q = base + k - 1 - pp;
+                } else {
+                    i = ((t >> lj) << (lj + 1)) + (t & (j - 1));
+                    q = i + j;
+                }
+                if (q < n) {
+                    const int x = a[i], y = a[q];
+                    if (x > y) {
+                        a[i] = y;
+                        a[q] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// One list per block iteration (a persistent grid takes them from a counter):
+// in shared memory up to SORT_SMEM entries, in place in global memory beyond.
+__global__ void __launch_bounds__(SORT_TPB) k_sort_long(const int* cnt, const int* off, int* list,
+                                                        const int* long_ids, const int* nlong, int* next)
+{
+    __shared__ int sm[SORT_SMEM];
+    __shared__ int s_i;
+    const int m = *nlong;
+    for (;;) {
+        if (threadIdx.x == 0) s_i = atomicAdd(next, 1);
+        __syncthreads();
+        const int i = s_i;
+        if (i >= m) break;
+        const int p = long_ids[i];
+        const int n = cnt[p];
+        int* L = list + off[p];
+        if (n <= SORT_SMEM) {
+            for (int k = threadIdx.x; k < n; k += blockDim.x) sm[k] = L[k];
+            __syncthreads();
+            block_bitonic_sort(sm, n);
+            for (int k = threadIdx.x; k < n; k += blockDim.x) L[k] = sm[k];
+        } else {
+            block_bitonic_sort(L, n);
+        }
+        __syncthreads();
     }
 }
 
@@ -1098,6 +1245,20 @@ struct LevelBuf {
     }
 };
 
+// Sorts every cell list: short ones by their own thread, long ones by a whole
+// block each (k_sort_long), so no thread holds its block for long.
+gahhg_status sort_lists(Grid* g, const int* cnt, const int* off, int nn, int* list, int sms, cudaStream_t s)
+{
+    int* d_nlong = g->d_counts + 20;  // [0] long lists, [1] next list to sort
+    GAHHG_CUDA_TRY(cudaMemsetAsync(d_nlong, 0, 2 * sizeof(int), s));
+    DevArray<int> long_ids;
+    GAHHG_TRY(long_ids.reserve(std::max(nn, 1), s, false));
+    k_sort_lists<<<blocks_for(nn), TPB, 0, s>>>(cnt, off, nn, list, long_ids.ptr, d_nlong);
+    k_sort_long<<<sms * 2, SORT_TPB, 0, s>>>(cnt, off, list, long_ids.ptr, d_nlong, d_nlong + 1);
+    GAHHG_CUDA_TRY(cudaGetLastError());
+    return GAHHG_OK;
+}
+
 const double HUBS[6][3] = {
     {1.0, 0.000731, 0.000419},  {-1.0, 0.000627, -0.000883}, {0.000577, 1.0, 0.000941},
     {-0.000351, -1.0, 0.000713}, {0.000809, -0.000467, 1.0}, {-0.000689, 0.000523, -1.0},
@@ -1248,9 +1409,27 @@ gahhg_status compute_domain(const Polygon* P, long long target, Geo* G)
         lon0 = ((gstart + glen) % 3600) * 0.1 - 180.0;
         lon_span = (3600 - glen) * 0.1;
     }
-    double lat0 = latmin, lat_span = std::max(latmax - latmin, 1e-6);
-    // cell size (degrees) for about `target` cells, with the padding included
-    double cell = sqrt(std::max(lon_span, 1e-6) * lat_span / (double)std::max(target, 1LL));
+    double lat_span = std::max(latmax - latmin, 1e-6);
+    // Cells are `aspect` times wider in longitude than in latitude, so that
+    // they are about square on the sphere at the median latitude of the
+    // vertices; near a pole square-in-degrees cells are needles that every
+    // edge crosses by the dozen.  Below an aspect of 2 cells stay square in
+    // degrees.
+    double aspect = 1.0;
+    {
+        // a strided sample of at most 65536 vertices is enough for the median
+        const int stride = std::max(1, P->pv_num / 65536);
+        std::vector<double> alat;
+        alat.reserve(P->pv_num / stride + 1);
+        for (int v = 0; v < P->pv_num; v += stride) alat.push_back(fabs(P->lonlat[2 * v + 1]));
+        if (!alat.empty()) {
+            std::nth_element(alat.begin(), alat.begin() + alat.size() / 2, alat.end());
+            const double a = 1.0 / std::max(cos(std::min(alat[alat.size() / 2], 89.99) * RAD), 1e-9);
+            if (a >= 2.0) aspect = std::min(a, 64.0);
+        }
+    }
+    // cell height (degrees) for about `target` cells, with the padding included
+    double cell = sqrt(std::max(lon_span, 1e-6) * lat_span / ((double)std::max(target, 1LL) * aspect));
     bool full_lon = full, north = false, south = false;
     for (int it = 0; it < 3; it++) {
         const double pad = cell * 1.5;
@@ -1261,7 +1440,7 @@ gahhg_status compute_domain(const Polygon* P, long long target, Geo* G)
         double lspan = 360.0, l0 = -180.0;
         if (!fl) {
             const double maxabs = std::min(89.0, std::max(fabs(la), fabs(lb)));
-            const double padlon = pad / cos(maxabs * RAD);
+            const double padlon = std::max(pad / cos(maxabs * RAD), pad * aspect);
             lspan = lon_span + 2.0 * padlon;
             l0 = lon0 - padlon;
             if (lspan >= 359.0) fl = true;
@@ -1284,13 +1463,14 @@ gahhg_status compute_domain(const Polygon* P, long long target, Geo* G)
         G->lon0 = l0;
         G->lat0 = la;
         lon_span = fl ? 360.0 : lon_span;
-        const double ncell = sqrt(lspan * (lb - la) / (double)std::max(target, 1LL));
+        const double ncell = sqrt(lspan * (lb - la) / ((double)std::max(target, 1LL) * aspect));
         if (it < 2 && fabs(ncell - cell) > 1e-3 * cell) {
             cell = ncell;
             if (!fl) lon0 = lon0;  // unchanged: padding recomputed from the unpadded span
             continue;
         }
-        long long W = std::max(1LL, (long long)ceil(lspan / cell)), H = std::max(1LL, (long long)ceil((lb - la) / cell));
+        long long W = std::max(1LL, (long long)ceil(lspan / (cell * aspect)));
+        long long H = std::max(1LL, (long long)ceil((lb - la) / cell));
         W = std::min(W, 16384LL);
         H = std::min(H, 16384LL);
         if ((long long)W * H >= (long long)INDEX_MASK / 4) {
@@ -1304,6 +1484,9 @@ gahhg_status compute_domain(const Polygon* P, long long target, Geo* G)
         G->full_lon = full_lon;
         G->to_north = north;
         G->to_south = south;
+        // cos(latitude) at the domain's equator-ward edge, rounded up
+        const double la_eq = (la <= 0.0 && lb >= 0.0) ? 0.0 : std::min(fabs(la), fabs(lb));
+        G->cap_cos = std::min(1.0, cos(la_eq * RAD) * (1.0 + 1e-9) + 1e-12);
         break;
     }
     return GAHHG_OK;
@@ -1316,10 +1499,21 @@ gahhg_status lattice_build(Grid* g)
     const int n = P->pv_num;
     Lattice* L = new Lattice();
     g->lattice = L;
+    // GAHHG_DEBUG: wall time of each phase (synchronising) on stderr
+    const bool dbg = getenv("GAHHG_DEBUG") != nullptr;
+    double tph = now_seconds();
+    auto phase = [&](const char* name) {
+        if (!dbg) return;
+        cudaStreamSynchronize(s);
+        const double t = now_seconds();
+        fprintf(stderr, "lattice phase %-12s %9.3f ms\n", name, (t - tph) * 1e3);
+        tph = t;
+    };
 
     long long target = g->opts.lattice_top > 0 ? (long long)g->opts.lattice_top
                                                 : std::min<long long>(std::max<long long>(8LL * n, 1024), 8LL << 20);
     GAHHG_TRY(compute_domain(P, target, &L->geo));
+    phase("domain");
     const int W = L->geo.W, H = L->geo.H;
     L->K = g->opts.lattice_leaf > 0 ? g->opts.lattice_leaf : 8;
     L->maxlev = 9;
@@ -1356,6 +1550,7 @@ gahhg_status lattice_build(Grid* g)
     }
     L->origin_label = label;
 
+    phase("origin");
     std::vector<LevelBuf> lv(1);
     // ---------------- level 0 ----------------
     LevelBuf& l0 = lv[0];
@@ -1366,16 +1561,44 @@ gahhg_status lattice_build(Grid* g)
     GAHHG_TRY(l0.cursor.reserve(l0.nn, s, false));
     GAHHG_CUDA_TRY(cudaMemsetAsync(l0.cnt.ptr, 0, sizeof(int) * l0.nn, s));
     GAHHG_CUDA_TRY(cudaMemsetAsync(l0.cursor.ptr, 0, sizeof(int) * l0.nn, s));
-    k_l0_pairs<0><<<blocks_for(n), TPB, 0, s>>>(bv, l0.cnt.ptr, nullptr, nullptr, nullptr);
-    GAHHG_TRY(scan_state_reserve(&g->scan_state, l0.nn));
+    // candidate boxes split into work items of bounded size, then the pair
+    // tests over the items (count pass, scan, fill pass)
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
+    DevArray<EdgeBox> boxes;
+    DevArray<int> items, item_off;
+    GAHHG_TRY(boxes.reserve(std::max(n, 1), s, false));
+    GAHHG_TRY(items.reserve(std::max(n, 1), s, false));
+    GAHHG_TRY(item_off.reserve(std::max(n, 1), s, false));
+    unsigned long long* d_items64 = reinterpret_cast<unsigned long long*>(g->d_counts + 16);
+    int* d_items = g->d_counts + 18;
+    GAHHG_CUDA_TRY(cudaMemsetAsync(d_items64, 0, sizeof(unsigned long long), s));
+    k_l0_box<<<blocks_for(n), TPB, 0, s>>>(bv, boxes.ptr, items.ptr, d_items64);
+    GAHHG_TRY(scan_state_reserve(&g->scan_state, std::max(n, l0.nn)));
+    GAHHG_TRY(scan_exclusive(items.ptr, item_off.ptr, n, d_items, g->scan_state, g->d_err, s));
+    k_l0_expand<0><<<sms * 8, TPB, 0, s>>>(bv, boxes.ptr, item_off.ptr, d_items, d_items64, l0.cnt.ptr, nullptr,
+                                            nullptr, nullptr);
     GAHHG_TRY(scan_exclusive(l0.cnt.ptr, l0.off.ptr, l0.nn, g->d_counts + 8, g->scan_state, g->d_err, s));
     int total = 0;
+    unsigned long long items64 = 0;
     GAHHG_CUDA_TRY(cudaMemcpyAsync(&total, g->d_counts + 8, sizeof(int), cudaMemcpyDeviceToHost, s));
+    GAHHG_CUDA_TRY(cudaMemcpyAsync(&items64, d_items64, sizeof(items64), cudaMemcpyDeviceToHost, s));
     GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+    if (items64 > (unsigned long long)INT_MAX) {
+        set_error("exact index: %llu level-0 candidate work items exceed 2^31 (fewer top cells are needed)",
+                  items64);
+        return GAHHG_ERR_CAPACITY;
+    }
+    phase("l0 count");
     l0.npairs = total;
     GAHHG_TRY(l0.list.reserve(std::max(total, 1), s, false));
-    k_l0_pairs<1><<<blocks_for(n), TPB, 0, s>>>(bv, l0.cnt.ptr, l0.off.ptr, l0.cursor.ptr, l0.list.ptr);
-    k_sort_lists<<<blocks_for(l0.nn), TPB, 0, s>>>(l0.cnt.ptr, l0.off.ptr, l0.nn, l0.list.ptr);
+    k_l0_expand<1><<<sms * 8, TPB, 0, s>>>(bv, boxes.ptr, item_off.ptr, d_items, d_items64, l0.cnt.ptr, l0.off.ptr,
+                                            l0.cursor.ptr, l0.list.ptr);
+    boxes.release();
+    items.release();
+    item_off.release();
+    GAHHG_TRY(sort_lists(g, l0.cnt.ptr, l0.off.ptr, l0.nn, l0.list.ptr, sms, s));
+    phase("l0 fill");
     GAHHG_TRY(l0.ix.reserve(l0.nn, s, false));
     GAHHG_TRY(l0.iy.reserve(l0.nn, s, false));
     k_l0_coords<<<blocks_for(l0.nn), TPB, 0, s>>>(W, l0.nn, l0.ix.ptr, l0.iy.ptr);
@@ -1424,6 +1647,7 @@ gahhg_status lattice_build(Grid* g)
         hpar.release();
     }
 
+    phase("l0 labels");
     // ---------------- refinement ----------------
     int gnext = l0.nn;
     for (int lvl = 0; lvl < L->maxlev; lvl++) {
@@ -1479,7 +1703,7 @@ gahhg_status lattice_build(Grid* g)
         k_child_pairs<1><<<blocks_for(pp.npairs), TPB, 0, s>>>(bv, lvl, pp.npairs, pp.pair_node.ptr, pp.list.ptr,
                                                                pp.child_base.ptr, pp.ix.ptr, pp.iy.ptr, cl.gstart,
                                                                cl.cnt.ptr, cl.off.ptr, cl.cursor.ptr, cl.list.ptr);
-        k_sort_lists<<<blocks_for(cl.nn), TPB, 0, s>>>(cl.cnt.ptr, cl.off.ptr, cl.nn, cl.list.ptr);
+        GAHHG_TRY(sort_lists(g, cl.cnt.ptr, cl.off.ptr, cl.nn, cl.list.ptr, sms, s));
         // child labels
         DevArray<int> child_parent;
         GAHHG_TRY(child_parent.reserve(cl.nn, s, false));
@@ -1496,6 +1720,7 @@ gahhg_status lattice_build(Grid* g)
     L->nlev = (int)lv.size();
     L->nnodes = gnext;
 
+    phase("refine");
     // ---------------- encode ----------------
     GAHHG_TRY(L->nodes.reserve(L->nnodes, s, false));
     std::vector<int> leaf_base(L->nlev), nleaf(L->nlev);
@@ -1562,6 +1787,7 @@ gahhg_status lattice_build(Grid* g)
     int bad[4];
     GAHHG_CUDA_TRY(cudaMemcpyAsync(bad, d_bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
     GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+    phase("encode");
     for (auto& b : lv) b.release();
     for (int lvl = 0; lvl < L->nlev; lvl++) {
         is_leaf[lvl].release();
