@@ -150,6 +150,39 @@ def device_points(n, seed, device):
     return pts
 
 
+def device_c2_points(rings, n, seed, device):
+    """C2 points on the device: half uniform by area, half on a uniform random
+    edge at a uniform arc parameter, offset along the edge-plane normal by
+    +-10^u rad with u ~ U[-15, -3] (the construction of synth.near_edge_points)."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    ll = torch.as_tensor(np.concatenate(rings), dtype=torch.float64, device=device)
+    starts = np.cumsum([0] + [len(r) for r in rings])
+    nxt = np.arange(len(ll)) + 1
+    for a, b in zip(starts[:-1], starts[1:]):
+        nxt[b - 1] = a
+    nxt = torch.as_tensor(nxt, device=device)
+    lo, la = torch.deg2rad(ll[:, 0]), torch.deg2rad(ll[:, 1])
+    xyz = torch.stack([torch.cos(la) * torch.sin(lo), torch.sin(la), torch.cos(la) * torch.cos(lo)], 1)
+    pts = device_points(n, seed + 1, device)
+    m = n // 2
+    e = torch.randint(0, len(ll), (m,), generator=g, device=device)
+    A, B = xyz[e], xyz[nxt[e]]
+    t = torch.rand((m, 1), generator=g, device=device, dtype=torch.float64)
+    P = (1 - t) * A + t * B
+    P = P / torch.linalg.norm(P, dim=1, keepdim=True)
+    N = torch.linalg.cross(A, B)
+    N = N / torch.clamp(torch.linalg.norm(N, dim=1, keepdim=True), min=1e-300)
+    u = torch.rand(m, generator=g, device=device, dtype=torch.float64) * 12.0 - 15.0
+    sign = torch.where(torch.rand(m, generator=g, device=device) < 0.5, -1.0, 1.0).to(torch.float64)
+    Q = P + (torch.pow(10.0, u) * sign)[:, None] * N
+    Q = Q / torch.linalg.norm(Q, dim=1, keepdim=True)
+    pts[m:, 1] = torch.rad2deg(torch.asin(torch.clamp(Q[:, 1], -1.0, 1.0)))
+    pts[m:, 0] = torch.rad2deg(torch.atan2(Q[:, 0], Q[:, 2]))
+    return pts
+
+
 def timed_loop(fn, steps, stream):
     import torch
     e0 = torch.cuda.Event(enable_timing=True)
@@ -525,7 +558,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per launch of the query kernel from an ncu capture (profiles/)")
-    ap.add_argument("--config", default="c1", choices=["c1", "c3", "c4"])
+    ap.add_argument("--config", default="c1", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--c2-points", type=int, default=20_000_000)
     ap.add_argument("--c3-polygons", type=int, default=4096)
     ap.add_argument("--c3-scale", type=float, default=1.0, help="scale the C3 point counts")
     ap.add_argument("--tune-budget", type=float, default=60.0)
@@ -577,8 +611,12 @@ def main():
     ref_build_wall = time.time() - t0
     st_ref = gref.stats()
 
-    n = args.points
-    pts = device_points(n, 1234 + rank, "cuda:%d" % local)
+    c2 = args.config == "c2"
+    n = args.c2_points if c2 else args.points
+    if c2:
+        pts = device_c2_points(rings, n, 2222 + rank, "cuda:%d" % local)
+    else:
+        pts = device_points(n, 1234 + rank, "cuda:%d" % local)
     labels = torch.empty(n, dtype=torch.uint8, device="cuda:%d" % local)
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
@@ -650,14 +688,20 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from gahhg_b200 import synth
-        sample = synth.uniform_points(args.ref_sample, np.random.default_rng(0))
+        rs = np.random.default_rng(0)
+        if c2:
+            sample = np.concatenate([synth.uniform_points(args.ref_sample // 2, rs),
+                                     synth.near_edge_points(rings, args.ref_sample - args.ref_sample // 2, rs)])
+        else:
+            sample = synth.uniform_points(args.ref_sample, rs)
         threads = os.cpu_count()
         v, info = cpu_reference_rate(rings, sample, threads, args.cpu_budget)
         if v is not None:
             cpu = {"value": round(v, 3), "unit": "Mpts/s", "cores": threads, "kind": "reference",
                    "sample": "reference GAHHG kernels built for the CPU, maxDepth %d, OpenMP %d threads; "
-                             "%d uniform C1 points per pass for %.0f s (%s)" % (
-                                 REF_DEPTH_C1, threads, len(sample), args.cpu_budget, json.dumps(info))}
+                             "%d %s points per pass for %.0f s (%s)" % (
+                                 REF_DEPTH_C1, threads, len(sample), "C2 (half near-edge)" if c2 else "uniform C1",
+                                 args.cpu_budget, json.dumps(info))}
         else:
             cpu = {"value": None, "unit": "Mpts/s", "cores": 0, "kind": "reference", "sample": info}
 
@@ -672,9 +716,13 @@ def main():
         "metric": METRIC, "value": round(rate, 1), "unit": "Mpts/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(per_launch * 1e3, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "C1: 1,000,000-vertex outer ring + 10 x 10,000-vertex holes (1.1M edges), "
+        "config": {"workload": ("C2: the C1 polygon (1.1M edges); %d FP64 points per GPU, half uniform by area, "
+                                "half within 10^U[-15,-3] rad of a random edge; exact labels, FP32 certified filter"
+                                % n) if c2 else
+                               "C1: 1,000,000-vertex outer ring + 10 x 10,000-vertex holes (1.1M edges), "
                                "1e8 uniform FP64 lon/lat points per GPU; exact labels, FP32 certified filter",
-                   "points_per_step": n, "edges": int(P.num_edges), "inputs": "1.6 GB per GPU, larger than L2",
+                   "points_per_step": n, "edges": int(P.num_edges),
+                   "inputs": "%.2f GB per GPU, larger than L2" % (16 * n / 1e9),
                    "parallelism": "replicas" if world > 1 else "single"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
@@ -703,7 +751,10 @@ def main():
                      "process_warmup_c0": round(cold_s * 1e3, 1)},
         "escalation": {"boundary_points": esc["boundary_points"], "fp64_tests": esc["esc_fp64"],
                        "exact_tests": esc["esc_exact"],
-                       "boundary_fraction": round(esc["boundary_points"] / n, 6)},
+                       "boundary_fraction": round(esc["boundary_points"] / n, 6),
+                       "fp32_to_fp64_per_point": esc["esc_fp64"] / n,
+                       "fp32_to_fp64_per_boundary_point": esc["esc_fp64"] / max(esc["boundary_points"], 1),
+                       "fp64_to_exact_per_point": esc["esc_exact"] / n},
         "inside_fraction": round(inside / n, 6),
         "lattice_bytes": st_build["lattice_bytes"],
     }

@@ -39,6 +39,7 @@ struct gahhg_batch {
     DevArray<uint32_t> g_queue;
     DevArray<unsigned int> g_counters;
     int g_nchunks = 0;
+    long long g_qcap = 0;
     cudaStream_t owner_stream = nullptr;  // stream for workspace allocations
 
     ~gahhg_batch()
@@ -279,8 +280,9 @@ gahhg_status gahhg_batch_query_device(gahhg_batch* b, const double* d_lonlat, co
     unsigned int* counters = nullptr;
     uint64_t* d_stats = nullptr;
     GAHHG_TRY(pool_alloc(&d_chunks, std::max<size_t>(chunks.size(), 16), b->device, s));
-    GAHHG_TRY(pool_alloc((void**)&queue, sizeof(uint32_t) * std::max<long long>(total, 1), b->device, s));
-    GAHHG_TRY(pool_alloc((void**)&counters, 4 * sizeof(unsigned int), b->device, s));
+    const long long qcap = std::max<long long>(total, 1);
+    GAHHG_TRY(pool_alloc((void**)&queue, sizeof(uint32_t) * batch_queue_words(qcap), b->device, s));
+    GAHHG_TRY(pool_alloc((void**)&counters, 8 * sizeof(unsigned int), b->device, s));
     if (!chunks.empty())
         GAHHG_CUDA_TRY(cudaMemcpyAsync(d_chunks, chunks.data(), chunks.size(), cudaMemcpyHostToDevice, s));
     if (sync) {
@@ -294,7 +296,7 @@ gahhg_status gahhg_batch_query_device(gahhg_batch* b, const double* d_lonlat, co
         cudaEventRecord(e0, s);
     }
     gahhg_status st = batch_query_launch(b->views.ptr, d_chunks, nchunks, d_lonlat, d_labels, precision, queue,
-                                         counters, d_stats, s, b->device);
+                                         qcap, counters, d_stats, s, b->device);
     if (sync && st == GAHHG_OK) {
         cudaEventRecord(e1, s);
         uint64_t c[4] = {0, 0, 0, 0};
@@ -350,8 +352,9 @@ gahhg_status gahhg_batch_query_graph(gahhg_batch* b, const double* d_lonlat, con
         batch_make_chunks((const long long*)offsets, b->count, b->chunk_points, b->swords.data(), nullptr, chunks,
                           &b->g_nchunks);
         GAHHG_TRY(b->g_chunks.reserve(std::max<size_t>(chunks.size(), 16), ws, false));
-        GAHHG_TRY(b->g_queue.reserve(std::max<long long>(total, 1), ws, false));
-        GAHHG_TRY(b->g_counters.reserve(4, ws, false));
+        b->g_qcap = std::max<long long>(total, 1);
+        GAHHG_TRY(b->g_queue.reserve(batch_queue_words(b->g_qcap), ws, false));
+        GAHHG_TRY(b->g_counters.reserve(8, ws, false));
         if (!chunks.empty())
             GAHHG_CUDA_TRY(cudaMemcpyAsync(b->g_chunks.ptr, chunks.data(), chunks.size(), cudaMemcpyHostToDevice, ws));
         GAHHG_CUDA_TRY(cudaStreamSynchronize(ws));
@@ -363,7 +366,7 @@ gahhg_status gahhg_batch_query_graph(gahhg_batch* b, const double* d_lonlat, con
             st = GAHHG_ERR_CUDA;
         } else {
             st = batch_query_launch(b->views.ptr, b->g_chunks.ptr, b->g_nchunks, d_lonlat, d_labels, precision,
-                                    b->g_queue.ptr, b->g_counters.ptr, nullptr, cs, b->device);
+                                    b->g_queue.ptr, b->g_qcap, b->g_counters.ptr, nullptr, cs, b->device);
             if (cudaStreamEndCapture(cs, &graph) != cudaSuccess) st = GAHHG_ERR_CUDA;
         }
         cudaStreamDestroy(cs);

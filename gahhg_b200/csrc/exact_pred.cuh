@@ -186,6 +186,28 @@ XHD int orient_fp64(const double* a, const double* b, const double* c)
     return 0;
 }
 
+// Stage 1 for b and c close to a: det[a; b; c] = det[a; b - a; c - a] (row
+// operations leave the determinant unchanged), evaluated on the rounded
+// differences.  This is Shewchuk's orient3d(O, b, c, a) stage A up to sign:
+// its bound (7 + 56 eps) eps x permanent(rows) covers the rounding of the
+// differences, and the permanent shrinks with |b - a| |c - a|, so points far
+// closer to an edge than orient_fp64 can resolve are still decided.
+XHD int orient_fp64_near(const double* a, const double* b, const double* c)
+{
+    const double ux = b[0] - a[0], uy = b[1] - a[1], uz = b[2] - a[2];
+    const double vx = c[0] - a[0], vy = c[1] - a[1], vz = c[2] - a[2];
+    const double m0 = uy * vz - uz * vy;
+    const double m1 = uz * vx - ux * vz;
+    const double m2 = ux * vy - uy * vx;
+    const double d = a[0] * m0 + a[1] * m1 + a[2] * m2;
+    const double perm = fabs(a[0]) * (fabs(uy * vz) + fabs(uz * vy)) + fabs(a[1]) * (fabs(uz * vx) + fabs(ux * vz)) +
+                        fabs(a[2]) * (fabs(ux * vy) + fabs(uy * vx));
+    const double bound = (7.0 + 56.0 * EPS53) * EPS53 * perm;
+    if (d > bound) return 1;
+    if (d < -bound) return -1;
+    return 0;
+}
+
 // Stages 2 and 3.
 XHDN int orient_exact(const double* a, const double* b, const double* c)
 {

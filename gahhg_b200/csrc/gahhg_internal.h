@@ -212,10 +212,14 @@ void batch_make_chunks(const long long* offsets, int nseg, int chunk_points, con
 void batch_write_chunks(const long long* offsets, int nseg, int chunk_points, const int* swords, const int* seg_view,
                         void* out, int* nchunks);
 size_t batch_chunk_count_bound(long long points, int nseg, int chunk_points);
-// counters[0..1] must be zero on entry unless zero_counters is set.
+// Words of a batch queue whose pass-2 part holds queue_cap points (the
+// escalation queues follow it).
+size_t batch_queue_words(long long queue_cap);
+// counters[0..4] must be zero on entry unless zero_counters is set.
 gahhg_status batch_query_launch(const void* d_views, const void* d_chunks, int nchunks, const double* d_lonlat,
-                                uint8_t* d_labels, int precision, uint32_t* queue, unsigned int* counters,
-                                uint64_t* d_stats, cudaStream_t s, int device, bool zero_counters = true);
+                                uint8_t* d_labels, int precision, uint32_t* queue, long long queue_cap,
+                                unsigned int* counters, uint64_t* d_stats, cudaStream_t s, int device,
+                                bool zero_counters = true);
 size_t lattice_bytes(const Lattice* L);
 size_t lattice_device_bytes(const Lattice* L);  // capacity held on the device
 

@@ -896,6 +896,72 @@ __device__ uint8_t leaf_label(const QueryView& Q, uint32_t leaf, PointCtx& P, bo
     return (uint8_t)(par ? 3 - L.label : L.label);
 }
 
+// ------------------------------------------------------ escalation tiers --
+//
+// The crossing tests of the queued points run in tiers, each its own launch
+// over the points the previous tier could not decide, so that no warp carries
+// the registers or waits on the branches of a rarer, costlier tier:
+//   tier 1: every sign from the certified FP32 filter (no FP64 code at all);
+//   tier 2: the canonical FP64 point, the vertex and center rules, and every
+//           sign from the FP64 filter on translated rows (orient_fp64_near);
+//   tier 3: the complete test (FP64 filter, then exact arithmetic with
+//           simulation of simplicity), leaf_label above.
+// Every sign a tier returns is exact, so a label does not depend on the tier
+// that produced it.
+constexpr uint8_t LABEL_DEFER = 0xFF;
+
+__device__ uint8_t leaf_label_fp32(const QueryView& Q, uint32_t leaf, const PointCtx& P)
+{
+    const LeafRec L = Q.leaves[leaf];
+    float sa, ca, so, co;
+    // arguments stay inside [-pi, pi], where __sincosf's error bound is documented
+    __sincosf((float)gahhg_canon_rad(P.lat_r), &sa, &ca);
+    __sincosf((float)gahhg_canon_rad(P.lon_r), &so, &co);
+    const float qx = ca * so, qy = sa, qz = ca * co;
+    int par = 0;
+    for (int k = 0; k < L.cnt; k++) {
+        const EdgeRec r = Q.recs[L.off + k];
+        const int s1 = (r.es >> 31) ? 1 : -1;
+        const int s2 = sign32(r.n1, qx, qy, qz);
+        if (s2 == 0) return LABEL_DEFER;
+        if (s2 == s1) continue;
+        const int s3 = sign32(r.n2, qx, qy, qz);
+        if (s3 == 0) return LABEL_DEFER;
+        if (s3 != s2) continue;
+        const int s4 = sign32(r.n3, qx, qy, qz);
+        if (s4 == 0) return LABEL_DEFER;
+        if (s4 == -s2) par ^= 1;
+    }
+    return (uint8_t)(par ? 3 - L.label : L.label);
+}
+
+__device__ uint8_t leaf_label_fp64(const QueryView& Q, uint32_t leaf, PointCtx& P)
+{
+    const LeafRec L = Q.leaves[leaf];
+    P.need64();
+    int par = 0;
+    for (int k = 0; k < L.cnt; k++) {
+        const EdgeRec r = Q.recs[L.off + k];
+        const int e = (int)(r.es & 0x7fffffffu);
+        const int s1 = (r.es >> 31) ? 1 : -1;
+        const D3 a = Q.pv[Q.pe[2 * e]], b = Q.pv[Q.pe[2 * e + 1]];
+        const double A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z};
+        if (exact::same(P.q, A) || exact::same(P.q, B)) return CELL_IN;  // vertex rule
+        if (exact::same(P.q, L.R)) return L.label;                       // q is the center
+        // every row is within a cap of the first: translated rows keep the bound small
+        const int s2 = exact::orient_fp64_near(A, B, P.q);
+        if (s2 == 0) return LABEL_DEFER;
+        if (s2 == s1) continue;
+        const int s3 = exact::orient_fp64_near(L.R, P.q, A);
+        if (s3 == 0) return LABEL_DEFER;
+        if (s3 != s2) continue;
+        const int s4 = exact::orient_fp64_near(L.R, P.q, B);
+        if (s4 == 0) return LABEL_DEFER;
+        if (s4 == -s2) par ^= 1;
+    }
+    return (uint8_t)(par ? 3 - L.label : L.label);
+}
+
 // Level-0 cell of a point from its longitude and FakeLL latitude + 90
 // (`laf`); false when the point lies outside the domain.
 struct Loc {
@@ -1065,11 +1131,10 @@ __global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, 
     if (STATS && ctr) count_inside(inside, ctr + 3);
 }
 
-// Pass 2 for one queued point.
-template <bool FP32>
-__device__ __forceinline__ uint8_t leaf_point(const QueryView& Q, double2 p, unsigned long long* ctr)
+// The leaf of a queued point (the point context filled in), or its label
+// with KIND_PURE when its cell has no edges.
+__device__ __forceinline__ uint32_t point_leaf(const QueryView& Q, double2 p, PointCtx& P)
 {
-    PointCtx P;
     P.lat = gahhg_canon_query_lat(p.y);
     P.lon = p.x;
     P.have64 = false;
@@ -1089,7 +1154,15 @@ __device__ __forceinline__ uint8_t leaf_point(const QueryView& Q, double2 p, uns
     P.lon_r = lr;
     P.lat_r = la;
     const bool in = domain_locate(Q, lo, la + 90.0, L);
-    const uint32_t w = in ? descend(Q, __ldg(Q.nodes + (size_t)L.iy * Q.W + L.ix), L.fu, L.fv) : Q.outside;
+    return in ? descend(Q, __ldg(Q.nodes + (size_t)L.iy * Q.W + L.ix), L.fu, L.fv) : Q.outside;
+}
+
+// One point through the untiered path (escalations inline, counted per test).
+template <bool FP32>
+__device__ __forceinline__ uint8_t leaf_point(const QueryView& Q, double2 p, unsigned long long* ctr)
+{
+    PointCtx P;
+    const uint32_t w = point_leaf(Q, p, P);
     if ((w & KIND_MASK) == KIND_PURE) return (uint8_t)(w & 3u);
     if (ctr) atomicAdd(ctr + 2, 1ull);
     return leaf_label(Q, w & INDEX_MASK, P, FP32, ctr);
@@ -1153,30 +1226,196 @@ __global__ void __launch_bounds__(TPB) k_batch_locate(const QueryView* __restric
     if (STATS && ctr) count_inside(inside, ctr + 3);
 }
 
-// Pass 2 over a batch: the view of a queued point by binary search of the
-// chunk starts (the chunk table stays in L1/L2).
-template <bool FP32>
-__global__ void __launch_bounds__(TPB) k_batch_leaf(const QueryView* __restrict__ views,
-                                                   const BatchChunk* __restrict__ chunks, int nchunks,
-                                                   const double2* __restrict__ ll, uint8_t* __restrict__ out,
-                                                   const uint32_t* __restrict__ queue,
-                                                   const unsigned int* __restrict__ qcount, unsigned long long* ctr)
-{
-    const unsigned int m = *qcount;
-    int inside = 0;
-    for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
-        const uint32_t i = queue[t];
+// Escalation queues of one pass-2 run.  cnt[0] / cnt[1] count the points
+// deferred to tier 2 / tier 3 (they keep counting past the capacities);
+// cnt[2] is raised when a point found its queue full: it stays unlabelled
+// (pass 1 wrote LABEL_PENDING) and the final sweep gives it the complete
+// test, so no tier carries the code of the tiers after it.
+struct Tiers {
+    uint32_t* q2;
+    uint32_t* q3;
+    unsigned int* cnt;
+    unsigned int cap2, cap3;
+};
+
+// Where a queued point's index view comes from: one polygon...
+struct OneView {
+    QueryView Q;
+    __device__ __forceinline__ const QueryView& of(uint32_t) const { return Q; }
+};
+
+// ...or the chunk holding it (binary search of the chunk starts).
+struct ChunkViews {
+    const QueryView* views;
+    const BatchChunk* chunks;
+    int nchunks;
+    __device__ __forceinline__ const QueryView& of(uint32_t i) const
+    {
         int lo = 0, hi = nchunks;  // chunks[lo].start <= i < chunks[hi].start
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
             if (__ldg(&chunks[mid].start) <= (long long)i) lo = mid;
             else hi = mid;
         }
-        const uint8_t lab = leaf_point<FP32>(views[__ldg(&chunks[lo].view)], ll[i], ctr);
+        return views[__ldg(&chunks[lo].view)];
+    }
+};
+
+// Appends i to q through counter *c, one atomic per group of converged
+// threads; false when the queue is full.
+__device__ __forceinline__ bool push_deferred(uint32_t i, uint32_t* q, unsigned int* c, unsigned int cap)
+{
+    const unsigned int act = __activemask();
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(act) - 1;
+    unsigned int base = 0;
+    if (lane == leader) base = atomicAdd(c, (unsigned int)__popc(act));
+    base = __shfl_sync(act, base, leader);
+    const unsigned int pos = base + __popc(act & ((1u << lane) - 1u));
+    if (pos >= cap) return false;
+    q[pos] = i;
+    return true;
+}
+
+__device__ __forceinline__ void count_stats(unsigned long long* ctr, int inside, int boundary, int fp64, int exact)
+{
+    count_inside(inside, ctr + 3);
+    count_inside(boundary, ctr + 2);
+    count_inside(fp64, ctr + 0);
+    count_inside(exact, ctr + 1);
+}
+
+// Tier 1 over the pass-1 queue.
+template <class VS>
+__global__ void __launch_bounds__(TPB) k_leaf_t1(VS vs, const double2* __restrict__ ll, uint8_t* __restrict__ out,
+                                                const uint32_t* __restrict__ queue,
+                                                const unsigned int* __restrict__ qcount, Tiers T,
+                                                unsigned long long* ctr)
+{
+    const unsigned int m = *qcount;
+    int inside = 0, boundary = 0, fp64 = 0;
+    for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+        const uint32_t i = queue[t];
+        const QueryView& Q = vs.of(i);
+        PointCtx P;
+        const uint32_t w = point_leaf(Q, ll[i], P);
+        uint8_t lab;
+        if ((w & KIND_MASK) == KIND_PURE) {
+            lab = (uint8_t)(w & 3u);
+        } else {
+            boundary++;
+            lab = leaf_label_fp32(Q, w & INDEX_MASK, P);
+            if (lab == LABEL_DEFER) {
+                fp64++;
+                if (!push_deferred(i, T.q2, T.cnt, T.cap2)) T.cnt[2] = 1;
+                continue;
+            }
+        }
+        out[i] = lab;
+        inside += lab == CELL_IN;
+    }
+    if (ctr) count_stats(ctr, inside, boundary, fp64, 0);
+}
+
+// Tier 2 over the tier-1 queue, or (FROM_PASS1, FP64-filter queries) over
+// the pass-1 queue itself.
+template <class VS, bool FROM_PASS1>
+__global__ void __launch_bounds__(TPB) k_leaf_t2(VS vs, const double2* __restrict__ ll, uint8_t* __restrict__ out,
+                                                const uint32_t* __restrict__ src,
+                                                const unsigned int* __restrict__ src_count, unsigned int src_cap,
+                                                Tiers T, unsigned long long* ctr)
+{
+    const unsigned int m = min(*src_count, src_cap);
+    int inside = 0, boundary = 0, exact = 0;
+    for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+        const uint32_t i = src[t];
+        const QueryView& Q = vs.of(i);
+        PointCtx P;
+        const uint32_t w = point_leaf(Q, ll[i], P);
+        uint8_t lab;
+        if ((w & KIND_MASK) == KIND_PURE) {
+            lab = (uint8_t)(w & 3u);
+        } else {
+            if (FROM_PASS1) boundary++;
+            lab = leaf_label_fp64(Q, w & INDEX_MASK, P);
+            if (lab == LABEL_DEFER) {
+                exact++;
+                if (!push_deferred(i, T.q3, T.cnt + 1, T.cap3)) T.cnt[2] = 1;
+                continue;
+            }
+        }
+        out[i] = lab;
+        inside += lab == CELL_IN;
+    }
+    if (ctr) count_stats(ctr, inside, boundary, 0, exact);
+}
+
+// Tier 3 over the tier-2 queue.
+template <class VS>
+__global__ void __launch_bounds__(TPB) k_leaf_t3(VS vs, const double2* __restrict__ ll, uint8_t* __restrict__ out,
+                                                Tiers T, unsigned long long* ctr)
+{
+    const unsigned int m = min(T.cnt[1], T.cap3);
+    int inside = 0;
+    for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+        const uint32_t i = T.q3[t];
+        const QueryView& Q = vs.of(i);
+        PointCtx P;
+        const uint32_t w = point_leaf(Q, ll[i], P);
+        const uint8_t lab = ((w & KIND_MASK) == KIND_PURE) ? (uint8_t)(w & 3u)
+                                                            : leaf_label(Q, w & INDEX_MASK, P, false, nullptr);
         out[i] = lab;
         inside += lab == CELL_IN;
     }
     if (ctr) count_inside(inside, ctr + 3);
+}
+
+// After a queue overflow: the complete test for every pass-1 point still
+// unlabelled.
+template <class VS>
+__global__ void __launch_bounds__(TPB) k_leaf_sweep(VS vs, const double2* __restrict__ ll, uint8_t* __restrict__ out,
+                                                   const uint32_t* __restrict__ queue,
+                                                   const unsigned int* __restrict__ qcount, Tiers T,
+                                                   unsigned long long* ctr)
+{
+    if (T.cnt[2] == 0) return;
+    const unsigned int m = *qcount;
+    int inside = 0;
+    for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+        const uint32_t i = queue[t];
+        if (out[i] != LABEL_PENDING) continue;
+        const QueryView& Q = vs.of(i);
+        PointCtx P;
+        const uint32_t w = point_leaf(Q, ll[i], P);
+        const uint8_t lab = ((w & KIND_MASK) == KIND_PURE) ? (uint8_t)(w & 3u)
+                                                            : leaf_label(Q, w & INDEX_MASK, P, false, nullptr);
+        out[i] = lab;
+        inside += lab == CELL_IN;
+    }
+    if (ctr) count_inside(inside, ctr + 3);
+}
+
+// Tier counters (T.cnt[0..2]) must be zero.
+template <class VS>
+void leaf_tiers_launch(const VS& vs, const double2* ll, uint8_t* out, const uint32_t* queue,
+                       const unsigned int* qcount, const Tiers& T, int precision, unsigned long long* ctr, int sms,
+                       cudaStream_t s)
+{
+    if (precision == GAHHG_QUERY_FP64_FILTER) {
+        k_leaf_t2<VS, true><<<sms * 4, TPB, 0, s>>>(vs, ll, out, queue, qcount, 0xffffffffu, T, ctr);
+    } else {
+        k_leaf_t1<VS><<<sms * 4, TPB, 0, s>>>(vs, ll, out, queue, qcount, T, ctr);
+        k_leaf_t2<VS, false><<<sms * 4, TPB, 0, s>>>(vs, ll, out, T.q2, T.cnt, T.cap2, T, ctr);
+    }
+    k_leaf_t3<VS><<<sms * 2, TPB, 0, s>>>(vs, ll, out, T, ctr);
+    k_leaf_sweep<VS><<<sms * 2, TPB, 0, s>>>(vs, ll, out, queue, qcount, T, ctr);
+}
+
+// Escalation queue capacities for a pass-2 queue of `points` entries.
+inline void tier_caps(long long points, unsigned int* cap2, unsigned int* cap3)
+{
+    *cap2 = (unsigned int)(points / 2 + 1024);
+    *cap3 = (unsigned int)(points / 8 + 1024);
 }
 
 }  // namespace
@@ -1806,7 +2045,7 @@ gahhg_status lattice_build(Grid* g)
 
 gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long long n, uint8_t* d_labels,
                                 int precision, cudaStream_t s, uint64_t* d_counters, uint32_t* queue,
-                                unsigned int* qcount, long long chunk, int device);
+                                unsigned int* qcount, long long chunk, int device, const Tiers* tiers);
 
 QueryView make_view(const Grid* g)
 {
@@ -1846,18 +2085,29 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
     if (n == 0) return GAHHG_OK;
     const QueryView Q = make_view(g);
     const long long chunk = std::min<long long>((long long)n, QUERY_CHUNK);
+    // [pass-2 queue][counters: queue fill, tier-2 fill, tier-3 fill, overflow][tier-2 queue][tier-3 queue]
+    unsigned int cap2 = 0, cap3 = 0;
+    tier_caps(chunk, &cap2, &cap3);
     uint32_t* queue = nullptr;
-    GAHHG_TRY(pool_alloc((void**)&queue, sizeof(uint32_t) * (chunk + 64), g->device, s));
+    GAHHG_TRY(pool_alloc((void**)&queue, sizeof(uint32_t) * (chunk + 64 + (size_t)cap2 + cap3), g->device, s));
     unsigned int* qcount = (unsigned int*)(queue + chunk + 32);
+    Tiers T;
+    T.cnt = qcount + 1;
+    T.q2 = queue + chunk + 64;
+    T.q3 = T.q2 + cap2;
+    T.cap2 = cap2;
+    T.cap3 = cap3;
     const gahhg_status st = lattice_query_with(Q, d_lonlat, (long long)n, d_labels, precision, s, d_counters,
-                                               queue, qcount, chunk, g->device);
+                                               queue, qcount, chunk, g->device, &T);
     cudaFreeAsync(queue, s);
     return st;
 }
 
+// tiers == nullptr: one pass-2 launch with escalations inline (no queues
+// beyond the pass-2 queue); else qcount[1..3] are the tier counters.
 gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long long n, uint8_t* d_labels,
                                 int precision, cudaStream_t s, uint64_t* d_counters, uint32_t* queue,
-                                unsigned int* qcount, long long chunk, int device)
+                                unsigned int* qcount, long long chunk, int device, const Tiers* tiers)
 {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -1865,14 +2115,16 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
     for (long long off = 0; off < n; off += chunk) {
         const int m = (int)std::min<long long>(chunk, n - off);
         const double2* ll = (const double2*)d_lonlat + off;
-        GAHHG_CUDA_TRY(cudaMemsetAsync(qcount, 0, sizeof(unsigned int), s));
+        GAHHG_CUDA_TRY(cudaMemsetAsync(qcount, 0, sizeof(unsigned int) * (tiers ? 4 : 1), s));
         const long long tiles = ((long long)m + TPB * LOC_UNROLL - 1) / (TPB * LOC_UNROLL);
         const int grid = (int)std::min<long long>(tiles, (long long)sms * 8);
         if (ctr)
             k_locate<true><<<grid, TPB, sizeof(uint32_t) * Q.swords, s>>>(ll, m, d_labels + off, Q, queue, qcount, ctr);
         else
             k_locate<false><<<grid, TPB, sizeof(uint32_t) * Q.swords, s>>>(ll, m, d_labels + off, Q, queue, qcount, ctr);
-        if (precision == GAHHG_QUERY_FP64_FILTER)
+        if (tiers)
+            leaf_tiers_launch(OneView{Q}, ll, d_labels + off, queue, qcount, *tiers, precision, ctr, sms, s);
+        else if (precision == GAHHG_QUERY_FP64_FILTER)
             k_leaf<false><<<sms * 4, TPB, 0, s>>>(ll, d_labels + off, Q, queue, qcount, ctr);
         else
             k_leaf<true><<<sms * 4, TPB, 0, s>>>(ll, d_labels + off, Q, queue, qcount, ctr);
@@ -1934,7 +2186,7 @@ gahhg_status lattice_query_noalloc(Grid* g, const double* d_lonlat, size_t n, ui
     // the queue count lives after the queue; lattice_query_with zeroes it before each pass
     unsigned int* qcount = (unsigned int*)(queue + NOALLOC_MAX_POINTS + 32);
     return lattice_query_with(Q, d_lonlat, (long long)n, d_labels, precision, s, nullptr, queue, qcount,
-                              NOALLOC_MAX_POINTS, g->device);
+                              NOALLOC_MAX_POINTS, g->device, nullptr);
 }
 
 // ------------------------------------------------------- batch launcher --
@@ -1986,11 +2238,21 @@ void batch_make_chunks(const long long* offsets, int nseg, int chunk_points, con
     batch_write_chunks(offsets, nseg, chunk_points, swords, seg_view, out.data(), nchunks);
 }
 
-// counters: [0] queue count, [1] next chunk.  Everything is enqueued on `s`
-// (no allocation, no host synchronisation), so it can be captured in a graph.
+size_t batch_queue_words(long long queue_cap)
+{
+    unsigned int cap2 = 0, cap3 = 0;
+    tier_caps(queue_cap, &cap2, &cap3);
+    return (size_t)queue_cap + cap2 + cap3;
+}
+
+// counters: [0] queue count, [1] next chunk, [2..4] tier counters.  The
+// queue holds batch_queue_words(queue_cap) words: the pass-2 queue, then the
+// escalation queues.  Everything is enqueued on `s` (no allocation, no host
+// synchronisation), so it can be captured in a graph.
 gahhg_status batch_query_launch(const void* d_views, const void* d_chunks, int nchunks, const double* d_lonlat,
-                                uint8_t* d_labels, int precision, uint32_t* queue, unsigned int* counters,
-                                uint64_t* d_stats, cudaStream_t s, int device, bool zero_counters)
+                                uint8_t* d_labels, int precision, uint32_t* queue, long long queue_cap,
+                                unsigned int* counters, uint64_t* d_stats, cudaStream_t s, int device,
+                                bool zero_counters)
 {
     if (nchunks == 0) return GAHHG_OK;
     static std::atomic<int> sms_cache[64];
@@ -2003,7 +2265,7 @@ gahhg_status batch_query_launch(const void* d_views, const void* d_chunks, int n
     const QueryView* views = (const QueryView*)d_views;
     const BatchChunk* chunks = (const BatchChunk*)d_chunks;
     unsigned long long* ctr = (unsigned long long*)d_stats;
-    if (zero_counters) GAHHG_CUDA_TRY(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned int), s));
+    if (zero_counters) GAHHG_CUDA_TRY(cudaMemsetAsync(counters, 0, 5 * sizeof(unsigned int), s));
     const int grid = std::min(nchunks, sms * 8);
     if (ctr)
         k_batch_locate<true><<<grid, TPB, 0, s>>>(views, chunks, nchunks, counters + 1, (const double2*)d_lonlat,
@@ -2011,12 +2273,13 @@ gahhg_status batch_query_launch(const void* d_views, const void* d_chunks, int n
     else
         k_batch_locate<false><<<grid, TPB, 0, s>>>(views, chunks, nchunks, counters + 1, (const double2*)d_lonlat,
                                                    d_labels, queue, counters, ctr);
-    if (precision == GAHHG_QUERY_FP64_FILTER)
-        k_batch_leaf<false><<<sms * 4, TPB, 0, s>>>(views, chunks, nchunks, (const double2*)d_lonlat, d_labels,
-                                                    queue, counters, ctr);
-    else
-        k_batch_leaf<true><<<sms * 4, TPB, 0, s>>>(views, chunks, nchunks, (const double2*)d_lonlat, d_labels,
-                                                   queue, counters, ctr);
+    Tiers T;
+    tier_caps(queue_cap, &T.cap2, &T.cap3);
+    T.q2 = queue + queue_cap;
+    T.q3 = T.q2 + T.cap2;
+    T.cnt = counters + 2;
+    leaf_tiers_launch(ChunkViews{views, chunks, nchunks}, (const double2*)d_lonlat, d_labels, queue, counters, T,
+                      precision, ctr, sms, s);
     GAHHG_CUDA_TRY(cudaGetLastError());
     return GAHHG_OK;
 }

@@ -49,7 +49,7 @@ using namespace gahhg;
 
 namespace {
 
-constexpr size_t HDR_BYTES = 64;  // [u32 queue count, u32 next chunk, pad][u64 stats x4 at +32]
+constexpr size_t HDR_BYTES = 64;  // [u32 queue count, next chunk, tier counters x3][u64 stats x4 at +32]
 constexpr size_t CHUNK_BYTES = 16;
 constexpr int MAX_SUMMARY_WORDS = 4096;  // the batch kernel stages at most 16 KB of summary
 constexpr size_t MAX_TRACE = 1 << 20;
@@ -320,7 +320,8 @@ struct gahhg_server {
         // labels end where the header starts, so one copy brings both back
         uint8_t* d_labels = sl->d + lcap - (size_t)sl->points;
         GAHHG_TRY(batch_query_launch(d_views, din + HDR_BYTES, nchunks, (const double*)(din + pts_off), d_labels,
-                                     o.precision, sl->d_queue, (unsigned int*)din, (uint64_t*)(din + 32), sl->s,
+                                     o.precision, sl->d_queue, o.slot_points, (unsigned int*)din,
+                                     (uint64_t*)(din + 32), sl->s,
                                      o.device, false));
         GAHHG_CUDA_TRY(cudaMemcpyAsync(sl->h + lcap - (size_t)sl->points, d_labels, (size_t)sl->points + HDR_BYTES,
                                        cudaMemcpyDeviceToHost, sl->s));
@@ -563,7 +564,7 @@ struct gahhg_server {
             GAHHG_CUDA_TRY(cudaEventCreate(&s.ev));
             GAHHG_CUDA_TRY(cudaHostAlloc((void**)&s.h, lcap + in_bytes, cudaHostAllocDefault));
             GAHHG_CUDA_TRY(cudaMalloc((void**)&s.d, lcap + in_bytes));
-            GAHHG_CUDA_TRY(cudaMalloc((void**)&s.d_queue, sizeof(uint32_t) * (size_t)o.slot_points));
+            GAHHG_CUDA_TRY(cudaMalloc((void**)&s.d_queue, sizeof(uint32_t) * batch_queue_words(o.slot_points)));
         }
         GAHHG_TRY(workers.create(o.device, o.build_workers, lo));
         if (o.hbm_budget <= 0) {
