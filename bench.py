@@ -584,9 +584,8 @@ def main():
 
     import torch
     import torch.distributed as dist
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from gahhg_b200 import replicas
+    rank, world, local = replicas.world()
     torch.cuda.set_device(local)
     if world > 1:
         from datetime import timedelta
@@ -639,21 +638,16 @@ def main():
     for _ in range(args.warmup):
         q32()
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     t = timed_loop(q32, args.steps, stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    if world > 1:
-        tt = torch.tensor([t], device="cuda:%d" % local, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t = float(tt.item())
+    t = replicas.max_over_ranks(t, "cuda:%d" % local)
     rate = world * n * args.steps / t / 1e6
     per_launch = t / args.steps
 
@@ -679,10 +673,7 @@ def main():
     for _ in range(args.e2e_steps):
         G.check(L.gahhg_query(g._h, hp, e2e_n, hl, G.QUERY_FP32_FILTER))
     te = (time.perf_counter() - te) / args.e2e_steps
-    if world > 1:
-        tt = torch.tensor([te], device="cuda:%d" % local, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        te = float(tt.item())
+    te = replicas.max_over_ranks(te, "cuda:%d" % local)
     e2e_rate = world * e2e_n / te / 1e6
 
     cpu = None
