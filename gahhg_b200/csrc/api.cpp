@@ -150,6 +150,7 @@ Grid::~Grid()
     if (h_counts) cudaFreeHost(h_counts);
     free_query_layout(qlayout);
     lattice_free(lattice);
+    if (aux_stream) cudaStreamDestroy(aux_stream);
     if (!borrowed) {
         scan_state_destroy(scan_state);
         if (stream) cudaStreamDestroy(stream);
@@ -401,32 +402,89 @@ gahhg_status gahhg_query_device_noalloc(gahhg_grid* G, const double* d_lonlat, s
 
 long long gahhg_query_noalloc_max_points(void) { return lattice_noalloc_max_points(); }
 
+// Host buffers: chunks of E2E_CHUNK points alternate between the grid's
+// stream and an auxiliary one, each chunk copied in, queried and copied out
+// on its stream, so one chunk's host-to-device copy overlaps the previous
+// chunk's query and device-to-host copy (the copy engines run both
+// directions at once).  Device memory: two chunk buffers.  query_s sums the
+// device time of the query launches alone, like the reference's PISPTime.
+static constexpr size_t E2E_CHUNK = (size_t)1 << 23;
+
 gahhg_status gahhg_query(gahhg_grid* G, const double* lonlat, size_t n, uint8_t* labels, int precision)
 {
     if (!G || (n && (!lonlat || !labels))) return GAHHG_ERR_ARG;
     Grid* g = &G->g;
-    GAHHG_CUDA_TRY(cudaSetDevice(g->device));
-    cudaStream_t s = g->stream;
-    double* d_ll = nullptr;
-    uint8_t* d_lab = nullptr;
-    if (n) {
-        GAHHG_TRY(pool_alloc((void**)&d_ll, n * 2 * sizeof(double), g->device, s));
-        GAHHG_TRY(pool_alloc((void**)&d_lab, n, g->device, s));
-        GAHHG_CUDA_TRY(cudaMemcpyAsync(d_ll, lonlat, n * 2 * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (!g->classified) {
+        set_error("query before classify");
+        return GAHHG_ERR_STATE;
     }
-    gahhg_status st = gahhg_query_device(G, d_ll, n, d_lab, precision, s, 1);
-    if (st == GAHHG_OK && n) {
-        cudaError_t e = cudaMemcpyAsync(labels, d_lab, n, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) {
-            set_error("query copy-out: %s", cudaGetErrorString(e));
-            st = GAHHG_ERR_CUDA;
+    GAHHG_CUDA_TRY(cudaSetDevice(g->device));
+    if (n == 0) return GAHHG_OK;
+    if (!g->aux_stream) GAHHG_CUDA_TRY(cudaStreamCreateWithFlags(&g->aux_stream, cudaStreamNonBlocking));
+    cudaStream_t st[2] = {g->stream, g->aux_stream};
+    const size_t chunk = std::min(n, E2E_CHUNK);
+    const size_t nchunks = (n + chunk - 1) / chunk;
+    uint8_t* buf[2] = {nullptr, nullptr};
+    uint64_t* d_cnt = nullptr;
+    GAHHG_TRY(pool_alloc((void**)&d_cnt, 4 * sizeof(uint64_t), g->device, st[0]));
+    GAHHG_CUDA_TRY(cudaMemsetAsync(d_cnt, 0, 4 * sizeof(uint64_t), st[0]));
+    std::vector<cudaEvent_t> ev(2 * nchunks + 2, nullptr);
+    for (auto& e : ev) cudaEventCreate(&e);
+    // the auxiliary stream starts after the counters are cleared
+    cudaEventRecord(ev[2 * nchunks], st[0]);
+    cudaStreamWaitEvent(st[1], ev[2 * nchunks], 0);
+    gahhg_status rc = GAHHG_OK;
+    for (int b = 0; b < 2 && rc == GAHHG_OK && (size_t)b < nchunks; b++)
+        rc = pool_alloc((void**)&buf[b], chunk * 17, g->device, st[b]);
+    for (size_t k = 0; k < nchunks && rc == GAHHG_OK; k++) {
+        const int b = (int)(k & 1);
+        cudaStream_t s = st[b];
+        const size_t off = k * chunk, m = std::min(chunk, n - off);
+        double* d_ll = (double*)buf[b];
+        uint8_t* d_lab = buf[b] + chunk * 16;
+        if (cudaMemcpyAsync(d_ll, lonlat + 2 * off, m * 16, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+            set_error("query copy-in: %s", cudaGetErrorString(cudaGetLastError()));
+            rc = GAHHG_ERR_CUDA;
+            break;
+        }
+        cudaEventRecord(ev[2 * k], s);
+        rc = run_query(g, d_ll, m, d_lab, precision, s, d_cnt);
+        cudaEventRecord(ev[2 * k + 1], s);
+        if (rc == GAHHG_OK && cudaMemcpyAsync(labels + off, d_lab, m, cudaMemcpyDeviceToHost, s) != cudaSuccess) {
+            set_error("query copy-out: %s", cudaGetErrorString(cudaGetLastError()));
+            rc = GAHHG_ERR_CUDA;
         }
     }
-    if (d_ll) cudaFreeAsync(d_ll, s);
-    if (d_lab) cudaFreeAsync(d_lab, s);
-    cudaStreamSynchronize(s);
-    return st;
+    // join the auxiliary stream, then read the counters
+    cudaEventRecord(ev[2 * nchunks + 1], st[1]);
+    cudaStreamWaitEvent(st[0], ev[2 * nchunks + 1], 0);
+    uint64_t cnt[4] = {0, 0, 0, 0};
+    cudaMemcpyAsync(cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, st[0]);
+    const cudaError_t e = cudaStreamSynchronize(st[0]);
+    if (rc == GAHHG_OK && e != cudaSuccess) {
+        set_error("query: %s", cudaGetErrorString(e));
+        rc = GAHHG_ERR_CUDA;
+    }
+    if (rc == GAHHG_OK) {
+        double ms_total = 0.0;
+        for (size_t k = 0; k < nchunks; k++) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[2 * k], ev[2 * k + 1]);
+            ms_total += ms;
+        }
+        g->stats.query_s = ms_total * 1e-3;
+        g->stats.query_points = (long long)n;
+        g->stats.esc_fp64 = (long long)cnt[0];
+        g->stats.esc_exact = (long long)cnt[1];
+        g->stats.boundary_points = (long long)cnt[2];
+        g->stats.in_count = (long long)cnt[3];
+    }
+    for (int b = 0; b < 2; b++)
+        if (buf[b]) cudaFreeAsync(buf[b], st[0]);
+    cudaFreeAsync(d_cnt, st[0]);
+    cudaStreamSynchronize(st[0]);
+    for (auto& x : ev) cudaEventDestroy(x);
+    return rc;
 }
 
 gahhg_status gahhg_stats_get(const gahhg_grid* G, gahhg_stats* s)

@@ -155,6 +155,7 @@ struct Grid {
     const Polygon* poly = nullptr;
     gahhg_build_opts opts{};
     cudaStream_t stream = nullptr;
+    cudaStream_t aux_stream = nullptr;  // second stream of the pipelined host-buffer query
     int device = 0;
 
     std::vector<Level> levels;    // levels[0..gnum-1]
