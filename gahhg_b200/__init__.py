@@ -62,13 +62,18 @@ class Polygon:
             self._h = None
 
 
-def load_points(path):
-    """GPISPTP::loadTPFromCSV -> (n, 2) float64 lon/lat."""
+def load_points(path, sidecar=False):
+    """GPISPTP::loadTPFromCSV -> (n, 2) float64 lon/lat.  sidecar=True reads
+    `<path>.f64` when it matches the CSV and writes it otherwise."""
     h = ctypes.c_void_p()
     L = _lib.lib()
-    check(L.gahhg_points_load(str(path).encode(), ctypes.byref(h)))
+    if sidecar:
+        check(L.gahhg_points_load_ex(str(path).encode(), _lib.POINTS_USE_SIDECAR | _lib.POINTS_WRITE_SIDECAR,
+                                     ctypes.byref(h)))
+    else:
+        check(L.gahhg_points_load(str(path).encode(), ctypes.byref(h)))
     n = L.gahhg_points_count(h)
-    out = np.zeros((n, 2), dtype=np.float64)
+    out = np.empty((n, 2), dtype=np.float64)
     if n:
         ctypes.memmove(out.ctypes.data, L.gahhg_points_lonlat(h), n * 16)
     L.gahhg_points_free(h)

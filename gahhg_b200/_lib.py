@@ -96,6 +96,9 @@ class ServerStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+POINTS_USE_SIDECAR = 1
+POINTS_WRITE_SIDECAR = 2
+
 SERVE_PINNED = 1
 SERVE_DETACHED = 2
 POLY_FREE, POLY_QUEUED, POLY_BUILDING, POLY_READY, POLY_FAILED, POLY_EVICTING = range(6)
@@ -112,6 +115,7 @@ _SIGS = {
     "gahhg_polygon_export": (ctypes.c_int, [_P, _P, _P]),
     "gahhg_polygon_free": (None, [_P]),
     "gahhg_points_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_P)]),
+    "gahhg_points_load_ex": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(_P)]),
     "gahhg_points_count": (ctypes.c_size_t, [_P]),
     "gahhg_points_lonlat": (_P, [_P]),
     "gahhg_points_free": (None, [_P]),

@@ -249,8 +249,26 @@ gahhg_status gahhg_points_load(const char* path, gahhg_points** out)
     return GAHHG_OK;
 }
 
-size_t gahhg_points_count(const gahhg_points* p) { return p ? p->p.lonlat.size() / 2 : 0; }
-const double* gahhg_points_lonlat(const gahhg_points* p) { return p ? p->p.lonlat.data() : nullptr; }
+size_t gahhg_points_count(const gahhg_points* p) { return p ? p->p.n : 0; }
+const double* gahhg_points_lonlat(const gahhg_points* p) { return p ? p->p.lonlat.get() : nullptr; }
+
+gahhg_status gahhg_points_load_ex(const char* path, int flags, gahhg_points** out)
+{
+    if (!path || !out) return GAHHG_ERR_ARG;
+    gahhg_points* p = new gahhg_points();
+    if ((flags & GAHHG_POINTS_USE_SIDECAR) && load_points_sidecar(path, &p->p) == GAHHG_OK) {
+        *out = p;
+        return GAHHG_OK;
+    }
+    gahhg_status s = load_points_file(path, &p->p);
+    if (s == GAHHG_OK && (flags & GAHHG_POINTS_WRITE_SIDECAR)) s = write_points_sidecar(path, p->p);
+    if (s != GAHHG_OK) {
+        delete p;
+        return s;
+    }
+    *out = p;
+    return GAHHG_OK;
+}
 void gahhg_points_free(gahhg_points* p) { delete p; }
 
 gahhg_status gahhg_build(const gahhg_polygon* poly, const gahhg_build_opts* opts, gahhg_grid** out)

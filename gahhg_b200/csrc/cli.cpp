@@ -4,7 +4,8 @@
 // skipped), same defaults (source/GPISPParam.h:64-77), same messages, same
 // return codes (-1 when a loader fails), the report block appended and the
 // result CSV overwritten.  Extra flags: /maxdepth N, /semantics exact|reference
-// (default reference, as GPISP.exe), /precision fp32|fp64.
+// (default reference, as GPISP.exe), /precision fp32|fp64, /sidecar (binary copy
+// of the query file, `<tpfile>.f64`, read when it matches the CSV).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -21,6 +22,7 @@ int main(int argc, char* argv[])
     o.semantics = GAHHG_SEMANTICS_REFERENCE;
     o.verbose = 1;
     int precision = GAHHG_QUERY_AUTO;
+    int point_flags = 0;
     for (int i = 1; i < argc; i++) {
         auto val = [&](std::string* dst) {
             if (i + 1 < argc) *dst = argv[++i];
@@ -36,12 +38,15 @@ int main(int argc, char* argv[])
         } else if (!strcmp(argv[i], "/precision") && i + 1 < argc) {
             const char* s = argv[++i];
             precision = !strcmp(s, "fp64") ? GAHHG_QUERY_FP64_FILTER : GAHHG_QUERY_FP32_FILTER;
+        } else if (!strcmp(argv[i], "/sidecar")) {
+            // read `<tpfile>.f64` when it matches the CSV, else parse and write it
+            point_flags = GAHHG_POINTS_USE_SIDECAR | GAHHG_POINTS_WRITE_SIDECAR;
         }
     }
     gahhg_polygon* P = nullptr;
     if (gahhg_polygon_load(poly.c_str(), &P) != GAHHG_OK) return -1;
     gahhg_points* T = nullptr;
-    if (gahhg_points_load(tp.c_str(), &T) != GAHHG_OK) return -1;
+    if (gahhg_points_load_ex(tp.c_str(), point_flags, &T) != GAHHG_OK) return -1;
     gahhg_grid* G = nullptr;
     gahhg_status s = gahhg_build(P, &o, &G);
     if (s == GAHHG_OK) s = gahhg_classify(G);

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -140,10 +141,15 @@ gahhg_status polygon_from_rings(const double* lonlat, const int64_t* ring_offset
                                 Polygon* out);
 
 struct Points {
-    std::vector<double> lonlat;
+    std::unique_ptr<double[]> lonlat;  // lon, lat per point (not zero-filled: every entry is parsed)
+    size_t n = 0;
     std::string path;
 };
 gahhg_status load_points_file(const char* path, Points* out);
+// Binary sidecar `<csv>.f64`: a 64-byte header (magic, point count, size
+// and modification time of the CSV it was made from) and the lon/lat doubles.
+gahhg_status load_points_sidecar(const char* csv_path, Points* out);  // GAHHG_ERR_STATE when absent or stale
+gahhg_status write_points_sidecar(const char* csv_path, const Points& pts);
 
 // ------------------------------------------------------------ level-0 grid --
 void build_grid0(std::vector<D3>& V, std::vector<Border>& B, std::vector<Cell>& C);

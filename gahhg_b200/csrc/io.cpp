@@ -10,13 +10,22 @@
 // outer ring is re-oriented counter-clockwise and holes clockwise by the
 // reference's local test at the northernmost vertex.  Vertex XYZ comes from
 // the canonical conversion (include/gahhg_canon.h).
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <charconv>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <cfloat>
 #include <fstream>
 #include <sstream>
+#include <thread>
+#include <vector>
 
 #include "gahhg_canon.h"
 #include "gahhg_internal.h"
@@ -222,48 +231,229 @@ gahhg_status polygon_from_rings(const double* lonlat, const int64_t* ring_offset
     return GAHHG_OK;
 }
 
+namespace {
+
+// Read-only map of a whole file (an empty file maps to nothing).
+struct MappedFile {
+    const char* data = nullptr;
+    size_t size = 0;
+    struct stat st {};
+    int fd = -1;
+    bool open(const char* path)
+    {
+        fd = ::open(path, O_RDONLY);
+        if (fd < 0 || fstat(fd, &st) != 0 || !S_ISREG(st.st_mode)) return false;
+        size = (size_t)st.st_size;
+        if (size == 0) return true;
+        void* p = mmap(nullptr, size, PROT_READ, MAP_PRIVATE, fd, 0);
+        if (p == MAP_FAILED) return false;
+        madvise(p, size, MADV_SEQUENTIAL);
+        data = (const char*)p;
+        return true;
+    }
+    ~MappedFile()
+    {
+        if (data) munmap((void*)data, size);
+        if (fd >= 0) ::close(fd);
+    }
+};
+
+inline bool in_line_space(char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\v' || c == '\f'; }
+
+// The serial loader's reading of one line [s, e) ("%lf,%lf": strtod for each
+// number, ',' right after the first, anything after the second ignored), on
+// a NUL-terminated copy: a number never spans a line end, and where strtod
+// skipped white space into the next line the line was rejected anyway.
+bool parse_point_strtod(const char* s, const char* e, double* lo, double* la)
+{
+    char small[256];
+    std::string big;
+    char* buf = small;
+    const size_t len = (size_t)(e - s);
+    if (len + 1 > sizeof(small)) {
+        big.assign(s, len);
+        buf = &big[0];
+    } else {
+        memcpy(small, s, len);
+        small[len] = 0;
+    }
+    const char* le = buf + len;
+    char* q;
+    *lo = strtod(buf, &q);
+    if (q == buf || q >= le || *q != ',') return false;
+    const char* p = q + 1;
+    *la = strtod(p, &q);
+    return q != p && q <= le;
+}
+
+// Fast path for the usual "lon,lat" line; false sends the line to the serial
+// reading above (a '+' sign, hex, out-of-range values, unusual separators).
+inline bool parse_point_fast(const char* s, const char* e, double* lo, double* la)
+{
+    const char* p = s;
+    while (p < e && in_line_space(*p)) p++;
+    auto r = std::from_chars(p, e, *lo);
+    if (r.ec != std::errc() || r.ptr >= e || *r.ptr != ',') return false;
+    p = r.ptr + 1;
+    while (p < e && in_line_space(*p)) p++;
+    r = std::from_chars(p, e, *la);
+    if (r.ec != std::errc()) return false;
+    return r.ptr == e || in_line_space(*r.ptr) || *r.ptr == ',' || *r.ptr == ';';
+}
+
+// Lines of [b, e) that start a line (b is a line start): '\n' ends a line; a
+// final line without '\n' counts when this chunk ends the file.
+long long count_lines(const char* b, const char* e, bool last)
+{
+    long long n = (long long)std::count(b, e, '\n');
+    if (last && e > b && e[-1] != '\n') n++;
+    return n;
+}
+
+constexpr uint64_t SIDECAR_MAGIC = 0x3146545032474847ull;  // "GHG2PTF1"
+
+struct SidecarHeader {
+    uint64_t magic;
+    uint64_t count;
+    uint64_t source_size;
+    int64_t source_mtime_ns;
+    uint64_t reserved[4];
+};
+static_assert(sizeof(SidecarHeader) == 64, "sidecar header");
+
+std::string sidecar_path(const char* csv) { return std::string(csv) + ".f64"; }
+
+int64_t mtime_ns(const struct stat& st) { return (int64_t)st.st_mtim.tv_sec * 1000000000LL + st.st_mtim.tv_nsec; }
+
+}  // namespace
+
+// GPISPTP::loadTPFromCSV (source/GPISPTP.cu:13-79).  The file is mapped and
+// split at line starts into one chunk per host thread; a first pass counts
+// each chunk's lines, a second parses them in place.  Values and the first
+// rejected line (and its message) are those of a serial strtod reading.
 gahhg_status load_points_file(const char* path, Points* T)
 {
     printf("Load test points from a CSV file: %s.\n", path);
-    std::string data;
-    if (!read_file(path, &data)) {
+    MappedFile f;
+    if (!f.open(path)) {
         printf("Error. Can not open %s\n.", path);
         set_error("cannot open %s", path);
         return GAHHG_ERR_IO;
     }
-    T->lonlat.clear();
-    T->lonlat.reserve(data.size() / 10);
-    const char* s = data.c_str();
-    const char* end = s + data.size();
-    long long count = 0;
-    while (s < end) {
-        const char* e = (const char*)memchr(s, '\n', end - s);
-        if (!e) e = end;
-        // "%lf,%lf": optional white space, number, ',', optional white space, number
-        char* q;
-        const char* p = s;
-        double lo = strtod(p, &q);
-        bool ok = q != p && q < e;
-        double la = 0;
-        if (ok) {
-            ok = (*q == ',');
-            if (ok) {
-                p = q + 1;
-                la = strtod(p, &q);
-                ok = q != p && q <= e;
-            }
+    const char* base = f.data;
+    const char* end = base + f.size;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nt = (int)std::min<size_t>(std::min(hw, 64u), std::max<size_t>(1, f.size >> 22));  // >= 4 MB each
+    std::vector<const char*> cut(nt + 1);
+    cut[0] = base;
+    cut[nt] = end;
+    for (int t = 1; t < nt; t++) {
+        const char* c = base + f.size / nt * t;
+        c = std::max(c, cut[t - 1]);
+        const char* nl = c < end ? (const char*)memchr(c, '\n', end - c) : nullptr;
+        cut[t] = nl ? nl + 1 : end;
+    }
+    std::vector<long long> first(nt + 1, 0);
+    auto run = [&](auto&& fn) {
+        if (nt == 1) {
+            fn(0);
+            return;
         }
-        if (!ok) {
-            printf("Error. Line %lld of %s. Wrong format.\n", count + 1, path);
-            set_error("line %lld of %s: wrong format", count + 1, path);
+        std::vector<std::thread> th;
+        for (int t = 0; t < nt; t++) th.emplace_back(fn, t);
+        for (auto& x : th) x.join();
+    };
+    run([&](int t) { first[t + 1] = count_lines(cut[t], cut[t + 1], t == nt - 1); });
+    for (int t = 0; t < nt; t++) first[t + 1] += first[t];
+    const long long n = first[nt];
+    T->lonlat.reset(n ? new double[(size_t)n * 2] : nullptr);
+    T->n = 0;
+    std::vector<long long> bad(nt, -1);  // first rejected line (global index) per chunk
+    run([&](int t) {
+        double* out = T->lonlat.get() + 2 * first[t];
+        const char* s = cut[t];
+        const char* ce = cut[t + 1];
+        long long k = 0;
+        while (s < ce) {
+            const char* e = (const char*)memchr(s, '\n', ce - s);
+            if (!e) e = ce;
+            double lo, la;
+            if (!parse_point_fast(s, e, &lo, &la) && !parse_point_strtod(s, e, &lo, &la)) {
+                bad[t] = first[t] + k;
+                return;
+            }
+            out[2 * k] = lo;
+            out[2 * k + 1] = la;
+            k++;
+            s = (e < ce) ? e + 1 : e;
+        }
+    });
+    for (int t = 0; t < nt; t++)
+        if (bad[t] >= 0) {
+            printf("Error. Line %lld of %s. Wrong format.\n", bad[t] + 1, path);
+            set_error("line %lld of %s: wrong format", bad[t] + 1, path);
+            T->lonlat.reset();
             return GAHHG_ERR_FORMAT;
         }
-        T->lonlat.push_back(lo);
-        T->lonlat.push_back(la);
-        count++;
-        s = (e < end) ? e + 1 : e;
-    }
+    T->n = (size_t)n;
     T->path = path;
+    return GAHHG_OK;
+}
+
+gahhg_status load_points_sidecar(const char* csv_path, Points* T)
+{
+    struct stat src;
+    if (stat(csv_path, &src) != 0) {
+        set_error("cannot open %s", csv_path);
+        return GAHHG_ERR_IO;
+    }
+    const std::string sp = sidecar_path(csv_path);
+    MappedFile f;
+    if (!f.open(sp.c_str()) || f.size < sizeof(SidecarHeader)) {
+        set_error("no sidecar %s", sp.c_str());
+        return GAHHG_ERR_STATE;
+    }
+    SidecarHeader h;
+    memcpy(&h, f.data, sizeof(h));
+    if (h.magic != SIDECAR_MAGIC || h.source_size != (uint64_t)src.st_size || h.source_mtime_ns != mtime_ns(src) ||
+        f.size != sizeof(h) + h.count * 16) {
+        set_error("sidecar %s does not match %s", sp.c_str(), csv_path);
+        return GAHHG_ERR_STATE;
+    }
+    T->lonlat.reset(h.count ? new double[h.count * 2] : nullptr);
+    if (h.count) memcpy(T->lonlat.get(), f.data + sizeof(h), h.count * 16);
+    T->n = h.count;
+    T->path = csv_path;
+    return GAHHG_OK;
+}
+
+gahhg_status write_points_sidecar(const char* csv_path, const Points& T)
+{
+    struct stat src;
+    if (stat(csv_path, &src) != 0) {
+        set_error("cannot open %s", csv_path);
+        return GAHHG_ERR_IO;
+    }
+    const std::string sp = sidecar_path(csv_path);
+    const std::string tmp = sp + ".tmp";
+    FILE* fp = fopen(tmp.c_str(), "wb");
+    if (!fp) {
+        set_error("cannot write %s", tmp.c_str());
+        return GAHHG_ERR_IO;
+    }
+    SidecarHeader h{};
+    h.magic = SIDECAR_MAGIC;
+    h.count = T.n;
+    h.source_size = (uint64_t)src.st_size;
+    h.source_mtime_ns = mtime_ns(src);
+    bool ok = fwrite(&h, sizeof(h), 1, fp) == 1;
+    if (ok && T.n) ok = fwrite(T.lonlat.get(), 16, T.n, fp) == T.n;
+    ok = (fclose(fp) == 0) && ok;
+    if (!ok || rename(tmp.c_str(), sp.c_str()) != 0) {
+        unlink(tmp.c_str());
+        set_error("cannot write %s", sp.c_str());
+        return GAHHG_ERR_IO;
+    }
     return GAHHG_OK;
 }
 

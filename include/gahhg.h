@@ -82,8 +82,8 @@ typedef struct {
     double query_s;            /* PISPTime of the last gahhg_query* call */
     long long query_points;
     long long in_count;        /* labels == 2 in the last query */
-    long long esc_fp64;        /* exact query: (point, edge) tests escalated to FP64 */
-    long long esc_exact;       /* exact query: tests escalated to expansion arithmetic */
+    long long esc_fp64;        /* exact query: points the FP32 tier deferred to FP64 */
+    long long esc_exact;       /* exact query: points the FP64 tier deferred to exact arithmetic */
     long long boundary_points; /* exact query: points that ran crossing tests */
     long long walk_limit_hits; /* edge walks stopped at the step limit (the reference would not terminate) */
 } gahhg_stats;
@@ -107,8 +107,17 @@ int gahhg_polygon_num_edges(const gahhg_polygon* p);
 gahhg_status gahhg_polygon_export(const gahhg_polygon* p, double* xyz, int* pe);
 void gahhg_polygon_free(gahhg_polygon* p);
 
-/* GPISPTP::loadTPFromCSV (source/GPISPTP.cu:13-79): "lon,lat" per line. */
+/* GPISPTP::loadTPFromCSV (source/GPISPTP.cu:13-79): "lon,lat" per line.
+ * The file is parsed by all host threads; values and the first rejected line
+ * are those of the reference's serial reading. */
 gahhg_status gahhg_points_load(const char* path, gahhg_points** out);
+/* The same with a binary sidecar `<path>.f64` (no counterpart in the
+ * reference): GAHHG_POINTS_USE_SIDECAR reads the sidecar instead of the CSV
+ * when it exists and matches the CSV's size and modification time;
+ * GAHHG_POINTS_WRITE_SIDECAR writes it after parsing the CSV. */
+#define GAHHG_POINTS_USE_SIDECAR 1
+#define GAHHG_POINTS_WRITE_SIDECAR 2
+gahhg_status gahhg_points_load_ex(const char* path, int flags, gahhg_points** out);
 size_t gahhg_points_count(const gahhg_points* p);
 const double* gahhg_points_lonlat(const gahhg_points* p);
 void gahhg_points_free(gahhg_points* p);
