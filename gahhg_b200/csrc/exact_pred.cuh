@@ -69,6 +69,40 @@ XHDN int sum_sign(const double* t, int n)
     return 0;
 }
 
+// The sum of n exactly representable terms (n <= 24) to within a few ulp of
+// the exact sum: the terms are accumulated into a non-overlapping expansion
+// (as in sum_sign), whose components are then added from the smallest up.
+XHDN double sum_value(const double* t, int n)
+{
+    double e[48];
+    int m = 0;
+    for (int i = 0; i < n; i++) {
+        double q = t[i];
+        if (q == 0.0) continue;
+        int k = 0;
+        for (int j = 0; j < m; j++) {
+            double s, r;
+            two_sum(q, e[j], s, r);
+            if (r != 0.0) e[k++] = r;
+            q = s;
+        }
+        if (q != 0.0 || k == 0) e[k++] = q;
+        m = k;
+    }
+    double v = 0.0;
+    for (int i = 0; i < m; i++) v += e[i];
+    return v;
+}
+
+// u0 v1 - u1 v0 to within a few ulp (exact products, then sum_value).
+XHD double det2_value(double u0, double u1, double v0, double v1)
+{
+    double t[4];
+    two_prod(u0, v1, t[0], t[1]);
+    two_prod(-u1, v0, t[2], t[3]);
+    return sum_value(t, 4);
+}
+
 XHD void triple(double a, double b, double c, double* o)
 {
     double p, e;
@@ -87,6 +121,27 @@ XHDN int det3_sign(const double* a, const double* b, const double* c)
     triple(a[2], b[0], c[1], t + 16);
     triple(-a[2], b[1], c[0], t + 20);
     return sum_sign(t, 24);
+}
+
+// det[a; b; c] to within a few ulp of its exact value.
+XHDN double det3_value(const double* a, const double* b, const double* c)
+{
+    double t[24];
+    triple(a[0], b[1], c[2], t + 0);
+    triple(-a[0], b[2], c[1], t + 4);
+    triple(a[1], b[2], c[0], t + 8);
+    triple(-a[1], b[0], c[2], t + 12);
+    triple(a[2], b[0], c[1], t + 16);
+    triple(-a[2], b[1], c[0], t + 20);
+    return sum_value(t, 24);
+}
+
+// a x b, each component to within a few ulp.
+XHD void cross_value(const double* a, const double* b, double* o)
+{
+    o[0] = det2_value(a[1], a[2], b[1], b[2]);
+    o[1] = det2_value(a[2], a[0], b[2], b[0]);
+    o[2] = det2_value(a[0], a[1], b[0], b[1]);
 }
 
 XHD int det2_sign(double u0, double u1, double v0, double v1)

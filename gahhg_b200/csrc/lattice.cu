@@ -43,6 +43,7 @@
 #include "exact_pred.cuh"
 #include "gahhg_canon.h"
 #include "gahhg_internal.h"
+#include "local_frame.cuh"
 
 namespace gahhg {
 
@@ -83,22 +84,27 @@ constexpr long long PAIR_BUDGET = 1LL << 30;
 constexpr float E_Q32 = 2.0e-6f;
 constexpr float C32 = E_Q32 + 5.0f * 5.9604645e-8f;
 
-struct __align__(32) LeafRec {
-    double R[3];
+// Leaf: its center as the lon/lat it was placed at (R = their canonical XYZ,
+// recomputed where needed), its edge records and its center's label.
+struct __align__(8) LeafRec {
+    double lon, lat;
     uint32_t off;
     uint16_t cnt;
     uint8_t label;
     uint8_t pad;
 };
-static_assert(sizeof(LeafRec) == 32, "LeafRec");
+static_assert(sizeof(LeafRec) == 24, "LeafRec");
 
+// (leaf, edge): the cross products and R . (A x B), each rounded to float
+// from a value within a few FP64 ulp of the exact one.
 struct EdgeRec {
     float n1[3];  // A x B
     float n2[3];  // A x R
     float n3[3];  // B x R
+    float h1;     // R . (A x B) = det[A; B; R]
     uint32_t es;  // edge index | (orient(A,B,R) > 0) << 31
 };
-static_assert(sizeof(EdgeRec) == 40, "EdgeRec");
+static_assert(sizeof(EdgeRec) == 44, "EdgeRec");
 
 // Level-0 grid over a lon/lat domain: W x H cells of dlon0 x dlat0 degrees
 // starting at (lon0, lat0).  full_lon: the domain spans all longitudes
@@ -697,9 +703,8 @@ __global__ void k_leaf_records(BuildView v, int lvl, int nn, const int* is_leaf,
     NodeCap c = node_cap(v.g, lvl, ix[p], iy[p]);
     nudge_center(v.g, lvl, c, v.pv, v.pe, list + off[p], cnt[p]);
     LeafRec L;
-    L.R[0] = c.R[0];
-    L.R[1] = c.R[1];
-    L.R[2] = c.R[2];
+    L.lon = c.lonc;
+    L.lat = c.latc;
     const long long ro = rec_base + rec_off[p];
     L.off = (uint32_t)ro;
     L.cnt = (uint16_t)min(cnt[p], 65535);
@@ -707,22 +712,21 @@ __global__ void k_leaf_records(BuildView v, int lvl, int nn, const int* is_leaf,
     L.pad = 0;
     leaves[leaf_base + leaf_off[p]] = L;
     if (cnt[p] > 65535) atomicAdd(bad + 2, 1);
-    const D3 R = d3(c.R[0], c.R[1], c.R[2]);
     for (int k = 0; k < cnt[p]; k++) {
         const int e = list[off[p] + k];
         const D3 a = v.pv[v.pe[2 * e]], b = v.pv[v.pe[2 * e + 1]];
-        const D3 n1 = cross(a, b), n2 = cross(a, R), n3 = cross(b, R);
-        EdgeRec r;
-        r.n1[0] = (float)n1.x;
-        r.n1[1] = (float)n1.y;
-        r.n1[2] = (float)n1.z;
-        r.n2[0] = (float)n2.x;
-        r.n2[1] = (float)n2.y;
-        r.n2[2] = (float)n2.z;
-        r.n3[0] = (float)n3.x;
-        r.n3[1] = (float)n3.y;
-        r.n3[2] = (float)n3.z;
         const double A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z};
+        double n1[3], n2[3], n3[3];
+        exact::cross_value(A, B, n1);
+        exact::cross_value(A, c.R, n2);
+        exact::cross_value(B, c.R, n3);
+        EdgeRec r;
+        for (int j = 0; j < 3; j++) {
+            r.n1[j] = (float)n1[j];
+            r.n2[j] = (float)n2[j];
+            r.n3[j] = (float)n3[j];
+        }
+        r.h1 = (float)exact::det3_value(A, B, c.R);
         const int s1 = exact::orient(A, B, c.R);
         if (s1 == 0) atomicAdd(bad, 1);
         r.es = (uint32_t)e | (s1 > 0 ? 0x80000000u : 0u);
@@ -831,6 +835,8 @@ __device__ __forceinline__ int sign_escalate(const double* x, const double* y, c
 __device__ uint8_t leaf_label(const QueryView& Q, uint32_t leaf, PointCtx& P, bool fp32, unsigned long long* ctr)
 {
     const LeafRec L = Q.leaves[leaf];
+    double LR[3];
+    gahhg_canon_vertex_xyz(L.lon, L.lat, LR);
     float qx = 0.f, qy = 0.f, qz = 0.f;
     if (fp32) {
         float sa, ca, so, co;
@@ -869,7 +875,7 @@ __device__ uint8_t leaf_label(const QueryView& Q, uint32_t leaf, PointCtx& P, bo
             P.need64();
             needAB();
             if (exact::same(P.q, A) || exact::same(P.q, B)) return CELL_IN;  // vertex rule
-            if (exact::same(P.q, L.R)) return L.label;                       // q is the center
+            if (exact::same(P.q, LR)) return L.label;                       // q is the center
             s2 = sign_escalate(A, B, P.q, c64, cx);
         }
         if (s2 == s1) continue;
@@ -879,8 +885,8 @@ __device__ uint8_t leaf_label(const QueryView& Q, uint32_t leaf, PointCtx& P, bo
             P.need64();
             needAB();
             if (exact::same(P.q, A) || exact::same(P.q, B)) return CELL_IN;
-            if (exact::same(P.q, L.R)) return L.label;
-            s3 = sign_escalate(L.R, P.q, A, c64, cx);
+            if (exact::same(P.q, LR)) return L.label;
+            s3 = sign_escalate(LR, P.q, A, c64, cx);
         }
         if (s3 != s2) continue;
         int s4 = fp32 ? sign32(r.n3, qx, qy, qz) : 0;
@@ -888,8 +894,8 @@ __device__ uint8_t leaf_label(const QueryView& Q, uint32_t leaf, PointCtx& P, bo
             P.need64();
             needAB();
             if (exact::same(P.q, A) || exact::same(P.q, B)) return CELL_IN;
-            if (exact::same(P.q, L.R)) return L.label;
-            s4 = sign_escalate(L.R, P.q, B, c64, cx);
+            if (exact::same(P.q, LR)) return L.label;
+            s4 = sign_escalate(LR, P.q, B, c64, cx);
         }
         if (s4 == -s2) par ^= 1;
     }
@@ -911,7 +917,8 @@ __device__ __forceinline__ void allow_dependents() { asm volatile("griddepcontro
 // The crossing tests of the queued points run in tiers, each its own launch
 // over the points the previous tier could not decide, so that no warp carries
 // the registers or waits on the branches of a rarer, costlier tier:
-//   tier 1: every sign from the certified FP32 filter (no FP64 code at all);
+//   tier 1: every sign from the certified FP32 filter in the leaf's local
+//           frame (local_frame.cuh);
 //   tier 2: the canonical FP64 point, the vertex and center rules, and every
 //           sign from the FP64 filter on translated rows (orient_fp64_near);
 //   tier 3: the complete test (FP64 filter, then exact arithmetic with
@@ -923,22 +930,19 @@ constexpr uint8_t LABEL_DEFER = 0xFF;
 __device__ uint8_t leaf_label_fp32(const QueryView& Q, uint32_t leaf, const PointCtx& P)
 {
     const LeafRec L = Q.leaves[leaf];
-    float sa, ca, so, co;
-    // arguments stay inside [-pi, pi], where __sincosf's error bound is documented
-    __sincosf((float)gahhg_canon_rad(P.lat_r), &sa, &ca);
-    __sincosf((float)gahhg_canon_rad(P.lon_r), &so, &co);
-    const float qx = ca * so, qy = sa, qz = ca * co;
+    local_frame::Offset o;
+    if (!(fabs(P.lon) <= 540.0) || !local_frame::offset(P.lon, P.lat, L.lon, L.lat, o)) return LABEL_DEFER;
     int par = 0;
     for (int k = 0; k < L.cnt; k++) {
         const EdgeRec r = Q.recs[L.off + k];
         const int s1 = (r.es >> 31) ? 1 : -1;
-        const int s2 = sign32(r.n1, qx, qy, qz);
+        const int s2 = local_frame::sign_at(o, r.n1, r.h1);
         if (s2 == 0) return LABEL_DEFER;
         if (s2 == s1) continue;
-        const int s3 = sign32(r.n2, qx, qy, qz);
+        const int s3 = local_frame::sign_at(o, r.n2, 0.0f);
         if (s3 == 0) return LABEL_DEFER;
         if (s3 != s2) continue;
-        const int s4 = sign32(r.n3, qx, qy, qz);
+        const int s4 = local_frame::sign_at(o, r.n3, 0.0f);
         if (s4 == 0) return LABEL_DEFER;
         if (s4 == -s2) par ^= 1;
     }
@@ -949,6 +953,8 @@ __device__ uint8_t leaf_label_fp64(const QueryView& Q, uint32_t leaf, PointCtx& 
 {
     const LeafRec L = Q.leaves[leaf];
     P.need64();
+    double LR[3];
+    gahhg_canon_vertex_xyz(L.lon, L.lat, LR);
     int par = 0;
     for (int k = 0; k < L.cnt; k++) {
         const EdgeRec r = Q.recs[L.off + k];
@@ -957,15 +963,15 @@ __device__ uint8_t leaf_label_fp64(const QueryView& Q, uint32_t leaf, PointCtx& 
         const D3 a = Q.pv[Q.pe[2 * e]], b = Q.pv[Q.pe[2 * e + 1]];
         const double A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z};
         if (exact::same(P.q, A) || exact::same(P.q, B)) return CELL_IN;  // vertex rule
-        if (exact::same(P.q, L.R)) return L.label;                       // q is the center
+        if (exact::same(P.q, LR)) return L.label;                       // q is the center
         // every row is within a cap of the first: translated rows keep the bound small
         const int s2 = exact::orient_fp64_near(A, B, P.q);
         if (s2 == 0) return LABEL_DEFER;
         if (s2 == s1) continue;
-        const int s3 = exact::orient_fp64_near(L.R, P.q, A);
+        const int s3 = exact::orient_fp64_near(LR, P.q, A);
         if (s3 == 0) return LABEL_DEFER;
         if (s3 != s2) continue;
-        const int s4 = exact::orient_fp64_near(L.R, P.q, B);
+        const int s4 = exact::orient_fp64_near(LR, P.q, B);
         if (s4 == 0) return LABEL_DEFER;
         if (s4 == -s2) par ^= 1;
     }
@@ -1054,7 +1060,7 @@ constexpr uint8_t LABEL_PENDING = 0;
 // evict-first policy so the node table stays in L2.  The index arithmetic
 // need not match the canonical conversion bit for bit: every cap carries a
 // margin far above its rounding (see LOC_MARGIN).
-template <bool STATS>
+template <bool STATS, bool LOCKSTEP = false>
 __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t* s_sum,
                                              const double2* __restrict__ ll, uint8_t* __restrict__ out,
                                              uint32_t* __restrict__ queue, unsigned int* __restrict__ qcount,
@@ -1074,6 +1080,12 @@ __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t*
         uint8_t lab[LOC_UNROLL];
         bool push[LOC_UNROLL];
         bool any = false;
+        // LOCKSTEP: the node words of all points are loaded first and the
+        // descents advance one level per round, so a thread keeps one
+        // independent load per point in flight (points that mostly need the
+        // node table, as around small polygons, are bound by its latency)
+        uint32_t w[LOC_UNROLL];
+        double fu[LOC_UNROLL], fv[LOC_UNROLL];
 #pragma unroll
         for (int k = 0; k < LOC_UNROLL; k++) {
             const int i = base + k * TPB + threadIdx.x;
@@ -1081,6 +1093,7 @@ __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t*
             const double laf = p[k].y + 90.0;  // the reference's FakeLL latitude + 90
             lab[k] = LABEL_PENDING;
             push[k] = false;
+            w[k] = KIND_PURE;
             if (full || i < count) {
                 if (laf >= 0.0 && laf <= 180.0 && fabs(lo) <= 540.0) {
                     Loc L;
@@ -1091,6 +1104,10 @@ __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t*
                         const uint32_t code = (s_sum[c >> 4] >> ((c & 15) << 1)) & 3u;
                         if (code < 2u) {
                             lab[k] = (uint8_t)(code + 1u);  // coarse cell without edges: most points end here
+                        } else if (LOCKSTEP) {
+                            w[k] = __ldg(Q.nodes + (size_t)L.iy * Q.W + L.ix);
+                            fu[k] = L.fu;
+                            fv[k] = L.fv;
                         } else {
                             const uint32_t d = descend(Q, __ldg(Q.nodes + (size_t)L.iy * Q.W + L.ix), L.fu, L.fv);
                             if ((d & KIND_MASK) == KIND_PURE)
@@ -1104,7 +1121,38 @@ __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t*
                     push[k] = isfinite(lo) && isfinite(laf);
                 }
             }
-            any |= push[k];
+            if (!LOCKSTEP) any |= push[k];
+        }
+        if (LOCKSTEP) {
+            bool inner = true;
+            while (inner) {
+                inner = false;
+#pragma unroll
+                for (int k = 0; k < LOC_UNROLL; k++)
+                    if ((w[k] & KIND_MASK) == KIND_INNER) {
+                        fu[k] *= FAN;
+                        fv[k] *= FAN;
+                        const int cx = min(max((int)fu[k], 0), FAN - 1), cy = min(max((int)fv[k], 0), FAN - 1);
+                        fu[k] -= cx;
+                        fv[k] -= cy;
+                        w[k] = __ldg(Q.nodes + (w[k] & INDEX_MASK) + cy * FAN + cx);
+                        inner = true;
+                    }
+            }
+#pragma unroll
+            for (int k = 0; k < LOC_UNROLL; k++) {
+                if (lab[k] == LABEL_PENDING && !push[k]) {
+                    const int i = base + k * TPB + threadIdx.x;
+                    if (full || i < count) {
+                        if ((w[k] & KIND_MASK) == KIND_PURE) {
+                            if (w[k] != KIND_PURE) lab[k] = (uint8_t)(w[k] & 3u);  // KIND_PURE alone: no node read
+                        } else {
+                            push[k] = true;
+                        }
+                    }
+                }
+                any |= push[k];
+            }
         }
         if (__any_sync(0xffffffffu, any)) {
 #pragma unroll
@@ -1231,7 +1279,7 @@ __global__ void __launch_bounds__(TPB) k_batch_locate(const QueryView* __restric
         const QueryView Q = views[c.view];
         for (int k = threadIdx.x; k < Q.swords; k += TPB) s_sum[k] = __ldg(Q.summary + k);
         __syncthreads();
-        locate_range<STATS>(Q, s_sum, ll, out, queue, qcount, c.start, c.count, 0, 1, inside);
+        locate_range<STATS, true>(Q, s_sum, ll, out, queue, qcount, c.start, c.count, 0, 1, inside);
         __syncthreads();
     }
     allow_dependents();

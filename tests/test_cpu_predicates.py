@@ -5,7 +5,9 @@ does return must be the exact sign of det[a; b; c].  The triples mimic the
 query's crossing tests: an edge (a, b) a few micro-radians long with a point
 c placed 10^U[-20,-3] rad off its great circle, and a leaf center with a
 point and an edge end near it.  The filters are compiled for the host from
-the same header the kernels use.
+the same headers the kernels use.  The FP32 local-frame tier is checked the
+same way on cells of 1e-7..1e-1 rad with points near an edge's great circle
+or near the arc from the cell center to an edge end.
 """
 import ctypes
 import os
@@ -22,11 +24,14 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 @pytest.fixture(scope="module")
 def probe(tmp_path_factory):
     out = str(tmp_path_factory.mktemp("pred") / "libpred_probe.so")
-    subprocess.check_call(["g++", "-O2", "-ffp-contract=off", "-shared", "-fPIC", "-o", out,
+    subprocess.check_call(["g++", "-O2", "-ffp-contract=off", "-shared", "-fPIC", "-I",
+                           os.path.join(os.path.dirname(HERE), "include"), "-o", out,
                            os.path.join(HERE, "native", "pred_probe.cpp")])
     lib = ctypes.CDLL(out)
     lib.filter_signs.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_int, ctypes.c_void_p]
     lib.filter_signs.restype = None
+    lib.local_signs.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p]
+    lib.local_signs.restype = None
 
     def signs(tri, near):
         tri = np.ascontiguousarray(tri, dtype=np.float64)
@@ -34,6 +39,13 @@ def probe(tmp_path_factory):
         lib.filter_signs(tri.ctypes.data, len(tri), 1 if near else 0, res.ctypes.data)
         return res
 
+    def local(cfg):
+        cfg = np.ascontiguousarray(cfg, dtype=np.float64)
+        res = np.zeros((len(cfg), 3), dtype=np.int32)
+        lib.local_signs(cfg.ctypes.data, len(cfg), res.ctypes.data)
+        return res
+
+    signs.local = local
     return signs
 
 
@@ -67,3 +79,59 @@ def test_fp64_filters_are_sound(probe):
     plain_decided = (probe(tri, False) != 0).mean()
     # the translated rows resolve points far closer to short edges
     assert near_decided > 0.9 and near_decided > plain_decided + 0.2, (near_decided, plain_decided)
+
+
+def _lonlat(v):
+    v = _unit(v)
+    return np.stack([np.degrees(np.arctan2(v[:, 0], v[:, 2])), np.degrees(np.arcsin(np.clip(v[:, 1], -1, 1)))], 1)
+
+
+def _xyz(ll):
+    lo, la = np.radians(ll[:, 0]), np.radians(ll[:, 1])
+    return np.stack([np.cos(la) * np.sin(lo), np.sin(la), np.cos(la) * np.cos(lo)], 1)
+
+
+def _local_cases(n, seed):
+    """Cells of 1e-7..1e-1 rad anywhere (poles, antimeridian); the point on
+    the edge's great circle or on the arc from the center to an edge end,
+    pushed off it by 10^U[-19,-2] times the cell size; longitudes wrapped by
+    +-360 degrees on either side."""
+    rng = np.random.default_rng(seed)
+    Rll = np.stack([rng.uniform(-180, 180, n), np.degrees(np.arcsin(rng.uniform(-1, 1, n)))], 1)
+    pole = rng.random(n) < 0.1
+    Rll[pole, 1] = np.sign(rng.uniform(-1, 1, pole.sum())) * rng.uniform(85, 90, pole.sum())
+    R = _xyz(Rll)
+    r = 10.0 ** rng.uniform(-7, -1, n)[:, None]
+    def near(scale):
+        return _unit(R + scale * r * rng.normal(size=(n, 3)))
+    A, B = near(1.0), near(1.0)
+    kind = rng.integers(0, 3, n)[:, None]  # 0: near edge AB, 1: near arc R-A, 2: near arc R-B
+    P0 = np.where(kind == 0, A, R)
+    P1 = np.where(kind == 2, B, np.where(kind == 0, B, A))
+    t = rng.uniform(-0.3, 1.3, (n, 1))
+    q = _unit((1 - t) * P0 + t * P1)
+    nrm = _unit(np.cross(P0, P1))
+    off = 10.0 ** rng.uniform(-19, -2, (n, 1)) * r * np.where(rng.random((n, 1)) < 0.5, -1.0, 1.0)
+    q = _unit(q + off * nrm)
+    qll, All, Bll = _lonlat(q), _lonlat(A), _lonlat(B)
+    qll[:, 0] += 360.0 * rng.integers(-1, 2, n) * (rng.random(n) < 0.2)
+    Rll[:, 0] += 360.0 * (rng.random(n) < 0.1)
+    return np.concatenate([qll, Rll, All, Bll], 1)
+
+
+def test_fp32_local_frame_is_sound(probe):
+    cfg = _local_cases(30000, 11)
+    got = probe.local(cfg)
+    ok = got[:, 0] != 9
+    assert ok.mean() > 0.99
+    want = np.zeros_like(got)
+    for i in np.nonzero(ok)[0]:
+        c = cfg[i]
+        q = exact.query_xyz(c[0:2].reshape(1, 2))[0]
+        R, A, B = exact.vertex_xyz(c[2:8].reshape(3, 2))
+        want[i] = (exact.orient(A, B, q, sos=False), exact.orient(R, q, A, sos=False), exact.orient(R, q, B, sos=False))
+    g, w = got[ok], want[ok]
+    decided = g != 0
+    assert np.array_equal(g[decided], w[decided]), "the local-frame FP32 tier returned a wrong sign"
+    # points 1e-5 of the cell size or more from the arc are decided in FP32
+    assert decided.mean() > 0.6, decided.mean()
