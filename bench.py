@@ -368,7 +368,7 @@ def run_c3(args):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": None, "bytes_per_point": BYTES_PER_POINT,
                      "peak_source": peak_kind},
-        "gpu_launches": 2 * steps, "clocks": clk,
+        "gpu_launches": 4 * steps, "clocks": clk,
         "build_ms": {"batch_build_wall": round(build_wall * 1e3, 1), "workers": bst["workers"],
                      "generate_s": round(gen_s, 1), "autotune_s": round(tune_s, 1)},
         "lattice_bytes": bst["lattice_bytes"], "tuning": tuning.as_dict(), "chunk_points": chunk,
@@ -537,7 +537,7 @@ def run_c4(args):
                            "build_p99": round(float(np.percentile(build_lag, 99)) * 1e3, 4) if build_lag else None},
         "escalation": {"boundary_points": st["boundary_points"], "fp64_tests": st["esc_fp64"],
                        "exact_tests": st["esc_exact"]},
-        "gpu_launches": 2 * int(st["batches"]), "clocks": clk,
+        "gpu_launches": 4 * int(st["batches"]), "clocks": clk,
         "build_ms": {"resident_set_wall": round(resident_build_s * 1e3, 1), "resident_bytes": resident,
                      "generate_s": round(gen_s, 1), "autotune_s": round(tune_s, 1)},
         "tuning": tuning.as_dict(),
@@ -723,7 +723,8 @@ def main():
         "cpu_baseline": cpu,
         "e2e": {"value": round(e2e_rate, 1), "unit": "Mpts/s", "h2d_bytes_per_step": 16 * e2e_n,
                 "d2h_bytes_per_step": e2e_n},
-        "gpu_launches": 2 * args.steps * ((n + (1 << 27) - 1) // (1 << 27)),
+        # per chunk of 2^27 points: k_locate and the three pass-2 tiers
+        "gpu_launches": 4 * args.steps * ((n + (1 << 27) - 1) // (1 << 27)),
         "clocks": clk,
         "comparison": {
             "fp64_filter_exact_mpts": round(world * n / t64 / 1e6, 1),
