@@ -1060,7 +1060,7 @@ constexpr uint8_t LABEL_PENDING = 0;
 // evict-first policy so the node table stays in L2.  The index arithmetic
 // need not match the canonical conversion bit for bit: every cap carries a
 // margin far above its rounding (see LOC_MARGIN).
-template <bool STATS, bool LOCKSTEP = false>
+template <bool STATS, bool LOCKSTEP = false, int UNROLL = LOC_UNROLL>
 __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t* s_sum,
                                              const double2* __restrict__ ll, uint8_t* __restrict__ out,
                                              uint32_t* __restrict__ queue, unsigned int* __restrict__ qcount,
@@ -1068,26 +1068,26 @@ __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t*
 {
     const int lane = threadIdx.x & 31;
     const int cs = Q.cshift, cw = Q.CW;
-    constexpr int TILE = TPB * LOC_UNROLL;
+    constexpr int TILE = TPB * UNROLL;
     for (int base = tile0 * TILE; base < count; base += tstride * TILE) {
         const bool full = base + TILE <= count;
-        double2 p[LOC_UNROLL];
+        double2 p[UNROLL];
 #pragma unroll
-        for (int k = 0; k < LOC_UNROLL; k++) {
+        for (int k = 0; k < UNROLL; k++) {
             const int i = base + k * TPB + threadIdx.x;
             p[k] = (full || i < count) ? __ldcs(ll + first + i) : make_double2(0.0, 0.0);
         }
-        uint8_t lab[LOC_UNROLL];
-        bool push[LOC_UNROLL];
+        uint8_t lab[UNROLL];
+        bool push[UNROLL];
         bool any = false;
         // LOCKSTEP: the node words of all points are loaded first and the
         // descents advance one level per round, so a thread keeps one
         // independent load per point in flight (points that mostly need the
         // node table, as around small polygons, are bound by its latency)
-        uint32_t w[LOC_UNROLL];
-        double fu[LOC_UNROLL], fv[LOC_UNROLL];
+        uint32_t w[UNROLL];
+        double fu[UNROLL], fv[UNROLL];
 #pragma unroll
-        for (int k = 0; k < LOC_UNROLL; k++) {
+        for (int k = 0; k < UNROLL; k++) {
             const int i = base + k * TPB + threadIdx.x;
             const double lo = p[k].x;
             const double laf = p[k].y + 90.0;  // the reference's FakeLL latitude + 90
@@ -1128,7 +1128,7 @@ __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t*
             while (inner) {
                 inner = false;
 #pragma unroll
-                for (int k = 0; k < LOC_UNROLL; k++)
+                for (int k = 0; k < UNROLL; k++)
                     if ((w[k] & KIND_MASK) == KIND_INNER) {
                         fu[k] *= FAN;
                         fv[k] *= FAN;
@@ -1140,7 +1140,7 @@ __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t*
                     }
             }
 #pragma unroll
-            for (int k = 0; k < LOC_UNROLL; k++) {
+            for (int k = 0; k < UNROLL; k++) {
                 if (lab[k] == LABEL_PENDING && !push[k]) {
                     const int i = base + k * TPB + threadIdx.x;
                     if (full || i < count) {
@@ -1156,7 +1156,7 @@ __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t*
         }
         if (__any_sync(0xffffffffu, any)) {
 #pragma unroll
-            for (int k = 0; k < LOC_UNROLL; k++) {
+            for (int k = 0; k < UNROLL; k++) {
                 const unsigned int mask = __ballot_sync(0xffffffffu, push[k]);
                 if (!mask) continue;
                 unsigned int pos = 0;
@@ -1168,7 +1168,7 @@ __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t*
             }
         }
 #pragma unroll
-        for (int k = 0; k < LOC_UNROLL; k++) {
+        for (int k = 0; k < UNROLL; k++) {
             const int i = base + k * TPB + threadIdx.x;
             if (full || i < count) __stcs(out + first + i, lab[k]);
             if (STATS) inside += lab[k] == CELL_IN;
@@ -1255,6 +1255,7 @@ struct BatchChunk {
 };
 
 constexpr int BATCH_SUMMARY_WORDS = 4096;  // 16 KB of shared memory
+constexpr int BATCH_UNROLL = 8;            // points per thread in flight in the batch locate (84 registers)
 
 // Pass 1 over a batch: a persistent grid takes chunks in order from an atomic
 // counter (polygons of very different sizes balance themselves), stages the
@@ -1279,7 +1280,7 @@ __global__ void __launch_bounds__(TPB) k_batch_locate(const QueryView* __restric
         const QueryView Q = views[c.view];
         for (int k = threadIdx.x; k < Q.swords; k += TPB) s_sum[k] = __ldg(Q.summary + k);
         __syncthreads();
-        locate_range<STATS, true>(Q, s_sum, ll, out, queue, qcount, c.start, c.count, 0, 1, inside);
+        locate_range<STATS, true, BATCH_UNROLL>(Q, s_sum, ll, out, queue, qcount, c.start, c.count, 0, 1, inside);
         __syncthreads();
     }
     allow_dependents();
