@@ -494,8 +494,9 @@ def run_c4(args):
     clk = clocks.stop()
     lat = srv.latencies(0)
     tr = srv.trace()
+    stalls = srv.stalls()
     if args.c4_trace:
-        np.savez(args.c4_trace, trace=tr, latencies=lat, builds=srv.latencies(1))
+        np.savez(args.c4_trace, trace=tr, latencies=lat, builds=srv.latencies(1), stalls=stalls)
     window = t_end - t_start
     srv.close()
     sustained = st["query_points"] / window
@@ -526,6 +527,8 @@ def run_c4(args):
                        "batches": int(st["batches"]), "mean_batch_pieces": round(st["mean_batch_pieces"], 2),
                        "mean_batch_points": round(st["mean_batch_points"], 1),
                        "drain_s": round(t_end - t_submit_end, 4)},
+        "host_stalls": {int(k): [int((stalls[:, 1] == k).sum()), round(float(stalls[stalls[:, 1] == k, 2].max()), 2)]
+                        for k in np.unique(stalls[:, 1])} if len(stalls) else {},
         "batch_trace_ms": {"enqueue_p99": pct(tr[:, 1], 99), "device_p50": pct(tr[:, 2], 50),
                            "device_p99": pct(tr[:, 2], 99), "device_max": pct(tr[:, 2], 100),
                            "complete_p99": pct(tr[:, 3], 99)},

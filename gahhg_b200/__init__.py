@@ -296,6 +296,15 @@ class Server:
             L.gahhg_server_trace(self._h, _lib.ptr(out), n)
         return out
 
+    def stalls(self):
+        """Host-side stalls of 2 ms or more: start (s), kind, ms (kinds in include/gahhg.h)."""
+        L = _lib.lib()
+        n = L.gahhg_server_stalls(self._h, None, 0)
+        out = np.zeros((n, 3), dtype=np.float64)
+        if n:
+            L.gahhg_server_stalls(self._h, _lib.ptr(out), n)
+        return out
+
     def close(self):
         if getattr(self, "_h", None):
             _lib.lib().gahhg_server_free(self._h)

@@ -156,6 +156,7 @@ _SIGS = {
     "gahhg_server_stats_reset": (ctypes.c_int, [_P]),
     "gahhg_server_latencies": (ctypes.c_longlong, [_P, ctypes.c_int, _P, ctypes.c_longlong]),
     "gahhg_server_trace": (ctypes.c_longlong, [_P, _P, ctypes.c_longlong]),
+    "gahhg_server_stalls": (ctypes.c_longlong, [_P, _P, ctypes.c_longlong]),
     "gahhg_server_free": (None, [_P]),
 }
 

@@ -53,6 +53,10 @@ constexpr size_t HDR_BYTES = 64;  // [u32 queue count, next chunk, tier counters
 constexpr size_t CHUNK_BYTES = 16;
 constexpr int MAX_SUMMARY_WORDS = 4096;  // the batch kernel stages at most 16 KB of summary
 constexpr size_t MAX_TRACE = 1 << 20;
+constexpr double STALL_MS = 2.0;
+// stall kinds (gahhg_server_stalls)
+enum { STALL_SUBMIT_LOCK = 1, STALL_POINTER_QUERY = 2, STALL_FREE = 3, STALL_ADMIT = 4, STALL_BUILD = 5,
+       STALL_VIEW_UPLOAD = 6, STALL_LAUNCH = 7, STALL_COPY_OUT = 8 };
 
 struct Req {
     int64_t ticket = 0;
@@ -155,6 +159,61 @@ struct gahhg_server {
     double t0 = 0.0;
     std::vector<double> lat_q, lat_b;
     std::vector<std::array<double, 6>> trace;
+    // Objects released under the server lock are freed after it is dropped:
+    // freeing makes CUDA calls, and a driver call can wait behind another
+    // thread's (a pool growing, say) for hundreds of milliseconds; nothing
+    // that submissions wait for may hold the lock meanwhile.
+    // A reaper thread frees them, so no thread on the query path waits either.
+    std::mutex grave_mu;
+    std::condition_variable cv_grave;
+    bool grave_stop = false;
+    std::vector<Grid*> grave_grids;
+    std::vector<std::unique_ptr<Polygon>> grave_polys;
+    std::thread reaper;
+    void bury_locked(SrvPoly& P)
+    {
+        {
+            std::lock_guard<std::mutex> lk(grave_mu);
+            if (P.grid) grave_grids.push_back(P.grid);
+            if (P.poly) grave_polys.push_back(std::move(P.poly));
+        }
+        P.grid = nullptr;
+        P.poly.reset();
+        cv_grave.notify_one();
+    }
+    void reap_loop()
+    {
+        cudaSetDevice(o.device);
+        std::unique_lock<std::mutex> lk(grave_mu);
+        for (;;) {
+            cv_grave.wait(lk, [&] { return grave_stop || !grave_grids.empty() || !grave_polys.empty(); });
+            std::vector<Grid*> g;
+            std::vector<std::unique_ptr<Polygon>> p;
+            g.swap(grave_grids);
+            p.swap(grave_polys);
+            const bool last = grave_stop;
+            lk.unlock();
+            if (!g.empty() || !p.empty()) {
+                const double tf = now_seconds();
+                for (Grid* x : g) delete x;
+                p.clear();
+                note_stall(STALL_FREE, tf, now_seconds());
+            }
+            lk.lock();
+            if (last && grave_grids.empty() && grave_polys.empty()) break;
+        }
+    }
+
+    // host-side stalls above STALL_MS: (seconds since the window start, kind, ms)
+    std::mutex stall_mu;
+    std::vector<std::array<double, 3>> stalls;
+    void note_stall(int kind, double t_begin, double t_end)
+    {
+        const double ms = (t_end - t_begin) * 1e3;
+        if (ms < STALL_MS) return;
+        std::lock_guard<std::mutex> lk(stall_mu);
+        if (stalls.size() < MAX_TRACE) stalls.push_back({t_begin - t0, (double)kind, ms});
+    }
     long long queries_done = 0, query_points = 0, builds_done = 0, builds_failed = 0, evictions = 0;
     long long batches = 0, pieces = 0, batch_points = 0;
     long long st_boundary = 0, st_fp64 = 0, st_exact = 0, st_in = 0;
@@ -188,9 +247,7 @@ struct gahhg_server {
     void free_poly_locked(int id)
     {
         SrvPoly& P = polys[id];
-        delete P.grid;
-        P.grid = nullptr;
-        P.poly.reset();
+        bury_locked(P);
         committed -= P.bytes;
         resident_bytes -= P.bytes;
         resident--;
@@ -268,8 +325,10 @@ struct gahhg_server {
             }
             sl->points = pts;
             lk.unlock();
+            const double tl = now_seconds();
             const gahhg_status st = launch(sl);
             sl->t_enq = now_seconds();
+            note_stall(STALL_LAUNCH, tl, sl->t_enq);
             lk.lock();
             batches++;
             pieces += (long long)sl->pieces.size();
@@ -371,9 +430,11 @@ struct gahhg_server {
             }
             float dev_ms = 0.f;
             if (err == cudaSuccess) {
+                const double tc = now_seconds();
                 const uint8_t* lab = done->h + lcap - (size_t)done->points;
                 for (const Piece& p : done->pieces) memcpy(p.r->labels + p.a, lab + p.dev, (size_t)p.n);
                 cudaEventElapsedTime(&dev_ms, done->ev0, done->ev);
+                note_stall(STALL_COPY_OUT, tc, now_seconds());
             }
             const double t_done = now_seconds();
             lk.lock();
@@ -462,7 +523,7 @@ struct gahhg_server {
         P.held.clear();
         if (P.build_req) complete_locked(P.build_req, st);
         P.build_req = nullptr;
-        P.poly.reset();
+        bury_locked(P);
     }
 
     void build_loop(int w)
@@ -473,7 +534,9 @@ struct gahhg_server {
             int id = -1;
             cv_build.wait(lk, [&] {
                 if (stop) return true;
+                const double ta = now_seconds();
                 id = admit_locked();
+                note_stall(STALL_ADMIT, ta, now_seconds());
                 return id >= 0;
             });
             if (stop && id < 0) break;
@@ -482,8 +545,10 @@ struct gahhg_server {
             const int top = P.top, leaf = P.leaf;
             lk.unlock();
             Grid* g = nullptr;
+            const double tb = now_seconds();
             gahhg_status st =
                 build_exact_grid(poly, o.device, workers.streams[w], &workers.scans[w], base, top, leaf, &g);
+            note_stall(STALL_BUILD, tb, now_seconds());
             int sw = 0;
             long long bytes = 0;
             std::string msg;
@@ -499,12 +564,14 @@ struct gahhg_server {
                 std::vector<uint8_t> v(view_bytes);
                 lattice_view_write(g, v.data());
                 cudaStream_t ws = workers.streams[w];
+                const double tv = now_seconds();
                 if (cudaMemcpyAsync(d_views + (size_t)id * view_bytes, v.data(), view_bytes, cudaMemcpyHostToDevice,
                                     ws) != cudaSuccess ||
                     cudaStreamSynchronize(ws) != cudaSuccess) {
                     set_error("view upload: %s", cudaGetErrorString(cudaGetLastError()));
                     st = GAHHG_ERR_CUDA;
                 }
+                note_stall(STALL_VIEW_UPLOAD, tv, now_seconds());
                 bytes = (long long)lattice_device_bytes(g->lattice) + (long long)poly->pv_num * 32;
             }
             if (st != GAHHG_OK) {
@@ -576,9 +643,25 @@ struct gahhg_server {
         // freed memory to the driver and mapping it again on the next build
         // would churn page mappings while queries run
         GAHHG_TRY(pool_keep(o.device, (size_t)o.hbm_budget + (4ull << 30)));
+        // map the budget into the pool once, up front: growing the pool
+        // while serving maps physical memory, and every build thread's
+        // allocations waited for it (half-second stalls of all builds)
+        {
+            size_t fr = 0, tot = 0;
+            GAHHG_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+            const size_t want = std::min<size_t>((size_t)o.hbm_budget + ((size_t)4 << 30), (size_t)(0.9 * (double)fr));
+            void* p = nullptr;
+            cudaStream_t s0 = workers.streams[0];
+            if (want > 0 && pool_alloc(&p, want, o.device, s0) == GAHHG_OK) {
+                cudaFreeAsync(p, s0);
+                cudaStreamSynchronize(s0);
+            }
+            cudaGetLastError();
+        }
         t0 = now_seconds();
         dispatcher = std::thread([this] { dispatch_loop(); });
         completer = std::thread([this] { complete_loop(); });
+        reaper = std::thread([this] { reap_loop(); });
         for (int w = 0; w < o.build_workers; w++) builders.emplace_back([this, w] { build_loop(w); });
         return GAHHG_OK;
     }
@@ -622,6 +705,12 @@ struct gahhg_server {
             if (s.d) cudaFree(s.d);
             if (s.d_queue) cudaFree(s.d_queue);
         }
+        {
+            std::lock_guard<std::mutex> lk(grave_mu);
+            grave_stop = true;
+        }
+        cv_grave.notify_all();
+        if (reaper.joinable()) reaper.join();
         for (SrvPoly& P : polys) {
             delete P.grid;
             P.grid = nullptr;
@@ -755,8 +844,11 @@ gahhg_status gahhg_server_submit_query(gahhg_server* s, int id, const double* lo
         cudaPointerAttributes a;
         if (cudaPointerGetAttributes(&a, lonlat) == cudaSuccess && a.type == cudaMemoryTypeHost) r->direct = true;
         cudaGetLastError();
+        s->note_stall(STALL_POINTER_QUERY, r->t_submit, now_seconds());
     }
+    const double tw = now_seconds();
     std::lock_guard<std::mutex> lk(s->mu);
+    s->note_stall(STALL_SUBMIT_LOCK, tw, now_seconds());
     if (s->broken) {
         delete r;
         set_error("server stopped after a device error: %s", s->broken_msg.c_str());
@@ -817,7 +909,7 @@ gahhg_status gahhg_server_drain(gahhg_server* s, double timeout_s) { return s ? 
 gahhg_status gahhg_server_evict(gahhg_server* s, int id)
 {
     if (!s) return GAHHG_ERR_ARG;
-    std::lock_guard<std::mutex> lk(s->mu);
+    std::unique_lock<std::mutex> lk(s->mu);
     if (id >= 0 && id < s->next_id && s->polys[id].state == GAHHG_POLY_FAILED && s->polys[id].refs == 0) {
         s->polys[id].state = GAHHG_POLY_FREE;  // releases the id of a failed build
         s->free_ids.push_back(id);
@@ -827,11 +919,13 @@ gahhg_status gahhg_server_evict(gahhg_server* s, int id)
         set_error("evict: polygon %d is not resident", id);
         return GAHHG_ERR_ARG;
     }
-    SrvPoly& P = s->polys[id];
-    if (P.refs == 0)
-        s->free_poly_locked(id);
-    else
-        P.state = GAHHG_POLY_EVICTING;
+    {
+        SrvPoly& P = s->polys[id];
+        if (P.refs == 0)
+            s->free_poly_locked(id);
+        else
+            P.state = GAHHG_POLY_EVICTING;
+    }
     return GAHHG_OK;
 }
 
@@ -897,6 +991,10 @@ gahhg_status gahhg_server_stats_reset(gahhg_server* s)
     s->lat_q.clear();
     s->lat_b.clear();
     s->trace.clear();
+    {
+        std::lock_guard<std::mutex> lk2(s->stall_mu);
+        s->stalls.clear();
+    }
     s->queries_done = s->query_points = s->builds_done = s->builds_failed = s->evictions = 0;
     s->batches = s->pieces = s->batch_points = 0;
     s->st_boundary = s->st_fp64 = s->st_exact = s->st_in = 0;
@@ -922,6 +1020,16 @@ long long gahhg_server_trace(gahhg_server* s, double* out, long long cap)
         for (long long i = 0; i < std::min<long long>(cap, (long long)s->trace.size()); i++)
             memcpy(out + 6 * i, s->trace[i].data(), 6 * sizeof(double));
     return (long long)s->trace.size();
+}
+
+long long gahhg_server_stalls(gahhg_server* s, double* out, long long cap)
+{
+    if (!s) return 0;
+    std::lock_guard<std::mutex> lk(s->stall_mu);
+    if (out)
+        for (long long i = 0; i < std::min<long long>(cap, (long long)s->stalls.size()); i++)
+            memcpy(out + 3 * i, s->stalls[i].data(), 3 * sizeof(double));
+    return (long long)s->stalls.size();
 }
 
 void gahhg_server_free(gahhg_server* s)

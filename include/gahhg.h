@@ -305,6 +305,13 @@ long long gahhg_server_latencies(gahhg_server* s, int kind, double* out, long lo
  * each - formed (s since the window start), host enqueue ms, device ms,
  * completion ms after forming, points, pieces.  Returns the record count. */
 long long gahhg_server_trace(gahhg_server* s, double* out, long long cap);
+/* Host-side stalls of 2 ms or more since the last stats reset: up to `cap`
+ * records of 3 doubles - start (s since the window start), kind, ms.  Kinds:
+ * 1 waiting for the server lock at submission, 2 the page-locked memory
+ * query at submission, 3 freeing an evicted polygon, 4 admission, 5 a build,
+ * 6 a view upload, 7 enqueueing a batch, 8 copying a batch's labels out.
+ * Returns the record count. */
+long long gahhg_server_stalls(gahhg_server* s, double* out, long long cap);
 /* Drains (up to 60 s), stops the threads and frees everything. */
 void gahhg_server_free(gahhg_server* s);
 
