@@ -320,6 +320,14 @@ def write_result(path, labels):
     check(_lib.lib().gahhg_result_write(str(path).encode(), _lib.ptr(labels), len(labels)))
 
 
+def staging_fallbacks(device=0):
+    """Locate blocks on `device` whose bulk copy of the coarse summary ran out
+    of time and fell back to plain loads (0 in normal operation)."""
+    v = ctypes.c_ulonglong(0)
+    check(_lib.lib().gahhg_staging_fallbacks(int(device), ctypes.byref(v)))
+    return int(v.value)
+
+
 def grid0():
     V = np.zeros((80, 3), dtype=np.float64)
     B = np.zeros(240, dtype=BORDER_DTYPE)

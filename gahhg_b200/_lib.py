@@ -109,6 +109,7 @@ _SIGS = {
     "gahhg_build_opts_init": (None, [ctypes.POINTER(BuildOpts)]),
     "gahhg_last_error": (ctypes.c_char_p, []),
     "gahhg_abi_version": (ctypes.c_int, []),
+    "gahhg_staging_fallbacks": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong)]),
     "gahhg_polygon_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_P)]),
     "gahhg_polygon_from_rings": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.POINTER(_P)]),
     "gahhg_polygon_num_edges": (ctypes.c_int, [_P]),

@@ -197,6 +197,15 @@ void gahhg_build_opts_init(gahhg_build_opts* o)
 const char* gahhg_last_error(void) { return last_error(); }
 int gahhg_abi_version(void) { return GAHHG_ABI_VERSION; }
 
+gahhg_status gahhg_staging_fallbacks(int device, unsigned long long* count)
+{
+    if (!count) {
+        set_error("null count");
+        return GAHHG_ERR_ARG;
+    }
+    return lattice_staging_fallbacks(device, count);
+}
+
 gahhg_status gahhg_polygon_load(const char* path, gahhg_polygon** out)
 {
     if (!path || !out) return GAHHG_ERR_ARG;

@@ -212,6 +212,8 @@ size_t lattice_view_bytes();
 size_t batch_chunk_bytes();
 void lattice_view_write(const Grid* g, void* dst);
 long long lattice_summary_words(const Grid* g);
+// Locate blocks on `device` whose summary copy ran out of time (plain loads instead).
+gahhg_status lattice_staging_fallbacks(int device, unsigned long long* out);
 // Chunks over segments of points stored segment after segment; segment p's
 // points belong to view seg_view[p] (p itself when seg_view is null).
 void batch_make_chunks(const long long* offsets, int nseg, int chunk_points, const int* swords, const int* seg_view,

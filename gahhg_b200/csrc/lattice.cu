@@ -912,6 +912,64 @@ __device__ uint8_t leaf_label(const QueryView& Q, uint32_t leaf, PointCtx& P, bo
 __device__ __forceinline__ void wait_for_predecessor() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void allow_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+// ------------------------------------------- summary staging by bulk copy --
+//
+// The coarse summary (up to 16 KB) goes to shared memory by one bulk copy
+// (TMA, untiled cp.async.bulk global -> shared, completion counted on an
+// mbarrier in bytes; no multicast) issued by one thread, instead of a load
+// per word by every thread.  Both addresses are 16-byte aligned (pool
+// allocations are 256-byte aligned, the shared arrays are declared so) and
+// the size is rounded up to 16 bytes (the summary's allocation holds at least
+// 1,024 words).  Every wait is bounded; a wait that runs out is counted in
+// g_tma_timeouts and the block falls back to loading the summary itself into
+// memory no pending copy can write (see the kernels), so labels never depend
+// on a copy completing.
+
+__device__ unsigned int g_tma_timeouts;
+constexpr int MBAR_POLL_LIMIT = 1 << 20;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// One thread: the copy of `bytes` from global `src` to shared `dst`,
+// completing the barrier's current phase.
+__device__ __forceinline__ void bulk_stage(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    // earlier generic-proxy reads of dst (ordered by the block barrier) come
+    // before the async-proxy write
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Bounded wait for the phase with the given parity; false when it ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+{
+    for (int i = 0; i < MBAR_POLL_LIMIT; i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__host__ __device__ __forceinline__ uint32_t summary_bytes(int swords) { return ((uint32_t)swords * 4u + 15u) & ~15u; }
+
 // ------------------------------------------------------ escalation tiers --
 //
 // The crossing tests of the queued points run in tiers, each its own launch
@@ -1181,11 +1239,27 @@ __global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, 
                                                QueryView Q, uint32_t* __restrict__ queue,
                                                unsigned int* __restrict__ qcount, unsigned long long* ctr)
 {
-    extern __shared__ uint32_t s_sum[];
-    for (int k = threadIdx.x; k < Q.swords; k += TPB) s_sum[k] = __ldg(Q.summary + k);
+    extern __shared__ __align__(16) uint32_t s_sum[];
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ int s_late;
+    if (threadIdx.x == 0) {
+        s_late = 0;
+        mbar_init(&s_bar);
+        bulk_stage(s_sum, Q.summary, summary_bytes(Q.swords), &s_bar);
+    }
     __syncthreads();
+    if (!mbar_wait(&s_bar, 0)) s_late = 1;
+    __syncthreads();
+    const bool late = s_late != 0;
+    if (late) {
+        // the pending copy can only write these same words
+        if (threadIdx.x == 0) atomicAdd(&g_tma_timeouts, 1u);
+        for (int k = threadIdx.x; k < Q.swords; k += TPB) s_sum[k] = __ldg(Q.summary + k);
+        __syncthreads();
+    }
     int inside = 0;
     locate_range<STATS>(Q, s_sum, ll, out, queue, qcount, 0, n, blockIdx.x, gridDim.x, inside);
+    if (late) mbar_wait(&s_bar, 0);  // the copy in flight ends before the block does (bounded)
     allow_dependents();
     if (STATS && ctr) count_inside(inside, ctr + 3);
 }
@@ -1268,8 +1342,18 @@ __global__ void __launch_bounds__(TPB) k_batch_locate(const QueryView* __restric
                                                      uint8_t* __restrict__ out, uint32_t* __restrict__ queue,
                                                      unsigned int* __restrict__ qcount, unsigned long long* ctr)
 {
-    __shared__ uint32_t s_sum[BATCH_SUMMARY_WORDS];
-    __shared__ int s_chunk;
+    // s_sum receives the bulk copies; after a wait runs out the block loads
+    // summaries itself into s_own, which no copy writes
+    __shared__ __align__(16) uint32_t s_sum[BATCH_SUMMARY_WORDS];
+    __shared__ __align__(16) uint32_t s_own[BATCH_SUMMARY_WORDS];
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ int s_chunk, s_late;
+    if (threadIdx.x == 0) {
+        s_late = 0;
+        mbar_init(&s_bar);
+    }
+    uint32_t phase = 0;
+    bool late = false;  // the same in every thread: read from s_late after a barrier
     int inside = 0;
     for (;;) {
         if (threadIdx.x == 0) s_chunk = (int)atomicAdd(next_chunk, 1u);
@@ -1278,10 +1362,25 @@ __global__ void __launch_bounds__(TPB) k_batch_locate(const QueryView* __restric
         if (ci >= nchunks) break;
         const BatchChunk c = chunks[ci];
         const QueryView Q = views[c.view];
-        for (int k = threadIdx.x; k < Q.swords; k += TPB) s_sum[k] = __ldg(Q.summary + k);
+        const uint32_t* sum = s_sum;
+        if (!late) {
+            if (threadIdx.x == 0) bulk_stage(s_sum, Q.summary, summary_bytes(Q.swords), &s_bar);
+            if (!mbar_wait(&s_bar, phase)) s_late = 1;  // any thread's timeout switches the block
+            phase ^= 1u;
+            __syncthreads();
+            late = s_late != 0;
+        }
+        if (late) {
+            for (int k = threadIdx.x; k < Q.swords; k += TPB) s_own[k] = __ldg(Q.summary + k);
+            sum = s_own;
+            __syncthreads();
+        }
+        locate_range<STATS, true, BATCH_UNROLL>(Q, sum, ll, out, queue, qcount, c.start, c.count, 0, 1, inside);
         __syncthreads();
-        locate_range<STATS, true, BATCH_UNROLL>(Q, s_sum, ll, out, queue, qcount, c.start, c.count, 0, 1, inside);
-        __syncthreads();
+    }
+    if (late) {
+        if (threadIdx.x == 0) atomicAdd(&g_tma_timeouts, 1u);
+        mbar_wait(&s_bar, phase ^ 1u);  // the copy in flight ends before the block does (bounded)
     }
     allow_dependents();
     if (STATS && ctr) count_inside(inside, ctr + 3);
@@ -2081,7 +2180,7 @@ gahhg_status lattice_build(Grid* g)
         k_shift_leaf_words<<<blocks_for(lv[lvl].nn), TPB, 0, s>>>(L->nodes.ptr, lv[lvl].gstart, lv[lvl].nn, leaf_base[lvl]);
     }
     {
-        // coarse summary: at most 256 x 128 cells (8 KB), staged in shared memory by the query
+        // coarse summary: at most 65,536 cells (16 KB), staged in shared memory by the query
         int cs = 0;
         auto blocks = [&](int c) { return (long long)((W + (1 << c) - 1) >> c) * ((H + (1 << c) - 1) >> c); };
         while (blocks(cs) > 65536) cs++;
@@ -2188,9 +2287,9 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
         const long long tiles = ((long long)m + TPB * LOC_UNROLL - 1) / (TPB * LOC_UNROLL);
         const int grid = (int)std::min<long long>(tiles, (long long)sms * 8);
         if (ctr)
-            k_locate<true><<<grid, TPB, sizeof(uint32_t) * Q.swords, s>>>(ll, m, d_labels + off, Q, queue, qcount, ctr);
+            k_locate<true><<<grid, TPB, summary_bytes(Q.swords), s>>>(ll, m, d_labels + off, Q, queue, qcount, ctr);
         else
-            k_locate<false><<<grid, TPB, sizeof(uint32_t) * Q.swords, s>>>(ll, m, d_labels + off, Q, queue, qcount, ctr);
+            k_locate<false><<<grid, TPB, summary_bytes(Q.swords), s>>>(ll, m, d_labels + off, Q, queue, qcount, ctr);
         if (tiers)
             leaf_tiers_launch(OneView{Q}, ll, d_labels + off, queue, qcount, *tiers, precision, ctr, sms, s);
         else if (precision == GAHHG_QUERY_FP64_FILTER)
@@ -2270,6 +2369,15 @@ void lattice_view_write(const Grid* g, void* dst)
 }
 
 long long lattice_summary_words(const Grid* g) { return g->lattice ? g->lattice->swords : 0; }
+
+gahhg_status lattice_staging_fallbacks(int device, unsigned long long* out)
+{
+    GAHHG_CUDA_TRY(cudaSetDevice(device));
+    unsigned int v = 0;
+    GAHHG_CUDA_TRY(cudaMemcpyFromSymbol(&v, g_tma_timeouts, sizeof(v)));
+    *out = v;
+    return GAHHG_OK;
+}
 
 // Chunks of at most `chunk_points` points, segment after segment.
 // A segment's chunks hold at least 16 points per word of its summary, so

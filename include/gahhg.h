@@ -333,6 +333,12 @@ gahhg_status gahhg_result_write(const char* path, const uint8_t* labels, size_t 
 /* The level-0 grid (80 vertices, 240 borders, 42 cells). */
 gahhg_status gahhg_grid0_export(double* v, void* b, void* c);
 
+/* Pass-1 (locate) blocks on `device` whose bulk copy (TMA) of the coarse
+ * summary into shared memory did not complete within the bounded wait, since
+ * the library was loaded.  Such a block loads the summary with plain loads
+ * instead, so labels are unaffected; 0 in normal operation. */
+gahhg_status gahhg_staging_fallbacks(int device, unsigned long long* count);
+
 const char* gahhg_last_error(void);
 int gahhg_abi_version(void);
 
