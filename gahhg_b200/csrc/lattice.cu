@@ -1329,7 +1329,7 @@ struct BatchChunk {
 };
 
 constexpr int BATCH_SUMMARY_WORDS = 4096;  // 16 KB of shared memory
-constexpr int BATCH_UNROLL = 8;            // points per thread in flight in the batch locate (84 registers)
+constexpr int BATCH_UNROLL = 8;            // points per thread in flight in the batch locate (86 registers)
 
 // Pass 1 over a batch: a persistent grid takes chunks in order from an atomic
 // counter (polygons of very different sizes balance themselves), stages the
