@@ -696,7 +696,7 @@ __global__ void k_leaf_flags(int nn, const int* cnt, const int* child_base, int*
 __global__ void k_leaf_records(BuildView v, int lvl, int nn, const int* is_leaf, const int* leaf_off,
                                const int* rec_off, int leaf_base, long long rec_base, const long long* ix,
                                const long long* iy, const int* cnt, const int* off, const int* list,
-                               const uint8_t* label, LeafRec* leaves, EdgeRec* recs, int* bad)
+                               const uint8_t* label, LeafRec* leaves, EdgeRec* recs, uint32_t* eids, int* bad)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nn || !is_leaf[p]) return;
@@ -731,7 +731,20 @@ __global__ void k_leaf_records(BuildView v, int lvl, int nn, const int* is_leaf,
         if (s1 == 0) atomicAdd(bad, 1);
         r.es = (uint32_t)e | (s1 > 0 ? 0x80000000u : 0u);
         recs[ro + k] = r;
+        eids[ro + k] = r.es;
     }
+}
+
+// The FP64 endpoints of every edge side by side, so the FP64 tier reads an
+// edge with three aligned 16-byte loads instead of the chain pe -> pv.
+__global__ void k_edge_ends(const D3* pv, const int* pe, int n, double2* ends)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const D3 a = pv[pe[2 * e]], b = pv[pe[2 * e + 1]];
+    ends[3 * (size_t)e + 0] = make_double2(a.x, a.y);
+    ends[3 * (size_t)e + 1] = make_double2(a.z, b.x);
+    ends[3 * (size_t)e + 2] = make_double2(b.y, b.z);
 }
 
 // Coarse summary of the top level: a coarse cell whose top cells are all
@@ -795,6 +808,8 @@ struct QueryView {
     const uint32_t* nodes;
     const LeafRec* leaves;
     const EdgeRec* recs;
+    const uint32_t* eids;     // per record: its edge id and sign bit (EdgeRec::es), 4 B apart
+    const double2* ends;      // per edge: A.xy, A.z B.x, B.yz (48 B, one aligned load each)
     const D3* pv;
     const int* pe;
 };
@@ -1007,31 +1022,51 @@ __device__ uint8_t leaf_label_fp32(const QueryView& Q, uint32_t leaf, const Poin
     return (uint8_t)(par ? 3 - L.label : L.label);
 }
 
+// Edges of a leaf whose FP64 endpoints the FP64 tier loads together: their
+// loads (edge id, then three 16-byte loads of the endpoints) are all in flight
+// before the first sign is evaluated, instead of one dependent chain per edge.
+constexpr int T2_GROUP = 4;
+
 __device__ uint8_t leaf_label_fp64(const QueryView& Q, uint32_t leaf, PointCtx& P)
 {
     const LeafRec L = Q.leaves[leaf];
     P.need64();
     double LR[3];
     gahhg_canon_vertex_xyz(L.lon, L.lat, LR);
+    const int cnt = L.cnt;
     int par = 0;
-    for (int k = 0; k < L.cnt; k++) {
-        const EdgeRec r = Q.recs[L.off + k];
-        const int e = (int)(r.es & 0x7fffffffu);
-        const int s1 = (r.es >> 31) ? 1 : -1;
-        const D3 a = Q.pv[Q.pe[2 * e]], b = Q.pv[Q.pe[2 * e + 1]];
-        const double A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z};
-        if (exact::same(P.q, A) || exact::same(P.q, B)) return CELL_IN;  // vertex rule
-        if (exact::same(P.q, LR)) return L.label;                       // q is the center
-        // every row is within a cap of the first: translated rows keep the bound small
-        const int s2 = exact::orient_fp64_near(A, B, P.q);
-        if (s2 == 0) return LABEL_DEFER;
-        if (s2 == s1) continue;
-        const int s3 = exact::orient_fp64_near(LR, P.q, A);
-        if (s3 == 0) return LABEL_DEFER;
-        if (s3 != s2) continue;
-        const int s4 = exact::orient_fp64_near(LR, P.q, B);
-        if (s4 == 0) return LABEL_DEFER;
-        if (s4 == -s2) par ^= 1;
+    for (int k0 = 0; k0 < cnt; k0 += T2_GROUP) {
+        uint32_t es[T2_GROUP];
+        double2 e[T2_GROUP][3];
+#pragma unroll
+        for (int j = 0; j < T2_GROUP; j++) es[j] = k0 + j < cnt ? __ldg(Q.eids + L.off + k0 + j) : 0u;
+#pragma unroll
+        for (int j = 0; j < T2_GROUP; j++) {
+            if (k0 + j < cnt) {
+                const double2* p = Q.ends + 3 * (size_t)(es[j] & 0x7fffffffu);
+                e[j][0] = __ldg(p);
+                e[j][1] = __ldg(p + 1);
+                e[j][2] = __ldg(p + 2);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < T2_GROUP; j++) {
+            if (k0 + j >= cnt) break;
+            const int s1 = (es[j] >> 31) ? 1 : -1;
+            const double A[3] = {e[j][0].x, e[j][0].y, e[j][1].x}, B[3] = {e[j][1].y, e[j][2].x, e[j][2].y};
+            if (exact::same(P.q, A) || exact::same(P.q, B)) return CELL_IN;  // vertex rule
+            if (exact::same(P.q, LR)) return L.label;                       // q is the center
+            // every row is within a cap of the first: translated rows keep the bound small
+            const int s2 = exact::orient_fp64_near(A, B, P.q);
+            if (s2 == 0) return LABEL_DEFER;
+            if (s2 == s1) continue;
+            const int s3 = exact::orient_fp64_near(LR, P.q, A);
+            if (s3 == 0) return LABEL_DEFER;
+            if (s3 != s2) continue;
+            const int s4 = exact::orient_fp64_near(LR, P.q, B);
+            if (s4 == 0) return LABEL_DEFER;
+            if (s4 == -s2) par ^= 1;
+        }
     }
     return (uint8_t)(par ? 3 - L.label : L.label);
 }
@@ -1596,8 +1631,11 @@ struct Lattice {
     DevArray<uint32_t> nodes;
     DevArray<LeafRec> leaves;
     DevArray<EdgeRec> recs;
+    DevArray<uint32_t> eids;
+    DevArray<double2> ends;
     DevArray<uint32_t> summary;
     int cshift = 0, swords = 0;
+    long long nedges = 0;
     int outside_label = 0;
     long long nnodes = 0, nleaves = 0, nrecs = 0;
     int origin_label = 0;
@@ -1610,6 +1648,8 @@ void lattice_free(Lattice* L)
     L->nodes.release();
     L->leaves.release();
     L->recs.release();
+    L->eids.release();
+    L->ends.release();
     L->summary.release();
     delete L;
 }
@@ -1617,14 +1657,15 @@ void lattice_free(Lattice* L)
 size_t lattice_bytes(const Lattice* L)
 {
     if (!L) return 0;
-    return L->nnodes * sizeof(uint32_t) + L->nleaves * sizeof(LeafRec) + L->nrecs * sizeof(EdgeRec);
+    return L->nnodes * sizeof(uint32_t) + L->nleaves * sizeof(LeafRec) +
+           L->nrecs * (sizeof(EdgeRec) + sizeof(uint32_t)) + L->nedges * 3 * sizeof(double2);
 }
 
 size_t lattice_device_bytes(const Lattice* L)
 {
     if (!L) return 0;
     return L->nodes.cap * sizeof(uint32_t) + L->leaves.cap * sizeof(LeafRec) + L->recs.cap * sizeof(EdgeRec) +
-           L->summary.cap * sizeof(uint32_t);
+           L->eids.cap * sizeof(uint32_t) + L->ends.cap * sizeof(double2) + L->summary.cap * sizeof(uint32_t);
 }
 
 namespace {
@@ -2163,14 +2204,18 @@ gahhg_status lattice_build(Grid* g)
     }
     GAHHG_TRY(L->leaves.reserve(std::max(leaf_total, 1LL), s, false));
     GAHHG_TRY(L->recs.reserve(std::max(rec_total, 1LL), s, false));
+    GAHHG_TRY(L->eids.reserve(std::max(rec_total, 1LL), s, false));
+    GAHHG_TRY(L->ends.reserve(3 * (size_t)std::max(n, 1), s, false));
     L->nleaves = leaf_total;
     L->nrecs = rec_total;
+    L->nedges = n;
+    k_edge_ends<<<blocks_for(n), TPB, 0, s>>>(bv.pv, bv.pe, n, L->ends.ptr);
     for (int lvl = 0; lvl < L->nlev; lvl++) {
         LevelBuf& b = lv[lvl];
         k_leaf_records<<<blocks_for(b.nn), TPB, 0, s>>>(bv, lvl, b.nn, is_leaf[lvl].ptr, leaf_off[lvl].ptr,
                                                         rec_off[lvl].ptr, leaf_base[lvl], rec_base[lvl], b.ix.ptr,
                                                         b.iy.ptr, b.cnt.ptr, b.off.ptr, b.list.ptr, b.label.ptr,
-                                                        L->leaves.ptr, L->recs.ptr, d_bad);
+                                                        L->leaves.ptr, L->recs.ptr, L->eids.ptr, d_bad);
     }
     GAHHG_CUDA_TRY(cudaGetLastError());
     GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
@@ -2235,6 +2280,8 @@ QueryView make_view(const Grid* g)
     Q.nodes = L->nodes.ptr;
     Q.leaves = L->leaves.ptr;
     Q.recs = L->recs.ptr;
+    Q.eids = L->eids.ptr;
+    Q.ends = L->ends.ptr;
     Q.pv = g->poly->d_pv;
     Q.pe = g->poly->d_pe;
     Q.cshift = L->cshift;
