@@ -221,8 +221,8 @@ void batch_make_chunks(const long long* offsets, int nseg, int chunk_points, con
 void batch_write_chunks(const long long* offsets, int nseg, int chunk_points, const int* swords, const int* seg_view,
                         void* out, int* nchunks);
 size_t batch_chunk_count_bound(long long points, int nseg, int chunk_points);
-// Words of a batch queue whose pass-2 part holds queue_cap points (the
-// escalation queues follow it).
+// Words of a batch queue whose pass-2 part holds queue_cap points (with their
+// leaf words; the escalation queues and theirs follow).
 size_t batch_queue_words(long long queue_cap);
 // counters[0..4] must be zero on entry unless zero_counters is set.
 gahhg_status batch_query_launch(const void* d_views, const void* d_chunks, int nchunks, const double* d_lonlat,

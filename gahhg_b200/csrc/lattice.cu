@@ -1138,6 +1138,9 @@ __device__ __forceinline__ void count_inside(int v, unsigned long long* dst)
 
 constexpr int LOC_UNROLL = 4;
 constexpr uint8_t LABEL_PENDING = 0;
+// Leaf word of a queued point that pass 1 did not locate (a pure node
+// without a label, which is never queued).
+constexpr uint32_t LEAF_UNKNOWN = KIND_PURE;
 
 // Pass 1: every point whose cell has no edges gets its label; the others are
 // queued (index within this chunk) for pass 2.  Lean on registers and
@@ -1156,8 +1159,9 @@ constexpr uint8_t LABEL_PENDING = 0;
 template <bool STATS, bool LOCKSTEP = false, int UNROLL = LOC_UNROLL>
 __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t* s_sum,
                                              const double2* __restrict__ ll, uint8_t* __restrict__ out,
-                                             uint32_t* __restrict__ queue, unsigned int* __restrict__ qcount,
-                                             long long first, int count, int tile0, int tstride, int& inside)
+                                             uint32_t* __restrict__ queue, uint32_t* __restrict__ leafq,
+                                             unsigned int* __restrict__ qcount, long long first, int count,
+                                             int tile0, int tstride, int& inside)
 {
     const int lane = threadIdx.x & 31;
     const int cs = Q.cshift, cw = Q.CW;
@@ -1207,6 +1211,7 @@ __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t*
                                 lab[k] = (uint8_t)(d & 3u);
                             else
                                 push[k] = true;
+                            w[k] = d;
                         }
                     }
                 } else {
@@ -1256,8 +1261,12 @@ __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t*
                 const int leader = __ffs(mask) - 1;
                 if (lane == leader) pos = atomicAdd(qcount, (unsigned int)__popc(mask));
                 pos = __shfl_sync(0xffffffffu, pos, leader);
-                if (push[k])
-                    queue[pos + __popc(mask & ((1u << lane) - 1u))] = (uint32_t)(first + base + k * TPB + threadIdx.x);
+                if (push[k]) {
+                    const unsigned int at = pos + __popc(mask & ((1u << lane) - 1u));
+                    queue[at] = (uint32_t)(first + base + k * TPB + threadIdx.x);
+                    // w is the leaf word, or KIND_PURE (LEAF_UNKNOWN) for an unlocated point
+                    if (leafq) leafq[at] = w[k];
+                }
             }
         }
 #pragma unroll
@@ -1272,7 +1281,8 @@ __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t*
 template <bool STATS>
 __global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, int n, uint8_t* __restrict__ out,
                                                QueryView Q, uint32_t* __restrict__ queue,
-                                               unsigned int* __restrict__ qcount, unsigned long long* ctr)
+                                               uint32_t* __restrict__ leafq, unsigned int* __restrict__ qcount,
+                                               unsigned long long* ctr)
 {
     extern __shared__ __align__(16) uint32_t s_sum[];
     __shared__ __align__(8) uint64_t s_bar;
@@ -1293,7 +1303,7 @@ __global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, 
         __syncthreads();
     }
     int inside = 0;
-    locate_range<STATS>(Q, s_sum, ll, out, queue, qcount, 0, n, blockIdx.x, gridDim.x, inside);
+    locate_range<STATS>(Q, s_sum, ll, out, queue, leafq, qcount, 0, n, blockIdx.x, gridDim.x, inside);
     if (late) mbar_wait(&s_bar, 0);  // the copy in flight ends before the block does (bounded)
     allow_dependents();
     if (STATS && ctr) count_inside(inside, ctr + 3);
@@ -1301,7 +1311,11 @@ __global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, 
 
 // The leaf of a queued point (the point context filled in), or its label
 // with KIND_PURE when its cell has no edges.
-__device__ __forceinline__ uint32_t point_leaf(const QueryView& Q, double2 p, PointCtx& P)
+// The point's context, and its node word: `known` when pass 1 located the
+// point (any leaf it finds serves: every leaf cap holds its points with a
+// margin above the locate arithmetic's rounding), else a descent from the top.
+__device__ __forceinline__ uint32_t point_leaf(const QueryView& Q, double2 p, PointCtx& P,
+                                              uint32_t known = LEAF_UNKNOWN)
 {
     P.lat = gahhg_canon_query_lat(p.y);
     P.lon = p.x;
@@ -1321,6 +1335,7 @@ __device__ __forceinline__ uint32_t point_leaf(const QueryView& Q, double2 p, Po
     if (lr < -180.0) lr += 360.0;
     P.lon_r = lr;
     P.lat_r = la;
+    if (known != LEAF_UNKNOWN) return known;
     const bool in = domain_locate(Q, lo, la + 90.0, L);
     return in ? descend(Q, __ldg(Q.nodes + (size_t)L.iy * Q.W + L.ix), L.fu, L.fv) : Q.outside;
 }
@@ -1375,7 +1390,8 @@ __global__ void __launch_bounds__(TPB) k_batch_locate(const QueryView* __restric
                                                      const BatchChunk* __restrict__ chunks, int nchunks,
                                                      unsigned int* next_chunk, const double2* __restrict__ ll,
                                                      uint8_t* __restrict__ out, uint32_t* __restrict__ queue,
-                                                     unsigned int* __restrict__ qcount, unsigned long long* ctr)
+                                                     uint32_t* __restrict__ leafq, unsigned int* __restrict__ qcount,
+                                                     unsigned long long* ctr)
 {
     // s_sum receives the bulk copies; after a wait runs out the block loads
     // summaries itself into s_own, which no copy writes
@@ -1410,7 +1426,8 @@ __global__ void __launch_bounds__(TPB) k_batch_locate(const QueryView* __restric
             sum = s_own;
             __syncthreads();
         }
-        locate_range<STATS, true, BATCH_UNROLL>(Q, sum, ll, out, queue, qcount, c.start, c.count, 0, 1, inside);
+        locate_range<STATS, true, BATCH_UNROLL>(Q, sum, ll, out, queue, leafq, qcount, c.start, c.count, 0, 1,
+                                                inside);
         __syncthreads();
     }
     if (late) {
@@ -1426,9 +1443,15 @@ __global__ void __launch_bounds__(TPB) k_batch_locate(const QueryView* __restric
 // cnt[2] is raised when a point found its queue full: it stays unlabelled
 // (pass 1 wrote LABEL_PENDING) and the final sweep gives it the complete
 // test, so no tier carries the code of the tiers after it.
+// Every queue of points has a parallel array of leaf words (l1 for the
+// pass-1 queue): the node word pass 1 found for the point, or LEAF_UNKNOWN
+// when it did not locate it, so the tiers need not descend again.
 struct Tiers {
     uint32_t* q2;
     uint32_t* q3;
+    uint32_t* l1;
+    uint32_t* l2;
+    uint32_t* l3;
     unsigned int* cnt;
     unsigned int cap2, cap3;
 };
@@ -1458,7 +1481,8 @@ struct ChunkViews {
 
 // Appends i to q through counter *c, one atomic per group of converged
 // threads; false when the queue is full.
-__device__ __forceinline__ bool push_deferred(uint32_t i, uint32_t* q, unsigned int* c, unsigned int cap)
+__device__ __forceinline__ bool push_deferred(uint32_t i, uint32_t w, uint32_t* q, uint32_t* l, unsigned int* c,
+                                              unsigned int cap)
 {
     const unsigned int act = __activemask();
     const int lane = threadIdx.x & 31;
@@ -1469,6 +1493,7 @@ __device__ __forceinline__ bool push_deferred(uint32_t i, uint32_t* q, unsigned 
     const unsigned int pos = base + __popc(act & ((1u << lane) - 1u));
     if (pos >= cap) return false;
     q[pos] = i;
+    l[pos] = w;
     return true;
 }
 
@@ -1494,7 +1519,7 @@ __global__ void __launch_bounds__(TPB) k_leaf_t1(VS vs, const double2* __restric
         const uint32_t i = queue[t];
         const QueryView& Q = vs.of(i);
         PointCtx P;
-        const uint32_t w = point_leaf(Q, ll[i], P);
+        const uint32_t w = point_leaf(Q, ll[i], P, T.l1[t]);
         uint8_t lab;
         if ((w & KIND_MASK) == KIND_PURE) {
             lab = (uint8_t)(w & 3u);
@@ -1503,7 +1528,7 @@ __global__ void __launch_bounds__(TPB) k_leaf_t1(VS vs, const double2* __restric
             lab = leaf_label_fp32(Q, w & INDEX_MASK, P);
             if (lab == LABEL_DEFER) {
                 fp64++;
-                if (!push_deferred(i, T.q2, T.cnt, T.cap2)) T.cnt[2] = 1;
+                if (!push_deferred(i, w, T.q2, T.l2, T.cnt, T.cap2)) T.cnt[2] = 1;
                 continue;
             }
         }
@@ -1518,7 +1543,7 @@ __global__ void __launch_bounds__(TPB) k_leaf_t1(VS vs, const double2* __restric
 // the pass-1 queue itself.
 template <class VS, bool FROM_PASS1>
 __global__ void __launch_bounds__(TPB) k_leaf_t2(VS vs, const double2* __restrict__ ll, uint8_t* __restrict__ out,
-                                                const uint32_t* __restrict__ src,
+                                                const uint32_t* __restrict__ src, const uint32_t* __restrict__ src_leaf,
                                                 const unsigned int* __restrict__ src_count, unsigned int src_cap,
                                                 Tiers T, unsigned long long* ctr)
 {
@@ -1529,7 +1554,7 @@ __global__ void __launch_bounds__(TPB) k_leaf_t2(VS vs, const double2* __restric
         const uint32_t i = src[t];
         const QueryView& Q = vs.of(i);
         PointCtx P;
-        const uint32_t w = point_leaf(Q, ll[i], P);
+        const uint32_t w = point_leaf(Q, ll[i], P, src_leaf[t]);
         uint8_t lab;
         if ((w & KIND_MASK) == KIND_PURE) {
             lab = (uint8_t)(w & 3u);
@@ -1538,7 +1563,7 @@ __global__ void __launch_bounds__(TPB) k_leaf_t2(VS vs, const double2* __restric
             lab = leaf_label_fp64(Q, w & INDEX_MASK, P);
             if (lab == LABEL_DEFER) {
                 exact++;
-                if (!push_deferred(i, T.q3, T.cnt + 1, T.cap3)) T.cnt[2] = 1;
+                if (!push_deferred(i, w, T.q3, T.l3, T.cnt + 1, T.cap3)) T.cnt[2] = 1;
                 continue;
             }
         }
@@ -1563,16 +1588,18 @@ __global__ void __launch_bounds__(TPB) k_leaf_t3(VS vs, const double2* __restric
     const unsigned int m = sweep ? *qcount : 0;
     int inside = 0;
     for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < m3 + m; t += gridDim.x * blockDim.x) {
-        uint32_t i;
+        uint32_t i, known;
         if (t < m3) {
             i = T.q3[t];
+            known = T.l3[t];
         } else {
             i = queue[t - m3];
             if (out[i] != LABEL_PENDING) continue;
+            known = T.l1[t - m3];
         }
         const QueryView& Q = vs.of(i);
         PointCtx P;
-        const uint32_t w = point_leaf(Q, ll[i], P);
+        const uint32_t w = point_leaf(Q, ll[i], P, known);
         const uint8_t lab = ((w & KIND_MASK) == KIND_PURE) ? (uint8_t)(w & 3u)
                                                             : leaf_label(Q, w & INDEX_MASK, P, false, nullptr);
         out[i] = lab;
@@ -1605,11 +1632,12 @@ void leaf_tiers_launch(const VS& vs, const double2* ll, uint8_t* out, const uint
                        cudaStream_t s)
 {
     if (precision == GAHHG_QUERY_FP64_FILTER) {
-        launch_dependent(k_leaf_t2<VS, true>, sms * 4, s, vs, ll, out, queue, qcount, 0xffffffffu, T, ctr);
+        launch_dependent(k_leaf_t2<VS, true>, sms * 4, s, vs, ll, out, queue, (const uint32_t*)T.l1, qcount,
+                         0xffffffffu, T, ctr);
     } else {
         launch_dependent(k_leaf_t1<VS>, sms * 4, s, vs, ll, out, queue, qcount, T, ctr);
         launch_dependent(k_leaf_t2<VS, false>, sms * 4, s, vs, ll, out, (const uint32_t*)T.q2,
-                         (const unsigned int*)T.cnt, T.cap2, T, ctr);
+                         (const uint32_t*)T.l2, (const unsigned int*)T.cnt, T.cap2, T, ctr);
     }
     launch_dependent(k_leaf_t3<VS>, sms * 2, s, vs, ll, out, queue, qcount, T, ctr);
 }
@@ -2300,16 +2328,21 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
     if (n == 0) return GAHHG_OK;
     const QueryView Q = make_view(g);
     const long long chunk = std::min<long long>((long long)n, QUERY_CHUNK);
-    // [pass-2 queue][counters: queue fill, tier-2 fill, tier-3 fill, overflow][tier-2 queue][tier-3 queue]
+    // [pass-2 queue][counters: queue fill, tier-2 fill, tier-3 fill, overflow]
+    // [pass-2 leaf words][tier-2 queue][its leaf words][tier-3 queue][its leaf words]
     unsigned int cap2 = 0, cap3 = 0;
     tier_caps(chunk, &cap2, &cap3);
     uint32_t* queue = nullptr;
-    GAHHG_TRY(pool_alloc((void**)&queue, sizeof(uint32_t) * (chunk + 64 + (size_t)cap2 + cap3), g->device, s));
+    GAHHG_TRY(pool_alloc((void**)&queue, sizeof(uint32_t) * (2 * (size_t)chunk + 64 + 2 * ((size_t)cap2 + cap3)),
+                         g->device, s));
     unsigned int* qcount = (unsigned int*)(queue + chunk + 32);
     Tiers T;
     T.cnt = qcount + 1;
-    T.q2 = queue + chunk + 64;
-    T.q3 = T.q2 + cap2;
+    T.l1 = queue + chunk + 64;
+    T.q2 = T.l1 + chunk;
+    T.l2 = T.q2 + cap2;
+    T.q3 = T.l2 + cap2;
+    T.l3 = T.q3 + cap3;
     T.cap2 = cap2;
     T.cap3 = cap3;
     const gahhg_status st = lattice_query_with(Q, d_lonlat, (long long)n, d_labels, precision, s, d_counters,
@@ -2333,10 +2366,13 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
         GAHHG_CUDA_TRY(cudaMemsetAsync(qcount, 0, sizeof(unsigned int) * (tiers ? 4 : 1), s));
         const long long tiles = ((long long)m + TPB * LOC_UNROLL - 1) / (TPB * LOC_UNROLL);
         const int grid = (int)std::min<long long>(tiles, (long long)sms * 8);
+        uint32_t* leafq = tiers ? tiers->l1 : nullptr;
         if (ctr)
-            k_locate<true><<<grid, TPB, summary_bytes(Q.swords), s>>>(ll, m, d_labels + off, Q, queue, qcount, ctr);
+            k_locate<true><<<grid, TPB, summary_bytes(Q.swords), s>>>(ll, m, d_labels + off, Q, queue, leafq, qcount,
+                                                                      ctr);
         else
-            k_locate<false><<<grid, TPB, summary_bytes(Q.swords), s>>>(ll, m, d_labels + off, Q, queue, qcount, ctr);
+            k_locate<false><<<grid, TPB, summary_bytes(Q.swords), s>>>(ll, m, d_labels + off, Q, queue, leafq,
+                                                                       qcount, ctr);
         if (tiers)
             leaf_tiers_launch(OneView{Q}, ll, d_labels + off, queue, qcount, *tiers, precision, ctr, sms, s);
         else if (precision == GAHHG_QUERY_FP64_FILTER)
@@ -2466,12 +2502,12 @@ size_t batch_queue_words(long long queue_cap)
 {
     unsigned int cap2 = 0, cap3 = 0;
     tier_caps(queue_cap, &cap2, &cap3);
-    return (size_t)queue_cap + cap2 + cap3;
+    return 2 * ((size_t)queue_cap + cap2 + cap3);
 }
 
 // counters: [0] queue count, [1] next chunk, [2..4] tier counters.  The
-// queue holds batch_queue_words(queue_cap) words: the pass-2 queue, then the
-// escalation queues.  Everything is enqueued on `s` (no allocation, no host
+// queue holds batch_queue_words(queue_cap) words: the pass-2 queue and its
+// leaf words, then the escalation queues, each followed by its leaf words.  Everything is enqueued on `s` (no allocation, no host
 // synchronisation), so it can be captured in a graph.
 gahhg_status batch_query_launch(const void* d_views, const void* d_chunks, int nchunks, const double* d_lonlat,
                                 uint8_t* d_labels, int precision, uint32_t* queue, long long queue_cap,
@@ -2491,17 +2527,20 @@ gahhg_status batch_query_launch(const void* d_views, const void* d_chunks, int n
     unsigned long long* ctr = (unsigned long long*)d_stats;
     if (zero_counters) GAHHG_CUDA_TRY(cudaMemsetAsync(counters, 0, 5 * sizeof(unsigned int), s));
     const int grid = std::min(nchunks, sms * 8);
-    if (ctr)
-        k_batch_locate<true><<<grid, TPB, 0, s>>>(views, chunks, nchunks, counters + 1, (const double2*)d_lonlat,
-                                                  d_labels, queue, counters, ctr);
-    else
-        k_batch_locate<false><<<grid, TPB, 0, s>>>(views, chunks, nchunks, counters + 1, (const double2*)d_lonlat,
-                                                   d_labels, queue, counters, ctr);
     Tiers T;
     tier_caps(queue_cap, &T.cap2, &T.cap3);
-    T.q2 = queue + queue_cap;
-    T.q3 = T.q2 + T.cap2;
+    T.l1 = queue + queue_cap;
+    T.q2 = T.l1 + queue_cap;
+    T.l2 = T.q2 + T.cap2;
+    T.q3 = T.l2 + T.cap2;
+    T.l3 = T.q3 + T.cap3;
     T.cnt = counters + 2;
+    if (ctr)
+        k_batch_locate<true><<<grid, TPB, 0, s>>>(views, chunks, nchunks, counters + 1, (const double2*)d_lonlat,
+                                                  d_labels, queue, T.l1, counters, ctr);
+    else
+        k_batch_locate<false><<<grid, TPB, 0, s>>>(views, chunks, nchunks, counters + 1, (const double2*)d_lonlat,
+                                                   d_labels, queue, T.l1, counters, ctr);
     leaf_tiers_launch(ChunkViews{views, chunks, nchunks}, (const double2*)d_lonlat, d_labels, queue, counters, T,
                       precision, ctr, sms, s);
     GAHHG_CUDA_TRY(cudaGetLastError());
