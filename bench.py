@@ -128,15 +128,15 @@ class quiet_stdout:
 
 
 def c1_polygon_cached():
-    from gahhg_b200 import synth
-    path = os.path.join(REPO, "_work", "bench_c1_rings.npz") if os.path.isdir(os.path.join(REPO, "_work")) else None
-    if path and os.path.exists(path):
-        z = np.load(path)
-        return [z["r%d" % i] for i in range(len(z.files))]
-    rings = synth.c1_polygon()
-    if path:
-        np.savez(path, **{"r%d" % i: r for i, r in enumerate(rings)})
-    return rings
+    """The C1 polygon (generated in under a second; kept for the process)."""
+    global _C1_RINGS
+    if _C1_RINGS is None:
+        from gahhg_b200 import synth
+        _C1_RINGS = synth.c1_polygon()
+    return _C1_RINGS
+
+
+_C1_RINGS = None
 
 
 def device_points(n, seed, device):
