@@ -79,11 +79,6 @@ constexpr double CAP_FACTOR = 1.25;
 constexpr long long NODE_BUDGET = 1LL << 27;
 constexpr long long PAIR_BUDGET = 1LL << 30;
 
-// Bound on |q32 - q| per component for q32 from __sincosf (documented error
-// 2^-21.41 on [-pi, pi]) of FP32-rounded canonical radians; see DESIGN.
-constexpr float E_Q32 = 2.0e-6f;
-constexpr float C32 = E_Q32 + 5.0f * 5.9604645e-8f;
-
 // Leaf: its center as the lon/lat it was placed at (R = their canonical XYZ,
 // recomputed where needed), its edge records and its center's label.
 struct __align__(8) LeafRec {
@@ -95,16 +90,10 @@ struct __align__(8) LeafRec {
 };
 static_assert(sizeof(LeafRec) == 24, "LeafRec");
 
-// (leaf, edge): the cross products and R . (A x B), each rounded to float
-// from a value within a few FP64 ulp of the exact one.
-struct EdgeRec {
-    float n1[3];  // A x B
-    float n2[3];  // A x R
-    float n3[3];  // B x R
-    float h1;     // R . (A x B) = det[A; B; R]
-    uint32_t es;  // edge index | (orient(A,B,R) > 0) << 31
-};
-static_assert(sizeof(EdgeRec) == 44, "EdgeRec");
+// (leaf, edge) records of the FP32 tier: float4 (a1, a2, b1, b2), the edge's
+// ends in the leaf's tangent frame (local_frame::edge_record), ordered so that
+// orient(A, B, R) = +1.  The edge id and the sign of orient(A, B, R) in the
+// edge's own order are in a parallel array of words (edge | (sign > 0) << 31).
 
 // Level-0 grid over a lon/lat domain: W x H cells of dlon0 x dlat0 degrees
 // starting at (lon0, lat0).  full_lon: the domain spans all longitudes
@@ -696,7 +685,7 @@ __global__ void k_leaf_flags(int nn, const int* cnt, const int* child_base, int*
 __global__ void k_leaf_records(BuildView v, int lvl, int nn, const int* is_leaf, const int* leaf_off,
                                const int* rec_off, int leaf_base, long long rec_base, const long long* ix,
                                const long long* iy, const int* cnt, const int* off, const int* list,
-                               const uint8_t* label, LeafRec* leaves, EdgeRec* recs, uint32_t* eids, int* bad)
+                               const uint8_t* label, LeafRec* leaves, float4* recs, uint32_t* eids, int* bad)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nn || !is_leaf[p]) return;
@@ -716,22 +705,12 @@ __global__ void k_leaf_records(BuildView v, int lvl, int nn, const int* is_leaf,
         const int e = list[off[p] + k];
         const D3 a = v.pv[v.pe[2 * e]], b = v.pv[v.pe[2 * e + 1]];
         const double A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z};
-        double n1[3], n2[3], n3[3];
-        exact::cross_value(A, B, n1);
-        exact::cross_value(A, c.R, n2);
-        exact::cross_value(B, c.R, n3);
-        EdgeRec r;
-        for (int j = 0; j < 3; j++) {
-            r.n1[j] = (float)n1[j];
-            r.n2[j] = (float)n2[j];
-            r.n3[j] = (float)n3[j];
-        }
-        r.h1 = (float)exact::det3_value(A, B, c.R);
         const int s1 = exact::orient(A, B, c.R);
         if (s1 == 0) atomicAdd(bad, 1);
-        r.es = (uint32_t)e | (s1 > 0 ? 0x80000000u : 0u);
-        recs[ro + k] = r;
-        eids[ro + k] = r.es;
+        float r[4];
+        local_frame::edge_record(A, B, c.lonc, c.latc, s1 < 0, r);
+        recs[ro + k] = make_float4(r[0], r[1], r[2], r[3]);
+        eids[ro + k] = (uint32_t)e | (s1 > 0 ? 0x80000000u : 0u);
     }
 }
 
@@ -807,19 +786,12 @@ struct QueryView {
     const uint32_t* summary;  // 2 bits per coarse cell: 0 out, 1 in, 2 mixed
     const uint32_t* nodes;
     const LeafRec* leaves;
-    const EdgeRec* recs;
-    const uint32_t* eids;     // per record: its edge id and sign bit (EdgeRec::es), 4 B apart
+    const float4* recs;       // per record: the FP32 tier's tangent-frame ends
+    const uint32_t* eids;     // per record: edge id | (orient(A, B, R) > 0) << 31
     const double2* ends;      // per edge: A.xy, A.z B.x, B.yz (48 B, one aligned load each)
     const D3* pv;
     const int* pe;
 };
-
-__device__ __forceinline__ int sign32(const float* n, float qx, float qy, float qz)
-{
-    const float d = fmaf(qz, n[2], fmaf(qy, n[1], qx * n[0]));
-    const float b = (fabsf(n[0]) + fabsf(n[1]) + fabsf(n[2])) * C32 + 4e-15f;
-    return d > b ? 1 : (d < -b ? -1 : 0);
-}
 
 struct PointCtx {
     double lon, lat;      // input longitude and FakeLL latitude (canonical XYZ)
@@ -852,26 +824,30 @@ __device__ uint8_t leaf_label(const QueryView& Q, uint32_t leaf, PointCtx& P, bo
     const LeafRec L = Q.leaves[leaf];
     double LR[3];
     gahhg_canon_vertex_xyz(L.lon, L.lat, LR);
-    float qx = 0.f, qy = 0.f, qz = 0.f;
+    local_frame::Frame f;
     if (fp32) {
-        float sa, ca, so, co;
-        // arguments stay inside [-pi, pi], where __sincosf's error bound is documented
-        __sincosf((float)gahhg_canon_rad(P.lat_r), &sa, &ca);
-        __sincosf((float)gahhg_canon_rad(P.lon_r), &so, &co);
-        qx = ca * so;
-        qy = sa;
-        qz = ca * co;
-    } else {
-        P.need64();
+        local_frame::Offset o;
+        fp32 = fabs(P.lon) <= 540.0 && local_frame::offset(P.lon, P.lat, L.lon, L.lat, o);
+        if (fp32) local_frame::project(o, f);
     }
+    if (!fp32) P.need64();
     unsigned long long* c64 = ctr ? ctr + 0 : nullptr;
     unsigned long long* cx = ctr ? ctr + 1 : nullptr;
     int par = 0;
     for (int k = 0; k < L.cnt; k++) {
-        const EdgeRec r = Q.recs[L.off + k];
-        const int e = (int)(r.es & 0x7fffffffu);
-        const int s1 = (r.es >> 31) ? 1 : -1;
-        int s2 = fp32 ? sign32(r.n1, qx, qy, qz) : 0;
+        const uint32_t es = __ldg(Q.eids + L.off + k);
+        const int e = (int)(es & 0x7fffffffu);
+        const int s1 = (es >> 31) ? 1 : -1;
+        // the record holds (A, B) when s1 = +1, else (B, A): see local_frame.cuh
+        int s2 = 0, ea = 0, eb = 0;
+        if (fp32) {
+            const float4 r = __ldg(Q.recs + L.off + k);
+            s2 = s1 * local_frame::sign_edge(f, r.x, r.y, r.z, r.w);
+            const float x1 = s1 > 0 ? r.x : r.z, x2 = s1 > 0 ? r.y : r.w;
+            const float y1 = s1 > 0 ? r.z : r.x, y2 = s1 > 0 ? r.w : r.y;
+            ea = local_frame::sign_end(f, x1, x2);
+            eb = local_frame::sign_end(f, y1, y2);
+        }
         double A[3], B[3];
         bool haveAB = false;
         auto needAB = [&]() {
@@ -894,8 +870,8 @@ __device__ uint8_t leaf_label(const QueryView& Q, uint32_t leaf, PointCtx& P, bo
             s2 = sign_escalate(A, B, P.q, c64, cx);
         }
         if (s2 == s1) continue;
-        // s3 = orient(R, q, A) = q . (A x R); crossing needs s3 == s2
-        int s3 = fp32 ? sign32(r.n2, qx, qy, qz) : 0;
+        // s3 = orient(R, q, A); crossing needs s3 == s2
+        int s3 = ea;
         if (s3 == 0) {
             P.need64();
             needAB();
@@ -904,7 +880,7 @@ __device__ uint8_t leaf_label(const QueryView& Q, uint32_t leaf, PointCtx& P, bo
             s3 = sign_escalate(LR, P.q, A, c64, cx);
         }
         if (s3 != s2) continue;
-        int s4 = fp32 ? sign32(r.n3, qx, qy, qz) : 0;
+        int s4 = eb;
         if (s4 == 0) {
             P.need64();
             needAB();
@@ -1005,19 +981,22 @@ __device__ uint8_t leaf_label_fp32(const QueryView& Q, uint32_t leaf, const Poin
     const LeafRec L = Q.leaves[leaf];
     local_frame::Offset o;
     if (!(fabs(P.lon) <= 540.0) || !local_frame::offset(P.lon, P.lat, L.lon, L.lat, o)) return LABEL_DEFER;
+    local_frame::Frame f;
+    local_frame::project(o, f);
     int par = 0;
     for (int k = 0; k < L.cnt; k++) {
-        const EdgeRec r = Q.recs[L.off + k];
-        const int s1 = (r.es >> 31) ? 1 : -1;
-        const int s2 = local_frame::sign_at(o, r.n1, r.h1);
+        // stored order: orient(A, B, R) = +1, so a crossing needs s2 = -1,
+        // s3 = orient(R, q, A) = -1 and s4 = orient(R, q, B) = +1
+        const float4 r = __ldg(Q.recs + L.off + k);
+        const int s2 = local_frame::sign_edge(f, r.x, r.y, r.z, r.w);
         if (s2 == 0) return LABEL_DEFER;
-        if (s2 == s1) continue;
-        const int s3 = local_frame::sign_at(o, r.n2, 0.0f);
+        if (s2 > 0) continue;
+        const int s3 = local_frame::sign_end(f, r.x, r.y);
         if (s3 == 0) return LABEL_DEFER;
-        if (s3 != s2) continue;
-        const int s4 = local_frame::sign_at(o, r.n3, 0.0f);
+        if (s3 > 0) continue;
+        const int s4 = local_frame::sign_end(f, r.z, r.w);
         if (s4 == 0) return LABEL_DEFER;
-        if (s4 == -s2) par ^= 1;
+        if (s4 > 0) par ^= 1;
     }
     return (uint8_t)(par ? 3 - L.label : L.label);
 }
@@ -1111,15 +1090,22 @@ __device__ __forceinline__ bool domain_locate(const QueryView& Q, double lo, dou
     return true;
 }
 
+// A cell fraction in [0, 1) as a 32-bit binary fraction, saturating (below 0
+// gives 0, 1 and above all ones).  Its base-4 digits are the children that
+// the recursion f -> 4 f - floor(4 f) (clamped to 0..3) visits: that FP64
+// recursion is exact, so digit k of the fraction is its k-th child for the
+// first 16 levels, and for the clamped out-of-range cases both give 0 or 3 at
+// every level.  The lattice has at most MAX_DESCENT levels below the top.
+constexpr int MAX_DESCENT = 16;
+__device__ __forceinline__ uint32_t frac_bits(double f) { return __double2uint_rz(f * 4294967296.0); }
+
 __device__ __forceinline__ uint32_t descend(const QueryView& Q, uint32_t w, double fu, double fv)
 {
+    uint32_t U = frac_bits(fu), V = frac_bits(fv);
     while ((w & KIND_MASK) == KIND_INNER) {
-        fu *= FAN;
-        fv *= FAN;
-        const int cx = min(max((int)fu, 0), FAN - 1), cy = min(max((int)fv, 0), FAN - 1);
-        fu -= cx;
-        fv -= cy;
-        w = __ldg(Q.nodes + (w & INDEX_MASK) + cy * FAN + cx);
+        w = __ldg(Q.nodes + (w & INDEX_MASK) + (V >> 30) * FAN + (U >> 30));
+        U <<= 2;
+        V <<= 2;
     }
     return w;
 }
@@ -1182,7 +1168,7 @@ __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t*
         // independent load per point in flight (points that mostly need the
         // node table, as around small polygons, are bound by its latency)
         uint32_t w[UNROLL];
-        double fu[UNROLL], fv[UNROLL];
+        uint32_t fu[UNROLL], fv[UNROLL];  // cell fractions as binary fractions (frac_bits)
 #pragma unroll
         for (int k = 0; k < UNROLL; k++) {
             const int i = base + k * TPB + threadIdx.x;
@@ -1203,8 +1189,8 @@ __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t*
                             lab[k] = (uint8_t)(code + 1u);  // coarse cell without edges: most points end here
                         } else if (LOCKSTEP) {
                             w[k] = __ldg(Q.nodes + (size_t)L.iy * Q.W + L.ix);
-                            fu[k] = L.fu;
-                            fv[k] = L.fv;
+                            fu[k] = frac_bits(L.fu);
+                            fv[k] = frac_bits(L.fv);
                         } else {
                             const uint32_t d = descend(Q, __ldg(Q.nodes + (size_t)L.iy * Q.W + L.ix), L.fu, L.fv);
                             if ((d & KIND_MASK) == KIND_PURE)
@@ -1228,12 +1214,9 @@ __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t*
 #pragma unroll
                 for (int k = 0; k < UNROLL; k++)
                     if ((w[k] & KIND_MASK) == KIND_INNER) {
-                        fu[k] *= FAN;
-                        fv[k] *= FAN;
-                        const int cx = min(max((int)fu[k], 0), FAN - 1), cy = min(max((int)fv[k], 0), FAN - 1);
-                        fu[k] -= cx;
-                        fv[k] -= cy;
-                        w[k] = __ldg(Q.nodes + (w[k] & INDEX_MASK) + cy * FAN + cx);
+                        w[k] = __ldg(Q.nodes + (w[k] & INDEX_MASK) + (fv[k] >> 30) * FAN + (fu[k] >> 30));
+                        fu[k] <<= 2;
+                        fv[k] <<= 2;
                         inner = true;
                     }
             }
@@ -1379,7 +1362,7 @@ struct BatchChunk {
 };
 
 constexpr int BATCH_SUMMARY_WORDS = 4096;  // 16 KB of shared memory
-constexpr int BATCH_UNROLL = 8;            // points per thread in flight in the batch locate (86 registers)
+constexpr int BATCH_UNROLL = 8;            // points per thread in flight in the batch locate (72 registers)
 
 // Pass 1 over a batch: a persistent grid takes chunks in order from an atomic
 // counter (polygons of very different sizes balance themselves), stages the
@@ -1658,7 +1641,7 @@ struct Lattice {
     int K = 8, maxlev = 10, nlev = 0;
     DevArray<uint32_t> nodes;
     DevArray<LeafRec> leaves;
-    DevArray<EdgeRec> recs;
+    DevArray<float4> recs;
     DevArray<uint32_t> eids;
     DevArray<double2> ends;
     DevArray<uint32_t> summary;
@@ -1686,13 +1669,13 @@ size_t lattice_bytes(const Lattice* L)
 {
     if (!L) return 0;
     return L->nnodes * sizeof(uint32_t) + L->nleaves * sizeof(LeafRec) +
-           L->nrecs * (sizeof(EdgeRec) + sizeof(uint32_t)) + L->nedges * 3 * sizeof(double2);
+           L->nrecs * (sizeof(float4) + sizeof(uint32_t)) + L->nedges * 3 * sizeof(double2);
 }
 
 size_t lattice_device_bytes(const Lattice* L)
 {
     if (!L) return 0;
-    return L->nodes.cap * sizeof(uint32_t) + L->leaves.cap * sizeof(LeafRec) + L->recs.cap * sizeof(EdgeRec) +
+    return L->nodes.cap * sizeof(uint32_t) + L->leaves.cap * sizeof(LeafRec) + L->recs.cap * sizeof(float4) +
            L->eids.cap * sizeof(uint32_t) + L->ends.cap * sizeof(double2) + L->summary.cap * sizeof(uint32_t);
 }
 
@@ -1993,6 +1976,7 @@ gahhg_status lattice_build(Grid* g)
     const int W = L->geo.W, H = L->geo.H;
     L->K = g->opts.lattice_leaf > 0 ? g->opts.lattice_leaf : 8;
     L->maxlev = 9;
+    static_assert(9 <= MAX_DESCENT, "the query's binary-fraction descent covers MAX_DESCENT levels");
     BuildView bv{L->geo, P->d_pv, P->d_pe, n};
 
     // exact label of the first level-0 center: from a point just left of an
@@ -2526,7 +2510,9 @@ gahhg_status batch_query_launch(const void* d_views, const void* d_chunks, int n
     const BatchChunk* chunks = (const BatchChunk*)d_chunks;
     unsigned long long* ctr = (unsigned long long*)d_stats;
     if (zero_counters) GAHHG_CUDA_TRY(cudaMemsetAsync(counters, 0, 5 * sizeof(unsigned int), s));
-    const int grid = std::min(nchunks, sms * 8);
+    // two blocks per SM: with three (which the registers would allow) the
+    // concurrent chunks' node tables crowd L2 and the pass runs slower
+    const int grid = std::min(nchunks, sms * 2);
     Tiers T;
     tier_caps(queue_cap, &T.cap2, &T.cap3);
     T.l1 = queue + queue_cap;

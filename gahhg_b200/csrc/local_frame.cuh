@@ -1,31 +1,28 @@
 // local_frame.cuh - the FP32 crossing tests in a leaf's local frame.
 //
 // The crossing tests of the exact query need the signs of
-//   s2 = det[A; B; q] = q . (A x B),  s3 = det[R; q; A] = q . (A x R),
-//   s4 = det[R; q; B] = q . (B x R)
+//   s2 = det[A; B; q],  s3 = det[R; q; A],  s4 = det[R; q; B]
 // on the canonical FP64 XYZ of the query q, the leaf center R and the edge
 // (A, B).  Evaluating them on an FP32 copy of q bounds the error by FP32's
 // resolution on the unit sphere (~1e-7 rad), so every point closer than that
-// to an edge escalates.  Here the offset d = q - R is computed in FP32 from
-// the differences of the canonical radians (sum-to-product identities with
-// accurate sines of the half differences), so its error is relative to |d|,
-// about the leaf's size, and
-//   s2 = sign(R.(A x B) + d.(A x B)),  s3 = sign(d.(A x R)),  s4 = sign(d.(B x R))
-// since R.(A x R) = R.(B x R) = 0.  R.(A x B) and the three cross products
-// are stored per (leaf, edge) record, each rounded from a value within a few
-// FP64 ulp of the exact one.
+// to an edge would escalate.  Here the offset d = q - R is computed in FP32
+// from the differences of the canonical radians (sum-to-product identities
+// with accurate sines of the half differences), so its error is relative to
+// |d|, about the leaf's size; the three determinants are then evaluated in
+// the tangent frame of R (see edge_record below), where an edge is four
+// floats and the query two coordinates and q . R.
 //
-// Error bound (u = 2^-24).  With h = half the canonical differences, m the
-// midpoints reduced to [-pi, pi]: |fl(m) - m| <= u pi; sinf/cosf are within
-// 2 ulp (CUDA's documented bound; the host functions are tighter), so each
-// of sin/cos(m) and of sin(a), cos(a), cos(b0) is within 7.2e-7 absolutely,
-// sin(h) within 3u relatively; each component of d is then within
-// KAPPA * (|hA| + |hB|) + DELTA of the offset of the canonical points
+// Error bound of the offset (u = 2^-24).  With h = half the canonical
+// differences, m the midpoints reduced to [-pi, pi]: |fl(m) - m| <= u pi;
+// sinf/cosf are within 2 ulp (CUDA's documented bound; the host functions are
+// tighter), so each of sin/cos(m) and of sin(a), cos(a), cos(b0) is within
+// 7.2e-7 absolutely, sin(h) within 3u relatively; each component of d is then
+// within KAPPA * (|hA| + |hB|) + DELTA of the offset of the canonical points
 // (worst case about 2e-6 * (|hA| + |hB|)), where DELTA covers the FP64
 // rounding of the radian differences (up to +-2 pi wraps, about 6e-15) and
-// the canonical conversion's own errors.  A dot product
-// with float vectors each rounded from a value within a few FP64 ulp adds
-// REL * (sum of |terms|).  The constants carry a margin of two or more.
+// the canonical conversion's own errors.  A product of floats each rounded
+// from a value within a few FP64 ulp adds REL * (sum of |terms|).  The
+// constants carry a margin of two or more.
 #pragma once
 
 #include <math.h>
@@ -49,7 +46,8 @@ constexpr double TWO_PI_LO = 2.4492935982947064e-16;     // 2 pi - TWO_PI_HI
 
 struct Offset {
     float d[3];
-    float err;  // bound on |d_i - (q - R)_i| for each component
+    float err;             // bound on |d_i - (q - R)_i| for each component
+    float cl, sl, cp, sp;  // cos/sin of R's longitude and latitude, each within BASIS_ERR
 };
 
 // q from (lon, lat) and R from (lonR, latR), degrees, as the canonical
@@ -82,18 +80,98 @@ LFHD bool offset(double lon, double lat, double lonR, double latR, Offset& o)
     o.d[1] = 2.0f * cmb * shb;                   // sin b - sin b0
     o.d[2] = dc * cos_a + cos_b0 * dca;          // cos b cos a - cos b0 cos a0
     o.err = KAPPA * (fabsf(fha) + fabsf(fhb)) + DELTA;
+    o.sl = sma * cha - cma * sha;  // a0 = ma - ha
+    o.cl = cma * cha + sma * sha;
+    o.sp = smb * chb - cmb * shb;  // b0 = mb - hb
+    o.cp = cos_b0;
     return true;
 }
 
 LFHD int sign_bounded(float v, float bound) { return v > bound ? 1 : (v < -bound ? -1 : 0); }
 
-// sign(h + d . n), 0 when undecided (h = 0 for s3 and s4).
-LFHD int sign_at(const Offset& o, const float* n, float h)
+// ---- the leaf's tangent frame -------------------------------------------
+//
+// With R at canonical radians (a0, b0), e1 = (cos a0, 0, -sin a0) (east) and
+// e2 = (-sin b0 sin a0, cos b0, -sin b0 cos a0) (north) complete R to a
+// right-handed orthonormal basis (det[R; e1; e2] = 1).  In it a point X has
+// coordinates (X.R, X.e1, X.e2); an edge end A with A.R > 0 is stored as its
+// gnomonic coordinates a = (A.e1, A.e2) / (A.R), and the query as
+// w = q.R = 1 + d.R and p = (d.e1, d.e2) (R.e1 = R.e2 = 0).  Then, exactly,
+//   det[A; B; q] = (A.R)(B.R) (w (a1 b2 - a2 b1) + (b1 - a1) p2 - (b2 - a2) p1)
+//   det[R; q; A] = (A.R) (p1 a2 - p2 a1)
+// (rows expanded in the basis), so an edge needs four floats.  Records are
+// stored in the order that makes orient(A, B, R) = +1; swapping A and B
+// negates det[A; B; q] and exchanges the two end tests, and the crossing test
+// (s2 != s1, s3 == s2, s4 == -s2) is symmetric under that exchange.
+//
+// Error terms beyond the offset's: the basis computed in FP32 from the sines
+// and cosines of the offset (BASIS_ERR absolutely per component) perturbs p
+// and w by BASIS_ERR (|d0| + |d1| + |d2|) each, three times over; the stored
+// coordinates are rounded from FP64 values within ~1e-16 relatively (REL per
+// product covers them and the FP32 arithmetic); R's canonical FP64 point
+// differs from the exact one at (a0, b0) by ~1e-16, which adds at most
+// 1e-16 (|p| + |a|) to an end test (END_DELTA, with a large margin) and is
+// inside the offset's DELTA for p and w.
+constexpr float BASIS_ERR = 2.0e-6f;
+constexpr float END_DELTA = 1.0e-14f;
+
+struct Frame {
+    float p1, p2, w;
+    float errp, errw;  // bounds on |p_i - exact| and |w - exact|
+};
+
+LFHD void project(const Offset& o, Frame& f)
 {
-    const float t0 = o.d[0] * n[0], t1 = o.d[1] * n[1], t2 = o.d[2] * n[2];
-    const float v = h + t0 + t1 + t2;
-    const float bound = o.err * (fabsf(n[0]) + fabsf(n[1]) + fabsf(n[2])) +
-                        REL * (fabsf(h) + fabsf(t0) + fabsf(t1) + fabsf(t2)) + 1e-30f;
+    const float t = o.d[0] * o.sl + o.d[2] * o.cl;
+    f.p1 = o.d[0] * o.cl - o.d[2] * o.sl;
+    f.p2 = o.d[1] * o.cp - o.sp * t;
+    f.w = 1.0f + (o.cp * t + o.sp * o.d[1]);
+    const float dn = fabsf(o.d[0]) + fabsf(o.d[1]) + fabsf(o.d[2]);
+    f.errp = 2.0f * o.err + (3.0f * BASIS_ERR + REL) * dn;
+    f.errw = f.errp + 1.0e-7f;
+}
+
+// Gnomonic coordinates of A, B around the center (canonical radians a0, b0
+// from the leaf center's degrees) on FP64 points, rounded to float; r gets
+// (a1, a2, b1, b2), in the order swap ? (B, A) : (A, B).  An end with
+// X.R < 0.5 gives NaN coordinates (every test on the record is undecided).
+LFHD void edge_record(const double* A, const double* B, double lonR, double latR, bool swap, float* r)
+{
+    const double a0 = gahhg_canon_rad(lonR), b0 = gahhg_canon_rad(latR);
+    const double sa = sin(a0), ca = cos(a0), sb = sin(b0), cb = cos(b0);
+    const double e1[3] = {ca, 0.0, -sa}, e2[3] = {-sb * sa, cb, -sb * ca}, R[3] = {cb * sa, sb, cb * ca};
+    const double* X[2] = {swap ? B : A, swap ? A : B};
+    for (int k = 0; k < 2; k++) {
+        const double* x = X[k];
+        const double den = x[0] * R[0] + x[1] * R[1] + x[2] * R[2];
+        if (!(den >= 0.5)) {
+            r[2 * k] = r[2 * k + 1] = NAN;
+            continue;
+        }
+        r[2 * k] = (float)((x[0] * e1[0] + x[2] * e1[2]) / den);
+        r[2 * k + 1] = (float)((x[0] * e2[0] + x[1] * e2[1] + x[2] * e2[2]) / den);
+    }
+}
+
+// sign det[A; B; q] for a record (a1, a2, b1, b2) in its stored order.
+LFHD int sign_edge(const Frame& f, float a1, float a2, float b1, float b2)
+{
+    const float u1 = b1 - a1, u2 = b2 - a2;
+    const float c = a1 * b2 - a2 * b1;
+    const float v = f.w * c + (u1 * f.p2 - u2 * f.p1);
+    const float bound = f.errp * (fabsf(u1) + fabsf(u2)) + f.errw * fabsf(c) +
+                        REL * (fabsf(f.w) * (fabsf(a1 * b2) + fabsf(a2 * b1)) + (fabsf(a1) + fabsf(b1)) * fabsf(f.p2) +
+                               (fabsf(a2) + fabsf(b2)) * fabsf(f.p1)) +
+                        1e-30f;
+    return sign_bounded(v, bound);
+}
+
+// sign det[R; q; X] for an end (x1, x2) of a record.
+LFHD int sign_end(const Frame& f, float x1, float x2)
+{
+    const float v = f.p1 * x2 - f.p2 * x1;
+    const float bound = f.errp * (fabsf(x1) + fabsf(x2)) + REL * (fabsf(f.p1 * x2) + fabsf(f.p2 * x1)) +
+                        END_DELTA * (fabsf(x1) + fabsf(x2) + fabsf(f.p1) + fabsf(f.p2)) + 1e-30f;
     return sign_bounded(v, bound);
 }
 

@@ -12,9 +12,11 @@ extern "C" void filter_signs(const double* xyz, long n, int near, int* out)
 }
 
 // The FP32 local-frame tier (gahhg_b200/csrc/local_frame.cuh) as the query
-// kernel runs it, with the edge record built as the index build builds it.
-// Per case (8 doubles): query lon, lat (raw; the FakeLL round trip is applied
-// here), center lon, lat, then A lon, lat and B lon, lat.  out: s2, s3, s4
+// kernel runs it, with the edge record built as the index build builds it
+// (ends in the order that makes orient(A, B, R) = +1).  Per case (8
+// doubles): query lon, lat (raw; the FakeLL round trip is applied here),
+// center lon, lat, then A lon, lat and B lon, lat.  out: s2 = orient(A, B, q),
+// s3 = orient(R, q, A), s4 = orient(R, q, B) in the given order of A and B
 // (0 = undecided), or 9 9 9 when the offset is not small.
 #include "../../gahhg_b200/csrc/local_frame.cuh"
 
@@ -23,28 +25,26 @@ extern "C" void local_signs(const double* cfg, long n, int* out)
     using namespace gahhg;
     for (long i = 0; i < n; i++) {
         const double* c = cfg + 8 * i;
-        double R[3], A[3], B[3], n1[3], n2[3], n3[3];
+        double R[3], A[3], B[3];
         gahhg_canon_vertex_xyz(c[2], c[3], R);
         gahhg_canon_vertex_xyz(c[4], c[5], A);
         gahhg_canon_vertex_xyz(c[6], c[7], B);
-        exact::cross_value(A, B, n1);
-        exact::cross_value(A, R, n2);
-        exact::cross_value(B, R, n3);
-        float f1[3], f2[3], f3[3];
-        for (int j = 0; j < 3; j++) {
-            f1[j] = (float)n1[j];
-            f2[j] = (float)n2[j];
-            f3[j] = (float)n3[j];
-        }
-        const float h1 = (float)exact::det3_value(A, B, R);
+        const int s1 = exact::orient(A, B, R);
+        const bool swap = s1 < 0;
+        float r[4];
+        local_frame::edge_record(A, B, c[2], c[3], swap, r);
         local_frame::Offset o;
         int* s = out + 3 * i;
-        if (!local_frame::offset(c[0], gahhg_canon_query_lat(c[1]), c[2], c[3], o)) {
+        if (s1 == 0 || !local_frame::offset(c[0], gahhg_canon_query_lat(c[1]), c[2], c[3], o)) {
             s[0] = s[1] = s[2] = 9;
             continue;
         }
-        s[0] = local_frame::sign_at(o, f1, h1);
-        s[1] = local_frame::sign_at(o, f2, 0.0f);
-        s[2] = local_frame::sign_at(o, f3, 0.0f);
+        local_frame::Frame f;
+        local_frame::project(o, f);
+        const int e = local_frame::sign_edge(f, r[0], r[1], r[2], r[3]);
+        const int ea = local_frame::sign_end(f, r[0], r[1]), eb = local_frame::sign_end(f, r[2], r[3]);
+        s[0] = swap ? -e : e;
+        s[1] = swap ? eb : ea;
+        s[2] = swap ? ea : eb;
     }
 }
