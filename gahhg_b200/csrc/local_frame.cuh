@@ -43,6 +43,7 @@ constexpr float DELTA = 3.0e-14f;  // absolute, per component of d
 constexpr float REL = 1.0e-6f;     // relative, per term of a dot product (rounding of terms and sums)
 constexpr double TWO_PI_HI = 6.283185307179586;          // 2 pi rounded to double
 constexpr double TWO_PI_LO = 2.4492935982947064e-16;     // 2 pi - TWO_PI_HI
+constexpr double INV_TWO_PI = 0.15915494309189535;       // 1 / (2 pi) rounded to double
 
 struct Offset {
     float d[3];
@@ -57,13 +58,16 @@ LFHD bool offset(double lon, double lat, double lonR, double latR, Offset& o)
 {
     const double a = gahhg_canon_rad(lon), a0 = gahhg_canon_rad(lonR);
     const double b = gahhg_canon_rad(lat), b0 = gahhg_canon_rad(latR);
+    // the nearest multiple of 2 pi by a reciprocal product: where it can differ
+    // from the quotient's (a half-integer number of turns) |ha| ~ pi / 2, and
+    // the offset is refused below; the midpoint lands in [-pi, pi] up to ulps
     double ta = a - a0;
-    const double k = rint(ta / TWO_PI_HI);
+    const double k = rint(ta * INV_TWO_PI);
     ta = (ta - k * TWO_PI_HI) - k * TWO_PI_LO;
     const double ha = 0.5 * ta, hb = 0.5 * (b - b0);
     if (!(fabs(ha) < 0.5 && fabs(hb) < 0.5)) return false;
     double ma = a0 + ha;
-    ma -= TWO_PI_HI * rint(ma / TWO_PI_HI);
+    ma -= TWO_PI_HI * rint(ma * INV_TWO_PI);
     const double mb = b0 + hb;
     const float fha = (float)ha, fhb = (float)hb, fma_ = (float)ma, fmb = (float)mb;
     const float sma = sinf(fma_), cma = cosf(fma_);
