@@ -7,9 +7,14 @@
 //   the walk loop              source/GPISPAHHG.cu:1208-1287 (mark),
 //                              :734-816 (count), :870-953 (write)
 // Differences, all in cases where the reference would read outside its
-// arrays: a missing partner (-1), a cell index outside the grid, or a walk
-// longer than WALK_STEP_LIMIT ends the walk and is counted in DeviceErrors
-// instead of reading garbage or spinning.
+// arrays or never finish: a missing partner (-1), a cell index outside the
+// grid, a walk that returns to a state it was in before (the next step
+// depends only on the current cell and the border it entered by, so such a
+// walk would repeat forever; Brent's cycle test finds it within a few times
+// the cycle's length) or a walk longer than WALK_STEP_LIMIT ends the walk and
+// is counted in DeviceErrors instead of reading garbage or spinning.  A walk
+// that ends in the reference never repeats a state, so none of these changes
+// a walk the reference completes.
 #pragma once
 
 #include "gahhg_internal.h"
@@ -143,10 +148,17 @@ __device__ __forceinline__ int walk_edge(D3 p0, D3 p1, int cur, const GridView& 
 {
     int in = -1;
     int steps = 0;
+    int seen_cur = cur, seen_in = in, window = 1, since = 0;  // Brent's cycle test
     while (true) {
-        if (steps >= WALK_STEP_LIMIT) {
+        if (steps >= WALK_STEP_LIMIT || (steps > 0 && cur == seen_cur && in == seen_in)) {
             atomicAdd(&err->walk_step_limit, 1);
             return steps;
+        }
+        if (++since == window) {
+            seen_cur = cur;
+            seen_in = in;
+            window <<= 1;
+            since = 0;
         }
         visit(cur, steps);
         steps++;

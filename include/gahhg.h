@@ -85,7 +85,8 @@ typedef struct {
     long long esc_fp64;        /* exact query: points the FP32 tier deferred to FP64 */
     long long esc_exact;       /* exact query: points the FP64 tier deferred to exact arithmetic */
     long long boundary_points; /* exact query: points that ran crossing tests */
-    long long walk_limit_hits; /* edge walks stopped at the step limit (the reference would not terminate) */
+    long long walk_limit_hits; /* edge walks stopped on a repeated state or at the step limit (the reference
+                                  would not terminate) */
 } gahhg_stats;
 
 /* Defaults as in GPISPParam::GPISPParam (source/GPISPParam.h:64-77). */
