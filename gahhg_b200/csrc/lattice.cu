@@ -39,6 +39,8 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <thread>
+#include <vector>
 
 #include "exact_pred.cuh"
 #include "gahhg_canon.h"
@@ -370,11 +372,21 @@ __global__ void k_l0_expand(BuildView v, const EdgeBox* __restrict__ box, const 
     }
 }
 
+// Cap (R, r) of every child node of a level, once: the pair passes below
+// test each child against every edge of its parent, twice.
+__global__ void k_child_caps(Geo g, int lvl, int nn, const long long* ix, const long long* iy, double4* caps)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nn) return;
+    const NodeCap nc = node_cap(g, lvl, ix[c], iy[c]);
+    caps[c] = make_double4(nc.R[0], nc.R[1], nc.R[2], nc.r);
+}
+
 // Children pairs: one thread per (refined parent, edge) pair.
 template <int PASS>
-__global__ void k_child_pairs(BuildView v, int lvl, int npairs, const int* pair_node, const int* plist,
-                              const int* child_base, const long long* pix, const long long* piy, int cstart,
-                              int* cnt, const int* off, int* cursor, int* list)
+__global__ void k_child_pairs(BuildView v, int npairs, const int* pair_node, const int* plist,
+                              const int* child_base, const double4* __restrict__ caps, int cstart, int* cnt,
+                              const int* off, int* cursor, int* list)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= npairs) return;
@@ -385,9 +397,10 @@ __global__ void k_child_pairs(BuildView v, int lvl, int npairs, const int* pair_
     const D3 A = v.pv[v.pe[2 * e]], B = v.pv[v.pe[2 * e + 1]];
     for (int cy = 0; cy < FAN; cy++)
         for (int cx = 0; cx < FAN; cx++) {
-            const NodeCap c = node_cap(v.g, lvl + 1, pix[p] * FAN + cx, piy[p] * FAN + cy);
-            if (!edge_hits_cap(A, B, c.R, c.r)) continue;
             const int node = cb + cy * FAN + cx - cstart;
+            const double4 c = caps[node];
+            const double R[3] = {c.x, c.y, c.z};
+            if (!edge_hits_cap(A, B, R, c.w)) continue;
             if (PASS == 0) {
                 atomicAdd(&cnt[node], 1);
             } else {
@@ -701,6 +714,8 @@ __global__ void k_leaf_records(BuildView v, int lvl, int nn, const int* is_leaf,
     L.pad = 0;
     leaves[leaf_base + leaf_off[p]] = L;
     if (cnt[p] > 65535) atomicAdd(bad + 2, 1);
+    local_frame::Basis fb;
+    local_frame::basis_at(c.lonc, c.latc, fb);
     for (int k = 0; k < cnt[p]; k++) {
         const int e = list[off[p] + k];
         const D3 a = v.pv[v.pe[2 * e]], b = v.pv[v.pe[2 * e + 1]];
@@ -708,7 +723,7 @@ __global__ void k_leaf_records(BuildView v, int lvl, int nn, const int* is_leaf,
         const int s1 = exact::orient(A, B, c.R);
         if (s1 == 0) atomicAdd(bad, 1);
         float r[4];
-        local_frame::edge_record(A, B, c.lonc, c.latc, s1 < 0, r);
+        local_frame::edge_record(A, B, fb, s1 < 0, r);
         recs[ro + k] = make_float4(r[0], r[1], r[2], r[3]);
         eids[ro + k] = (uint32_t)e | (s1 > 0 ? 0x80000000u : 0u);
     }
@@ -1801,12 +1816,16 @@ int nearest_hub(const double* q)
 // cells of near-equal size in degrees whose count is about `target`.  A
 // domain that reaches within a degree of a pole takes in the whole polar cap
 // (all longitudes), so that points outside it are never close to an edge.
-gahhg_status compute_domain(const Polygon* P, long long target, Geo* G)
-{
+// Latitude range and touched 0.1-degree longitude bins of edges [e0, e1).
+struct DomainScan {
     double latmin = 90.0, latmax = -90.0;
     bool full = false;
-    std::vector<uint8_t> bins(3600, 0);  // 0.1-degree longitude bins touched by some arc
-    for (int e = 0; e < P->pv_num; e++) {
+    std::vector<uint8_t> bins = std::vector<uint8_t>(3600, 0);
+};
+
+static void scan_domain(const Polygon* P, int e0, int e1, DomainScan& D)
+{
+    for (int e = e0; e < e1; e++) {
         const int ia = P->pe[2 * e], ib = P->pe[2 * e + 1];
         const D3 a = P->pv[ia], b = P->pv[ib];
         if (a.x == b.x && a.y == b.y && a.z == b.z) continue;
@@ -1834,14 +1853,44 @@ gahhg_status compute_domain(const Polygon* P, long long target, Geo* G)
             }
             if (fabs(ta) > 89.9 || fabs(tb) > 89.9) fl = true;
         }
-        latmin = std::min(latmin, la0);
-        latmax = std::max(latmax, la1);
+        D.latmin = std::min(D.latmin, la0);
+        D.latmax = std::max(D.latmax, la1);
         if (fl) {
-            full = true;
+            D.full = true;
             continue;
         }
         const long long b0 = (long long)floor((lo0 + 180.0) * 10.0) - 1, b1 = (long long)floor((lo1 + 180.0) * 10.0) + 1;
-        for (long long k = b0; k <= b1; k++) bins[((k % 3600) + 3600) % 3600] = 1;
+        for (long long k = b0; k <= b1; k++) D.bins[((k % 3600) + 3600) % 3600] = 1;
+    }
+}
+
+gahhg_status compute_domain(const Polygon* P, long long target, Geo* G)
+{
+    // large polygons are scanned by several host threads (each over a range
+    // of edges, merged after); the result does not depend on the split
+    constexpr int EDGES_PER_THREAD = 1 << 17;
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int nt = std::max(1, std::min(std::min(hw, 16), P->pv_num / EDGES_PER_THREAD));
+    std::vector<DomainScan> part(nt);
+    if (nt == 1) {
+        scan_domain(P, 0, P->pv_num, part[0]);
+    } else {
+        std::vector<std::thread> th;
+        for (int t = 0; t < nt; t++) {
+            const int e0 = (int)((long long)P->pv_num * t / nt), e1 = (int)((long long)P->pv_num * (t + 1) / nt);
+            th.emplace_back(scan_domain, P, e0, e1, std::ref(part[t]));
+        }
+        for (auto& t : th) t.join();
+    }
+    double latmin = 90.0, latmax = -90.0;
+    bool full = false;
+    std::vector<uint8_t>& bins = part[0].bins;  // 0.1-degree longitude bins touched by some arc
+    for (int t = 0; t < nt; t++) {
+        latmin = std::min(latmin, part[t].latmin);
+        latmax = std::max(latmax, part[t].latmax);
+        full = full || part[t].full;
+        if (t > 0)
+            for (int k = 0; k < 3600; k++) bins[k] |= part[t].bins[k];
     }
     if (latmin > latmax) {
         set_error("exact index: polygon has no edges of positive length");
@@ -2151,9 +2200,12 @@ gahhg_status lattice_build(Grid* g)
         GAHHG_TRY(cl.cursor.reserve(cl.nn, s, false));
         GAHHG_CUDA_TRY(cudaMemsetAsync(cl.cnt.ptr, 0, sizeof(int) * cl.nn, s));
         GAHHG_CUDA_TRY(cudaMemsetAsync(cl.cursor.ptr, 0, sizeof(int) * cl.nn, s));
-        k_child_pairs<0><<<blocks_for(pp.npairs), TPB, 0, s>>>(bv, lvl, pp.npairs, pp.pair_node.ptr, pp.list.ptr,
-                                                               pp.child_base.ptr, pp.ix.ptr, pp.iy.ptr, cl.gstart,
-                                                               cl.cnt.ptr, nullptr, nullptr, nullptr);
+        DevArray<double4> caps;
+        GAHHG_TRY(caps.reserve(cl.nn, s, false));
+        k_child_caps<<<blocks_for(cl.nn), TPB, 0, s>>>(L->geo, lvl + 1, cl.nn, cl.ix.ptr, cl.iy.ptr, caps.ptr);
+        k_child_pairs<0><<<blocks_for(pp.npairs), TPB, 0, s>>>(bv, pp.npairs, pp.pair_node.ptr, pp.list.ptr,
+                                                               pp.child_base.ptr, caps.ptr, cl.gstart, cl.cnt.ptr,
+                                                               nullptr, nullptr, nullptr);
         GAHHG_TRY(scan_state_reserve(&g->scan_state, cl.nn));
         GAHHG_TRY(scan_exclusive(cl.cnt.ptr, cl.off.ptr, cl.nn, g->d_counts + 10, g->scan_state, g->d_err, s));
         int ctotal = 0;
@@ -2161,9 +2213,10 @@ gahhg_status lattice_build(Grid* g)
         GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
         cl.npairs = ctotal;
         GAHHG_TRY(cl.list.reserve(std::max(ctotal, 1), s, false));
-        k_child_pairs<1><<<blocks_for(pp.npairs), TPB, 0, s>>>(bv, lvl, pp.npairs, pp.pair_node.ptr, pp.list.ptr,
-                                                               pp.child_base.ptr, pp.ix.ptr, pp.iy.ptr, cl.gstart,
-                                                               cl.cnt.ptr, cl.off.ptr, cl.cursor.ptr, cl.list.ptr);
+        k_child_pairs<1><<<blocks_for(pp.npairs), TPB, 0, s>>>(bv, pp.npairs, pp.pair_node.ptr, pp.list.ptr,
+                                                               pp.child_base.ptr, caps.ptr, cl.gstart, cl.cnt.ptr,
+                                                               cl.off.ptr, cl.cursor.ptr, cl.list.ptr);
+        caps.release();
         GAHHG_TRY(sort_lists(g, cl.cnt.ptr, cl.off.ptr, cl.nn, cl.list.ptr, sms, s));
         // child labels
         DevArray<int> child_parent;

@@ -135,25 +135,42 @@ LFHD void project(const Offset& o, Frame& f)
     f.errw = f.errp + 1.0e-7f;
 }
 
-// Gnomonic coordinates of A, B around the center (canonical radians a0, b0
-// from the leaf center's degrees) on FP64 points, rounded to float; r gets
-// (a1, a2, b1, b2), in the order swap ? (B, A) : (A, B).  An end with
-// X.R < 0.5 gives NaN coordinates (every test on the record is undecided).
-LFHD void edge_record(const double* A, const double* B, double lonR, double latR, bool swap, float* r)
+// The tangent frame at the center (canonical radians of its degrees), FP64.
+struct Basis {
+    double e1[3], e2[3], R[3];
+};
+
+LFHD void basis_at(double lonR, double latR, Basis& f)
 {
     const double a0 = gahhg_canon_rad(lonR), b0 = gahhg_canon_rad(latR);
     const double sa = sin(a0), ca = cos(a0), sb = sin(b0), cb = cos(b0);
-    const double e1[3] = {ca, 0.0, -sa}, e2[3] = {-sb * sa, cb, -sb * ca}, R[3] = {cb * sa, sb, cb * ca};
+    f.e1[0] = ca;
+    f.e1[1] = 0.0;
+    f.e1[2] = -sa;
+    f.e2[0] = -sb * sa;
+    f.e2[1] = cb;
+    f.e2[2] = -sb * ca;
+    f.R[0] = cb * sa;
+    f.R[1] = sb;
+    f.R[2] = cb * ca;
+}
+
+// Gnomonic coordinates of A, B in the frame f on FP64 points, rounded to
+// float; r gets (a1, a2, b1, b2), in the order swap ? (B, A) : (A, B).  An end
+// with X.R < 0.5 gives NaN coordinates (every test on the record is
+// undecided).
+LFHD void edge_record(const double* A, const double* B, const Basis& f, bool swap, float* r)
+{
     const double* X[2] = {swap ? B : A, swap ? A : B};
     for (int k = 0; k < 2; k++) {
         const double* x = X[k];
-        const double den = x[0] * R[0] + x[1] * R[1] + x[2] * R[2];
+        const double den = x[0] * f.R[0] + x[1] * f.R[1] + x[2] * f.R[2];
         if (!(den >= 0.5)) {
             r[2 * k] = r[2 * k + 1] = NAN;
             continue;
         }
-        r[2 * k] = (float)((x[0] * e1[0] + x[2] * e1[2]) / den);
-        r[2 * k + 1] = (float)((x[0] * e2[0] + x[1] * e2[1] + x[2] * e2[2]) / den);
+        r[2 * k] = (float)((x[0] * f.e1[0] + x[2] * f.e1[2]) / den);
+        r[2 * k + 1] = (float)((x[0] * f.e2[0] + x[1] * f.e2[1] + x[2] * f.e2[2]) / den);
     }
 }
 

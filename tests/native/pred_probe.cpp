@@ -32,7 +32,9 @@ extern "C" void local_signs(const double* cfg, long n, int* out)
         const int s1 = exact::orient(A, B, R);
         const bool swap = s1 < 0;
         float r[4];
-        local_frame::edge_record(A, B, c[2], c[3], swap, r);
+        local_frame::Basis fb;
+        local_frame::basis_at(c[2], c[3], fb);
+        local_frame::edge_record(A, B, fb, swap, r);
         local_frame::Offset o;
         int* s = out + 3 * i;
         if (s1 == 0 || !local_frame::offset(c[0], gahhg_canon_query_lat(c[1]), c[2], c[3], o)) {
