@@ -604,6 +604,14 @@ def main():
     G.Grid(G.Polygon.from_rings(synth.c0_polygon()), semantics=G.SEMANTICS_EXACT, device=local).classify()
     G.Grid(G.Polygon.from_rings(synth.c0_polygon()), semantics=G.SEMANTICS_REFERENCE, device=local).classify()
     cold_s = time.time() - t0
+    # the first C1 build of the process also grows the device memory pool
+    # (first use of the memory it maps): timed apart as the cold build; the
+    # second, timed build is the warm one the queries use
+    t0 = time.time()
+    g = G.Grid(P, semantics=G.SEMANTICS_EXACT, device=local).classify()
+    cold_build_wall = time.time() - t0
+    st_cold = g.stats()
+    del g
     t0 = time.time()
     g = G.Grid(P, semantics=G.SEMANTICS_EXACT, device=local).classify()
     build_wall = time.time() - t0
@@ -736,6 +744,8 @@ def main():
             "reference_fp64_max_depth": REF_DEPTH_C1,
         },
         "build_ms": {"exact_total_wall": round(build_wall * 1e3, 1),
+                     "exact_total_wall_first_in_process": round(cold_build_wall * 1e3, 1),
+                     "lattice_first_in_process": round(st_cold["lattice_s"] * 1e3, 2),
                      "hierarchy_create": round(st_build["create_s"] * 1e3, 2),
                      "hierarchy_classify": round(st_build["classify_s"] * 1e3, 2),
                      "lattice": round(st_build["lattice_s"] * 1e3, 2),
