@@ -91,14 +91,15 @@ def _xyz(ll):
     return np.stack([np.cos(la) * np.sin(lo), np.sin(la), np.cos(la) * np.cos(lo)], 1)
 
 
-def _local_cases(n, seed):
-    """Cells of 1e-7..1e-1 rad anywhere (poles, antimeridian); the point on
-    the edge's great circle or on the arc from the center to an edge end,
-    pushed off it by 10^U[-19,-2] times the cell size; longitudes wrapped by
-    +-360 degrees on either side."""
+def _local_cases(n, seed, polar=0.1):
+    """Cells of 1e-7..1e-1 rad anywhere (a fraction `polar` of them within 5
+    degrees of a pole; antimeridian wraps); the point on the edge's great
+    circle or on the arc from the center to an edge end, pushed off it by
+    10^U[-19,-2] times the cell size; longitudes wrapped by +-360 degrees on
+    either side."""
     rng = np.random.default_rng(seed)
     Rll = np.stack([rng.uniform(-180, 180, n), np.degrees(np.arcsin(rng.uniform(-1, 1, n)))], 1)
-    pole = rng.random(n) < 0.1
+    pole = rng.random(n) < polar
     Rll[pole, 1] = np.sign(rng.uniform(-1, 1, pole.sum())) * rng.uniform(85, 90, pole.sum())
     R = _xyz(Rll)
     r = 10.0 ** rng.uniform(-7, -1, n)[:, None]
@@ -119,11 +120,14 @@ def _local_cases(n, seed):
     return np.concatenate([qll, Rll, All, Bll], 1)
 
 
-def test_fp32_local_frame_is_sound(probe):
-    cfg = _local_cases(30000, 11)
+@pytest.mark.parametrize("seed,polar", [(11, 0.1), (23, 0.6)])
+def test_fp32_local_frame_is_sound(probe, seed, polar):
+    cfg = _local_cases(30000, seed, polar)
     got = probe.local(cfg)
     ok = got[:, 0] != 9
-    assert ok.mean() > 0.99
+    # near a pole cells span wide longitude differences, and more offsets are
+    # refused (those points defer to the FP64 tier)
+    assert ok.mean() > (0.99 if polar < 0.5 else 0.95)
     want = np.zeros_like(got)
     for i in np.nonzero(ok)[0]:
         c = cfg[i]
