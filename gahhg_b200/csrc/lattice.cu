@@ -163,8 +163,6 @@ __host__ __device__ inline void nudge_center(const Geo& g, int lvl, NodeCap& c, 
     }
 }
 
-__host__ __device__ inline bool same3(const double* a, const D3& b) { return a[0] == b.x && a[1] == b.y && a[2] == b.z; }
-
 // Conservative: may arc AB (unit vectors) come within angle r of R?
 __host__ __device__ inline bool edge_hits_cap(const D3& A, const D3& B, const double* R, double r)
 {
