@@ -22,8 +22,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <fstream>
-#include <sstream>
+#include <climits>
+#include <cmath>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -34,37 +35,22 @@ namespace gahhg {
 
 namespace {
 
+// The whole file in one read into a string sized from fstat.
 bool read_file(const char* path, std::string* out)
 {
-    std::ifstream f(path, std::ios::binary);
+    FILE* f = fopen(path, "rb");
     if (!f) return false;
-    std::ostringstream ss;
-    ss << f.rdbuf();
-    *out = ss.str();
+    struct stat st;
+    if (fstat(fileno(f), &st) != 0 || !S_ISREG(st.st_mode)) {
+        fclose(f);
+        return false;
+    }
+    out->resize((size_t)st.st_size);
+    const size_t got = st.st_size ? fread(&(*out)[0], 1, (size_t)st.st_size, f) : 0;
+    fclose(f);
+    out->resize(got);
     return true;
 }
-
-// Splits into lines the way repeated istream::getline does: '\n' ends a line
-// and is dropped; a final line without '\n' still counts; nothing after the
-// last '\n' means no further line.
-struct LineReader {
-    const std::string& s;
-    size_t pos = 0;
-    explicit LineReader(const std::string& str) : s(str) {}
-    // returns false at end of data (getline would fail); *line = "" then
-    bool next(std::string* line)
-    {
-        if (pos >= s.size()) {
-            line->clear();
-            return false;
-        }
-        size_t e = s.find('\n', pos);
-        if (e == std::string::npos) e = s.size();
-        line->assign(s, pos, e - pos);
-        pos = (e < s.size()) ? e + 1 : e;
-        return true;
-    }
-};
 
 D3 vertex_xyz(double lon, double lat)
 {
@@ -96,13 +82,75 @@ bool ring_clockwise(const double* lonlat, int n)
     return !(temp > 0);
 }
 
+// `sscanf(buf, "%lf %lf", &lo, &la) == 2` with the same acceptance.
+bool parse_two(const std::string& line, double* lo, double* la)
+{
+    return sscanf(line.c_str(), "%lf %lf", lo, la) == 2;
+}
+
+inline bool poly_space(char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\v' || c == '\f'; }
+
+// A plain decimal number at p (sign '-' or none): the cases where
+// std::from_chars and the reference's "%lf" read the same characters to the
+// same (correctly rounded) value.  False leaves the line to sscanf.
+inline bool plain_number(const char* p, const char* e, double* v, const char** end)
+{
+    if (p >= e || !((*p >= '0' && *p <= '9') || *p == '-' || *p == '.')) return false;
+    const auto r = std::from_chars(p, e, *v);
+    if (r.ec != std::errc() || !std::isfinite(*v)) return false;
+    // an exponent or hex marker that from_chars stopped before may be read
+    // differently by scanf (which cannot back out of "1e")
+    if (r.ptr < e && (*r.ptr == 'e' || *r.ptr == 'E' || *r.ptr == 'x' || *r.ptr == 'X')) return false;
+    *end = r.ptr;
+    return true;
+}
+
+// "%lf %lf" on line [s, e): the usual "lon lat" by from_chars, anything else
+// (a '+' sign, hex, inf/nan, no white space between the numbers, a second
+// number missing) by sscanf itself on a NUL-terminated copy.
+bool parse_two_line(const char* s, const char* e, double* lo, double* la)
+{
+    const char* p = s;
+    while (p < e && poly_space(*p)) p++;
+    const char* q;
+    if (plain_number(p, e, lo, &q) && q < e && poly_space(*q)) {
+        p = q;
+        while (p < e && poly_space(*p)) p++;
+        if (plain_number(p, e, la, &q)) return true;
+    }
+    return parse_two(std::string(s, e), lo, la);
+}
+
+// Vertex XYZ of points [a, b) of P (canonical conversion).
+void vertex_range(Polygon* P, int a, int b)
+{
+    for (int i = a; i < b; i++) P->pv[i] = vertex_xyz(P->lonlat[2 * i], P->lonlat[2 * i + 1]);
+}
+
+// Splits [0, n) into up to `hw` ranges of at least `grain` items and runs
+// f(a, b) on each, the first on the calling thread.
+template <class F>
+void parallel_ranges(long long n, long long grain, F f)
+{
+    const int hw = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const int nt = (int)std::max(1LL, std::min<long long>(hw, n / std::max(grain, 1LL)));
+    if (nt == 1) {
+        f(0LL, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; t++) th.emplace_back(f, n * t / nt, n * (t + 1) / nt);
+    f(0LL, n / nt);
+    for (auto& x : th) x.join();
+}
+
 // Builds pv and pe from ring vertex lists (closing vertices already removed).
 void assemble(Polygon* P)
 {
     const int nr = P->num_rings;
     P->pv_num = P->ring_start[nr];
     P->pv.resize(P->pv_num);
-    for (int i = 0; i < P->pv_num; i++) P->pv[i] = vertex_xyz(P->lonlat[2 * i], P->lonlat[2 * i + 1]);
+    parallel_ranges(P->pv_num, 1 << 16, [P](long long a, long long b) { vertex_range(P, (int)a, (int)b); });
     P->pe.assign(2 * (size_t)P->pv_num, 0);
     int index = 0;
     for (int r = 0; r < nr; r++) {
@@ -129,12 +177,6 @@ void assemble(Polygon* P)
     }
 }
 
-// `sscanf(buf, "%lf %lf", &lo, &la) == 2` with the same acceptance.
-bool parse_two(const std::string& line, double* lo, double* la)
-{
-    return sscanf(line.c_str(), "%lf %lf", lo, la) == 2;
-}
-
 }  // namespace
 
 gahhg_status load_polygon_file(const char* path, Polygon* P)
@@ -146,64 +188,121 @@ gahhg_status load_polygon_file(const char* path, Polygon* P)
         set_error("cannot open %s", path);
         return GAHHG_ERR_IO;
     }
-    LineReader rd(data);
-    std::string line;
-    int lineindex = 0;
-    auto fail_format = [&](const char* what) {
-        printf("Error. Line %d of %s. %s\n", lineindex, path, what);
-        set_error("line %d of %s: %s", lineindex, path, what);
-        return GAHHG_ERR_FORMAT;
-    };
     const char* WRONG = "Wrong format.";
     const char* FEW = "Number of edges should be greater than 3. ";
+    // Lines as repeated getline sees them: '\n' ends a line; a final line
+    // without '\n' counts; reading past the last line gives "".
+    std::vector<size_t> start;
+    start.reserve(data.size() / 16 + 2);
+    for (size_t pos = 0; pos < data.size();) {
+        start.push_back(pos);
+        const void* nl = memchr(data.data() + pos, '\n', data.size() - pos);
+        pos = nl ? (size_t)((const char*)nl - data.data()) + 1 : data.size();
+    }
+    const long long nlines = (long long)start.size();
+    auto line_begin = [&](long long k) { return data.data() + start[k]; };
+    auto line_end = [&](long long k) {
+        const size_t e = (k + 1 < nlines) ? start[k + 1] - 1 : data.size();
+        return data.data() + ((e > start[k] && data[e - 1] == '\n') ? e - 1 : e);
+    };
+    auto line_str = [&](long long k) {
+        return k < nlines ? std::string(line_begin(k), line_end(k)) : std::string();
+    };
+    // The first failing line (1-based, as the reference counts) and its message.
+    long long fail_line = LLONG_MAX;
+    const char* fail_what = nullptr;
+    auto note = [&](long long line, const char* what) {
+        if (line < fail_line) {
+            fail_line = line;
+            fail_what = what;
+        }
+    };
 
+    // The structure (ring headers and the vertex blocks they announce) is
+    // read serially; vertex lines are parsed afterwards, in parallel.
+    struct Block {
+        long long first;  // 0-based line of the ring's first vertex
+        int nv;           // vertex lines announced (the last closes the ring)
+    };
+    std::vector<Block> blocks;
     int inNum = 0, outVNum = 0, temp = 0;
-    rd.next(&line);
-    lineindex++;
-    if (sscanf(line.c_str(), "POLYGON 1 %d", &inNum) != 1) return fail_format(WRONG);
-    rd.next(&line);
-    lineindex++;
-    if (sscanf(line.c_str(), "0 %d", &outVNum) != 1) return fail_format(WRONG);
-    if (outVNum < 4) return fail_format(FEW);
-
-    std::vector<std::vector<double>> rings;
-    rings.emplace_back();
-    for (int i = 0; i < outVNum; i++) {
-        rd.next(&line);
-        lineindex++;
-        double lo, la;
-        if (!parse_two(line, &lo, &la)) return fail_format(WRONG);
-        if (i < outVNum - 1) {
-            rings[0].push_back(lo);
-            rings[0].push_back(la);
+    long long k = 0;
+    if (sscanf(line_str(k).c_str(), "POLYGON 1 %d", &inNum) != 1) {
+        note(k + 1, WRONG);
+    } else if (sscanf(line_str(k + 1).c_str(), "0 %d", &outVNum) != 1) {
+        note(k + 2, WRONG);
+    } else if (outVNum < 4) {
+        note(k + 2, FEW);
+    } else {
+        k = 2;
+        blocks.push_back({k, outVNum});
+        k += outVNum;
+        for (int h = 0; h < inNum && k <= nlines; h++) {
+            int nv = 0;
+            if (sscanf(line_str(k).c_str(), "%d %d", &temp, &nv) != 2) {
+                note(k + 1, WRONG);
+                break;
+            }
+            if (nv < 4) {
+                note(k + 1, FEW);
+                break;
+            }
+            blocks.push_back({k + 1, nv});
+            k += 1 + (long long)nv;
         }
     }
-    for (int h = 0; h < inNum; h++) {
-        rd.next(&line);
-        lineindex++;
-        int nv = 0;
-        if (sscanf(line.c_str(), "%d %d", &temp, &nv) != 2) return fail_format(WRONG);
-        if (nv < 4) return fail_format(FEW);
-        rings.emplace_back();
-        for (int j = 0; j < nv; j++) {
-            rd.next(&line);
-            lineindex++;
+    // vertex lines beyond the end of the file read as "": the first fails
+    std::vector<long long> vfirst(blocks.size() + 1, 0);  // flattened vertex index of each block
+    for (size_t r = 0; r < blocks.size(); r++) {
+        long long have = std::max(0LL, std::min<long long>(blocks[r].nv, nlines - blocks[r].first));
+        if (have < blocks[r].nv) note(blocks[r].first + have + 1, WRONG);
+        vfirst[r + 1] = vfirst[r] + have;
+    }
+    // (announced counts may be absurd in a truncated file: 64-bit sums, and
+    // vertex storage only once every announced line is present)
+    std::vector<long long> ring_start(1, 0);
+    for (const Block& bl : blocks) ring_start.push_back(ring_start.back() + bl.nv - 1);
+    std::vector<double> lonlat;
+    if (fail_line == LLONG_MAX) {
+        if (ring_start.back() > INT_MAX / 2) {
+            set_error("%s: %lld vertices exceed the loader's limit", path, ring_start.back());
+            return GAHHG_ERR_CAPACITY;
+        }
+        lonlat.resize(2 * (size_t)ring_start.back());
+    }
+    std::mutex mu;
+    parallel_ranges(vfirst.back(), 1 << 15, [&](long long a, long long b) {
+        long long bad = LLONG_MAX;
+        size_t r = std::upper_bound(vfirst.begin(), vfirst.end(), a) - vfirst.begin() - 1;
+        for (long long v = a; v < b; v++) {
+            while (v >= vfirst[r + 1]) r++;
+            const long long j = v - vfirst[r];
+            const long long ln = blocks[r].first + j;
             double lo, la;
-            if (!parse_two(line, &lo, &la)) return fail_format(WRONG);
-            if (j < nv - 1) {
-                rings.back().push_back(lo);
-                rings.back().push_back(la);
+            if (!parse_two_line(line_begin(ln), line_end(ln), &lo, &la)) {
+                bad = std::min(bad, ln + 1);
+                continue;
+            }
+            if (j < blocks[r].nv - 1 && !lonlat.empty()) {
+                const size_t at = 2 * ((size_t)ring_start[r] + (size_t)j);
+                lonlat[at] = lo;
+                lonlat[at + 1] = la;
             }
         }
+        if (bad != LLONG_MAX) {
+            std::lock_guard<std::mutex> lock(mu);
+            note(bad, WRONG);
+        }
+    });
+    if (fail_line != LLONG_MAX) {
+        printf("Error. Line %lld of %s. %s\n", fail_line, path, fail_what);
+        set_error("line %lld of %s: %s", fail_line, path, fail_what);
+        return GAHHG_ERR_FORMAT;
     }
     P->path = path;
-    P->num_rings = (int)rings.size();
-    P->ring_start.assign(1, 0);
-    P->lonlat.clear();
-    for (auto& r : rings) {
-        P->lonlat.insert(P->lonlat.end(), r.begin(), r.end());
-        P->ring_start.push_back(P->ring_start.back() + (int)(r.size() / 2));
-    }
+    P->num_rings = (int)blocks.size();
+    P->ring_start.assign(ring_start.begin(), ring_start.end());
+    P->lonlat = std::move(lonlat);
     assemble(P);
     return GAHHG_OK;
 }

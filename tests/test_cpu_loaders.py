@@ -102,3 +102,83 @@ def test_sidecar(tmp_path):
     with pytest.raises(G.GahhgError) as e:
         G.load_points(path, sidecar=True)
     assert e.value.status == _lib.ERR_IO
+
+
+# ---- POLYGON files large enough for the threaded vertex parse ------------
+
+def _big_polygon_lines():
+    """A 200,000-vertex outer ring and three holes as POLYGON text lines,
+    with some vertex lines in the forms that only the serial "%lf %lf"
+    reading handles (a '+' sign, hex, tabs, CRLF, trailing text, no space
+    before a minus sign)."""
+    from gahhg_b200 import synth
+    rng = np.random.default_rng(31)
+    rings = [synth.star_ring(40.0, -10.0, 200_000, 20.0, 0.2, rng)]
+    for k in range(3):
+        rings.append(synth.star_ring(40.0 + 4.0 * (k - 1), -10.0, 5_000 + k, 1.0, 0.1, rng)[::-1])
+    lines = ["POLYGON 1 %d" % (len(rings) - 1)]
+    for i, r in enumerate(rings):
+        lines.append("%d %d" % (i, len(r) + 1))
+        lines += ["%.17g %.17g" % (lo, la) for lo, la in np.concatenate([r, r[:1]])]
+    for at, form in [(10, "+{} {}"), (50_001, "{}\t{}"), (120_000, "{} {}\r"), (150_000, "{}  {} trailing"),
+                     (180_000, "  {} {}")]:
+        lo, la = (float(x) for x in lines[at].split())
+        lines[at] = form.format(repr(lo), repr(la))
+    lines[70_000] = "%s %s" % (float(lines[70_000].split()[0]).hex(), lines[70_000].split()[1])
+    lo, la = (float(x) for x in lines[90_000].split())
+    lines[90_000] = "%r%r" % (lo, -abs(la)) if la != 0 else lines[90_000]
+    return lines
+
+
+@pytest.fixture(scope="module")
+def big_polygon_lines():
+    return _big_polygon_lines()
+
+
+def _write_lines(path, lines, final_newline=True):
+    with open(path, "w", newline="") as f:
+        f.write("\n".join(lines) + ("\n" if final_newline else ""))
+
+
+def test_large_polygon_matches_reference(big_polygon_lines, tmp_path, oracle_ref):
+    path = str(tmp_path / "big.txt")
+    _write_lines(path, big_polygon_lines)
+    P = G.Polygon.from_file(path)
+    xyz, pe = P.export()
+    assert len(xyz) == 200_000 + 5_000 + 5_001 + 5_002
+    rx, rp = oracle_ref.RefGPISP(path, maxdepth=1).polygon()
+    assert np.array_equal(xyz, rx) and np.array_equal(pe, rp)
+    # no final newline: same polygon
+    _write_lines(path, big_polygon_lines, final_newline=False)
+    x2, p2 = G.Polygon.from_file(path).export()
+    assert np.array_equal(x2, rx) and np.array_equal(p2, rp)
+
+
+def test_large_polygon_first_error(big_polygon_lines, tmp_path, capfd, oracle_ref):
+    """Wherever the faults are, the message names the first one in file order,
+    as the reference's serial reading does."""
+    hole1 = 2 + 200_001          # 0-based line of the first hole's header
+    cases = [
+        {150_000: "1.0 x"},                            # a vertex line of the outer ring
+        {hole1 + 3: "nan?", 199_000: "1,2"},            # two faults: the earlier one counts
+        {hole1: "1 3"},                                 # a hole with too few vertices
+        {hole1 + 5_002: "junk"},                        # the second hole's header
+        {hole1 + 5_002: "junk", 60_000: "1e 2"},        # a vertex fault before a header fault
+        {"truncate": hole1 + 5_002 + 100},              # the file ends inside a hole
+    ]
+    for case in cases:
+        lines = list(big_polygon_lines)
+        if "truncate" in case:
+            lines = lines[:case["truncate"]]
+        else:
+            for at, text in case.items():
+                lines[at] = text
+        path = str(tmp_path / "bad.txt")
+        _write_lines(path, lines)
+        with pytest.raises(G.GahhgError):
+            G.Polygon.from_file(path)
+        ours = [l for l in capfd.readouterr().out.splitlines() if l.startswith("Error.")]
+        with pytest.raises(ValueError):
+            oracle_ref.RefGPISP(path, maxdepth=1)
+        ref = [l for l in capfd.readouterr().out.splitlines() if l.startswith("Error.")]
+        assert ours == ref and len(ours) == 1, (case, ours, ref)
