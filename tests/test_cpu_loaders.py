@@ -182,3 +182,31 @@ def test_large_polygon_first_error(big_polygon_lines, tmp_path, capfd, oracle_re
             oracle_ref.RefGPISP(path, maxdepth=1)
         ref = [l for l in capfd.readouterr().out.splitlines() if l.startswith("Error.")]
         assert ours == ref and len(ours) == 1, (case, ours, ref)
+
+
+@pytest.mark.parametrize("text", [
+    "",                                                     # empty file
+    "POLYGON 1 0\n",                                        # header only
+    "POLYGON 1 1\n0 5\n0 0\n10 0\n10 10\n0 10\n0 0",        # a hole announced, the file ends
+    "POLYGON 1 0\r\n0 5\r\n0 0\r\n10 0\r\n10 10\r\n0 10\r\n0 0\r\n",   # CRLF lines
+    "POLYGON 1 0\n0 5 extra\n0 0\n10 0\n10 10\n0 10\n0 0",  # text after the count, no final newline
+    "POLYGON 1 0\n0 5\n0 0\n10 0\n10 10\n0 10\n",           # one vertex line short
+])
+def test_polygon_edge_cases_match_reference(text, tmp_path, capfd, oracle_ref):
+    path = str(tmp_path / "p.txt")
+    with open(path, "w", newline="") as f:
+        f.write(text)
+    try:
+        ours = G.Polygon.from_file(path).export()
+    except G.GahhgError:
+        ours = None
+    out_ours = [l for l in capfd.readouterr().out.splitlines() if l.startswith("Error.")]
+    try:
+        ref = oracle_ref.RefGPISP(path, maxdepth=1).polygon()
+    except ValueError:
+        ref = None
+    out_ref = [l for l in capfd.readouterr().out.splitlines() if l.startswith("Error.")]
+    assert out_ours == out_ref
+    assert (ours is None) == (ref is None)
+    if ours is not None:
+        assert np.array_equal(ours[0], ref[0]) and np.array_equal(ours[1], ref[1])
