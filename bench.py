@@ -53,15 +53,28 @@ def _peaks():
         return 6650.0, "fallback"
 
 
+def gpu_uuid(local):
+    """nvidia-smi id of the GPU this process uses: its UUID (nvidia-smi's own
+    indices ignore CUDA_VISIBLE_DEVICES, so a local ordinal may name another
+    job's GPU)."""
+    try:
+        import torch
+        u = str(torch.cuda.get_device_properties(local).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return str(local)
+
+
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+    """nvidia-smi clocks and throttle reasons while the timed region runs
+    (read-only queries of the GPU given by its UUID)."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index):
-        self.index = index
+    def __init__(self, local):
+        self.index = gpu_uuid(local)
         self.proc = None
         self.lines = []
 
@@ -103,7 +116,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "gpu": self.index}
 
 
 class quiet_stdout:

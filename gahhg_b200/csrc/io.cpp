@@ -205,8 +205,16 @@ gahhg_status load_polygon_file(const char* path, Polygon* P)
         const size_t e = (k + 1 < nlines) ? start[k + 1] - 1 : data.size();
         return data.data() + ((e > start[k] && data[e - 1] == '\n') ? e - 1 : e);
     };
+    // The reference reads each line with getline(buf, size), size = the
+    // file's size, which stores at most size - 1 characters: only a file that
+    // is a single line without '\n' reaches that, and it loses its last
+    // character (the stream then fails, so later lines read as "").
+    const bool cut_last = nlines == 1 && !data.empty() && data.back() != '\n';
     auto line_str = [&](long long k) {
-        return k < nlines ? std::string(line_begin(k), line_end(k)) : std::string();
+        if (k >= nlines) return std::string();
+        std::string s(line_begin(k), line_end(k));
+        if (cut_last && !s.empty()) s.pop_back();
+        return s;
     };
     // The first failing line (1-based, as the reference counts) and its message.
     long long fail_line = LLONG_MAX;

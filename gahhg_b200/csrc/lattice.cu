@@ -1292,14 +1292,12 @@ __global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, 
     if (!mbar_wait(&s_bar, 0)) s_late = 1;
     __syncthreads();
     const bool late = s_late != 0;
-    if (late) {
-        // the pending copy can only write these same words
-        if (threadIdx.x == 0) atomicAdd(&g_tma_timeouts, 1u);
-        for (int k = threadIdx.x; k < Q.swords; k += TPB) s_sum[k] = __ldg(Q.summary + k);
-        __syncthreads();
-    }
+    // after a wait that ran out the block reads the summary from global
+    // memory and never touches s_sum, which the pending copy still targets
+    if (late && threadIdx.x == 0) atomicAdd(&g_tma_timeouts, 1u);
     int inside = 0;
-    locate_range<STATS>(Q, s_sum, ll, out, queue, leafq, qcount, 0, n, blockIdx.x, gridDim.x, inside);
+    locate_range<STATS>(Q, late ? Q.summary : s_sum, ll, out, queue, leafq, qcount, 0, n, blockIdx.x, gridDim.x,
+                        inside);
     if (late) mbar_wait(&s_bar, 0);  // the copy in flight ends before the block does (bounded)
     allow_dependents();
     if (STATS && ctr) count_inside(inside, ctr + 3);
@@ -2431,30 +2429,25 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
 constexpr long long NOALLOC_MAX_POINTS = 1LL << 21;  // 2,097,152 points per call
 static __device__ __align__(256) uint32_t g_noalloc_queue[NOALLOC_MAX_POINTS + 64];
 
-static std::mutex g_noalloc_mu;
-static uint32_t* g_noalloc_addr[64] = {};
-
 long long lattice_noalloc_max_points() { return NOALLOC_MAX_POINTS; }
 
-// Device address of the array on the current device, looked up once per
-// device (the caller has made g->device current).
+// Device address of the array on the current device (the caller has made
+// g->device current).  In host code `g_noalloc_queue` names a host-side
+// stand-in, never the device array, so the address is asked of the runtime.
+// It is looked up on every call rather than cached: after cudaDeviceReset
+// (or any other teardown of the primary context) the module is loaded again
+// and the array may sit at another address.  The lookup allocates nothing;
+// the first one on a device loads the module there, which is why the first
+// call on a device should come before any stream capture.
 static gahhg_status noalloc_queue_address(int device, uint32_t** out)
 {
-    if (device < 0 || device >= 64) {
-        set_error("device ordinal %d out of range", device);
-        return GAHHG_ERR_ARG;
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_queue);
+    if (e != cudaSuccess || !p) {
+        set_error("cudaGetSymbolAddress(g_noalloc_queue) on device %d: %s", device, cudaGetErrorString(e));
+        return GAHHG_ERR_CUDA;
     }
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[device]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_queue);
-        if (e != cudaSuccess || !p) {
-            set_error("cudaGetSymbolAddress(g_noalloc_queue) on device %d: %s", device, cudaGetErrorString(e));
-            return GAHHG_ERR_CUDA;
-        }
-        g_noalloc_addr[device] = (uint32_t*)p;
-    }
-    *out = g_noalloc_addr[device];
+    *out = (uint32_t*)p;
     return GAHHG_OK;
 }
 

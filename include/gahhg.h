@@ -159,9 +159,11 @@ gahhg_status gahhg_query(gahhg_grid* g, const double* lonlat, size_t n, uint8_t*
  *
  * Limits: at most gahhg_query_noalloc_max_points() points per call (2,097,152;
  * more returns GAHHG_ERR_CAPACITY); exact grids only (GAHHG_QUERY_AUTO,
- * _FP32_FILTER or _FP64_FILTER); no statistics are collected.  The first call
- * on a device looks up the array's device address, so make that first call
- * before any stream capture.  All calls share the one array and it keeps the
+ * _FP32_FILTER or _FP64_FILTER); no statistics are collected.  Every call
+ * asks the runtime for the array's device address (nothing is cached, so the
+ * address stays right after a cudaDeviceReset); the first call on a device
+ * also loads the library's kernels there, so make that first call before any
+ * stream capture.  All calls share the one array and it keeps the
  * last call's contents: calls whose work overlaps on the GPU (two streams,
  * two host threads) race, so order them on one stream or serialise them. */
 gahhg_status gahhg_query_device_noalloc(gahhg_grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels,

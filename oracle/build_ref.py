@@ -33,7 +33,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 OUT = os.path.join(HERE, "_ref")
 SHIM = os.path.join(HERE, "refshim")
-DEFAULT_SRC = "/root/reference/source"
+# The reference checkout: $GAHHG_REFERENCE (default /root/reference); its
+# sources are under source/.
+REFERENCE_ROOT = os.environ.get("GAHHG_REFERENCE", "/root/reference")
+DEFAULT_SRC = os.path.join(REFERENCE_ROOT, "source")
 
 LAUNCH_RE = re.compile(r"(\w+)\s*<<\s*<\s*(.+?)\s*>>\s*>\s*\(")
 BBOX_BUG = "for (int j = 0; j < inVNum[i]; i++)"

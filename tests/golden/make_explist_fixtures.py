@@ -81,7 +81,8 @@ def _run_one(args):
     return stats, dig, lab, ex
 
 
-def main(refroot="/root/reference"):
+def main(refroot=None):
+    refroot = refroot or os.environ.get("GAHHG_REFERENCE", "/root/reference")
     from tests.golden.fixtures import Inputs, fmt6
     store = Inputs()
     invs = select(invocations(refroot))

@@ -97,7 +97,8 @@ def digest(*arrays):
     return h.hexdigest()
 
 
-def main(refroot="/root/reference"):
+def main(refroot=None):
+    refroot = refroot or os.environ.get("GAHHG_REFERENCE", "/root/reference")
     from tests.golden import fixtures
     from oracle import ref
 

@@ -187,6 +187,8 @@ def test_large_polygon_first_error(big_polygon_lines, tmp_path, capfd, oracle_re
 @pytest.mark.parametrize("text", [
     "",                                                     # empty file
     "POLYGON 1 0\n",                                        # header only
+    "POLYGON 1 0",                                          # one line, no newline: getline keeps size - 1 chars
+    "POLYGON 1 12",                                         # the same, with a count the cut shortens
     "POLYGON 1 1\n0 5\n0 0\n10 0\n10 10\n0 10\n0 0",        # a hole announced, the file ends
     "POLYGON 1 0\r\n0 5\r\n0 0\r\n10 0\r\n10 10\r\n0 10\r\n0 0\r\n",   # CRLF lines
     "POLYGON 1 0\n0 5 extra\n0 0\n10 0\n10 10\n0 10\n0 0",  # text after the count, no final newline
