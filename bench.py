@@ -14,6 +14,14 @@ antimeridian and containing the north pole) and ten 10,000-vertex holes;
 host buffers, host->device and device->host copies inside the timed region.
 With N > 1 (torchrun) each rank queries its own replica (the path shards by
 points, with no exchange); the slowest rank's time is used.
+
+At N = 1 the same line carries the other configurations as keys (skipped
+with --no-legs): "c2" (the C1 polygon's index on 2e7 points, half within
+10^U[-15,-3] rad of an edge: FP32-filtered and FP64-filtered rates and
+escalation fractions), "c3" (a batch of 1,024 batch-configuration polygons,
+autotuned, CUDA-graph replay) and "c4" (10 s of serving at 2,000 requests/s
+over those 1,024 polygons: p50/p99 latency and sustained points/s).
+--config c2|c3|c4 runs one configuration alone at full size.
 """
 import argparse
 import ctypes
@@ -152,50 +160,6 @@ def c1_polygon_cached():
 _C1_RINGS = None
 
 
-def device_points(n, seed, device):
-    import torch
-    g = torch.Generator(device=device)
-    g.manual_seed(seed)
-    u = torch.rand((n, 2), generator=g, device=device, dtype=torch.float64)
-    pts = torch.empty((n, 2), device=device, dtype=torch.float64)
-    pts[:, 0] = u[:, 0] * 360.0 - 180.0
-    pts[:, 1] = torch.rad2deg(torch.asin(u[:, 1] * 2.0 - 1.0))
-    return pts
-
-
-def device_c2_points(rings, n, seed, device):
-    """C2 points on the device: half uniform by area, half on a uniform random
-    edge at a uniform arc parameter, offset along the edge-plane normal by
-    +-10^u rad with u ~ U[-15, -3] (the construction of synth.near_edge_points)."""
-    import torch
-    g = torch.Generator(device=device)
-    g.manual_seed(seed)
-    ll = torch.as_tensor(np.concatenate(rings), dtype=torch.float64, device=device)
-    starts = np.cumsum([0] + [len(r) for r in rings])
-    nxt = np.arange(len(ll)) + 1
-    for a, b in zip(starts[:-1], starts[1:]):
-        nxt[b - 1] = a
-    nxt = torch.as_tensor(nxt, device=device)
-    lo, la = torch.deg2rad(ll[:, 0]), torch.deg2rad(ll[:, 1])
-    xyz = torch.stack([torch.cos(la) * torch.sin(lo), torch.sin(la), torch.cos(la) * torch.cos(lo)], 1)
-    pts = device_points(n, seed + 1, device)
-    m = n // 2
-    e = torch.randint(0, len(ll), (m,), generator=g, device=device)
-    A, B = xyz[e], xyz[nxt[e]]
-    t = torch.rand((m, 1), generator=g, device=device, dtype=torch.float64)
-    P = (1 - t) * A + t * B
-    P = P / torch.linalg.norm(P, dim=1, keepdim=True)
-    N = torch.linalg.cross(A, B)
-    N = N / torch.clamp(torch.linalg.norm(N, dim=1, keepdim=True), min=1e-300)
-    u = torch.rand(m, generator=g, device=device, dtype=torch.float64) * 12.0 - 15.0
-    sign = torch.where(torch.rand(m, generator=g, device=device) < 0.5, -1.0, 1.0).to(torch.float64)
-    Q = P + (torch.pow(10.0, u) * sign)[:, None] * N
-    Q = Q / torch.linalg.norm(Q, dim=1, keepdim=True)
-    pts[m:, 1] = torch.rad2deg(torch.asin(torch.clamp(Q[:, 1], -1.0, 1.0)))
-    pts[m:, 0] = torch.rad2deg(torch.atan2(Q[:, 0], Q[:, 2]))
-    return pts
-
-
 def timed_loop(fn, steps, stream):
     import torch
     e0 = torch.cuda.Event(enable_timing=True)
@@ -274,55 +238,19 @@ def run_reference(args):
     return 0
 
 
-def device_cap_points(lons, lats, radii_deg, counts, seed, device):
-    """Points uniform by area inside each polygon's cap (1.5 x the bounding
-    radius 1.2 r of a star polygon of radius r), generated on the device."""
-    import torch
-    g = torch.Generator(device=device)
-    g.manual_seed(seed)
-    counts = np.asarray(counts, dtype=np.int64)
-    n = int(counts.sum())
-    pts = torch.empty((n, 2), dtype=torch.float64, device=device)
-    lon_all = torch.as_tensor(lons, dtype=torch.float64, device=device) * (np.pi / 180)
-    lat_all = torch.as_tensor(lats, dtype=torch.float64, device=device) * (np.pi / 180)
-    R_all = torch.clamp(torch.as_tensor(radii_deg, dtype=torch.float64, device=device) * (1.5 * 1.2 * np.pi / 180),
-                        max=np.pi)
-    starts = np.concatenate([[0], np.cumsum(counts)])
-    p0 = 0
-    while p0 < len(counts):  # polygon ranges of about 32M points keep the temporaries small
-        p1 = p0
-        while p1 < len(counts) and (p1 == p0 or starts[p1 + 1] - starts[p0] <= (1 << 25)):
-            p1 += 1
-        cnt = torch.as_tensor(counts[p0:p1], dtype=torch.int64, device=device)
-        idx = torch.repeat_interleave(torch.arange(p0, p1, device=device), cnt)
-        m = int(starts[p1] - starts[p0])
-        lon0, lat0, R = lon_all[idx], lat_all[idx], R_all[idx]
-        u = torch.rand((m, 2), generator=g, device=device, dtype=torch.float64)
-        c = torch.cos(R) + (1.0 - torch.cos(R)) * u[:, 0]
-        d = torch.arccos(torch.clamp(c, -1.0, 1.0))
-        b = u[:, 1] * 2 * np.pi
-        sl = torch.sin(lat0) * torch.cos(d) + torch.cos(lat0) * torch.sin(d) * torch.cos(b)
-        la2 = torch.asin(torch.clamp(sl, -1.0, 1.0))
-        lo2 = lon0 + torch.atan2(torch.sin(b) * torch.sin(d) * torch.cos(lat0), torch.cos(d) - torch.sin(lat0) * sl)
-        out = pts[starts[p0]:starts[p1]]
-        out[:, 0] = torch.remainder(lo2 * (180 / np.pi) + 180.0, 360.0) - 180.0
-        out[:, 1] = la2 * (180 / np.pi)
-        del idx, lon0, lat0, R, u, c, d, b, sl, la2, lo2
-        p0 = p1
-    return pts
-
-
-def run_c3(args):
+def run_c3(args, count=None, tune_budget=None, steps=None, polys=None):
     """Batch configuration: 4,096 star polygons (16-200,000 vertices, 0-8
     holes, radius 0.5-40 deg, ~5 % around a pole), each with 1e3-1e6 points
     inside its 1.5x bounding cap; autotuned lattices; one CUDA-graph query
-    over all points per step."""
+    over all points per step.  `count` polygons of that generator (default
+    --c3-polygons); returns the result line as a dict (and the polygons)."""
     import torch
     import gahhg_b200 as G
     from gahhg_b200 import autotune, synth
     dev = "cuda:0"
     t0 = time.time()
-    polys = synth.c3_polygons(args.c3_polygons, seed=3)
+    if polys is None:
+        polys = synth.c3_polygons(count or args.c3_polygons, seed=3)
     P = [G.Polygon.from_rings(r) for r, _c, _r in polys]
     gen_s = time.time() - t0
     rng = np.random.default_rng(4)
@@ -338,7 +266,8 @@ def run_c3(args):
     def sample(i):
         return synth.cap_points(lons[i], lats[i], 1.5 * 1.2 * radii[i], 20000, np.random.default_rng(100 + i))
 
-    tuning = autotune.tune(P, sample, per_class=2, reps=3, budget_s=args.tune_budget)
+    tuning = autotune.tune(P, sample, per_class=2, reps=3,
+                           budget_s=args.tune_budget if tune_budget is None else tune_budget)
     tune_s = time.time() - t0
     tc, le = tuning.for_polygons(P)
     torch.cuda.synchronize()
@@ -346,7 +275,7 @@ def run_c3(args):
     B = G.Batch(P, top_cells=tc, leaf_edges=le)
     build_wall = time.time() - t0
     bst = B.stats()
-    d_pts = device_cap_points(lons, lats, radii, counts, 5, dev)
+    d_pts = synth.device_cap_points(lons, lats, radii, counts, 5, dev)
     n = int(offsets[-1])
     d_lab = torch.empty(n, dtype=torch.uint8, device=dev)
     chunk = autotune.tune_chunk(B, d_pts, offsets, d_lab, reps=2)
@@ -364,13 +293,15 @@ def run_c3(args):
     clocks = ClockSampler(0)
     clocks.start()
     time.sleep(0.3)
-    steps = max(3, args.steps // 20)
+    steps = steps or max(3, args.steps // 20)
     t = timed_loop(step, steps, stream)
     clk = clocks.stop()
     per = t / steps
     peak, peak_kind = _peaks()
     achieved = BYTES_PER_POINT * n / per / 1e9
-    print(json.dumps({
+    del d_pts, d_lab, B
+    torch.cuda.empty_cache()
+    return ({
         "metric": METRIC, "value": round(n / per / 1e6, 1), "unit": "Mpts/s", "n_gpus": 1, "steps": steps,
         "warmup": args.warmup, "ms_per_step": round(per * 1e3, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -387,11 +318,10 @@ def run_c3(args):
         "lattice_bytes": bst["lattice_bytes"], "tuning": tuning.as_dict(), "chunk_points": chunk,
         "escalation": {"boundary_points": esc["boundary_points"], "fp64_tests": esc["esc_fp64"],
                        "exact_tests": esc["esc_exact"], "boundary_fraction": round(esc["boundary_points"] / n, 6)},
-    }))
-    return 0
+    }, polys)
 
 
-def run_c4(args):
+def run_c4(args, polys=None, seconds=None, pool_n=None, tune_budget=None):
     """Serving configuration: 1,024 resident C3-style polygons (built through
     the server, pinned); open-loop Poisson arrivals at `--c4-rate` requests/s
     for `--c4-seconds`: 95 % queries (polygon uniform over the residents,
@@ -399,13 +329,15 @@ def run_c4(args):
     memory), 5 % builds of new C3-style polygons admitted by HBM footprint
     (the budget leaves `--c4-headroom` GB above the residents; the least
     recently used unpinned indexes are evicted).  Latency is submission to
-    labels in host memory."""
+    labels in host memory.  `polys` (generator output) replaces the resident
+    set's generation; returns the result line as a dict."""
     import torch
     import gahhg_b200 as G
     from gahhg_b200 import autotune, synth
     dev = "cuda:0"
     t0 = time.time()
-    polys = synth.c3_polygons(args.c4_polygons, seed=41)
+    if polys is None:
+        polys = synth.c3_polygons(args.c4_polygons, seed=41)
     fresh = synth.c3_polygons(args.c4_new, seed=42)
     P = [G.Polygon.from_rings(r) for r, _c, _r in polys]
     NP = [G.Polygon.from_rings(r) for r, _c, _r in fresh]
@@ -418,7 +350,8 @@ def run_c4(args):
         return synth.cap_points(lons[i], lats[i], 1.5 * 1.2 * radii[i], 20000, np.random.default_rng(200 + i))
 
     t0 = time.time()
-    tuning = autotune.tune(P, sample, per_class=1, reps=2, budget_s=args.tune_budget)
+    tuning = autotune.tune(P, sample, per_class=1, reps=2,
+                           budget_s=args.tune_budget if tune_budget is None else tune_budget)
     tune_s = time.time() - t0
     tc, le = tuning.for_polygons(P)
     ntc, nle = tuning.for_polygons(NP)
@@ -439,8 +372,9 @@ def run_c4(args):
     srv.close()
     srv, ids, _ = serve(resident * 1.02 + args.c4_headroom * 1e9)
     # point pools: pool_n points per polygon inside its cap, pageable host memory
-    pool_n = args.c4_pool
-    d_pool = device_cap_points(lons, lats, radii, [pool_n] * len(P), 43, dev)
+    pool_n = pool_n or args.c4_pool
+    seconds = seconds or args.c4_seconds
+    d_pool = synth.device_cap_points(lons, lats, radii, [pool_n] * len(P), 43, dev)
     pool = d_pool.cpu().numpy()
     del d_pool
     torch.cuda.empty_cache()
@@ -448,9 +382,9 @@ def run_c4(args):
     total = len(pool)
     # the arrival schedule
     rng = np.random.default_rng(44)
-    nev = int(args.c4_rate * args.c4_seconds * 1.1) + 16
+    nev = int(args.c4_rate * seconds * 1.1) + 16
     times = np.cumsum(rng.exponential(1.0 / args.c4_rate, nev))
-    times = times[times < args.c4_seconds]
+    times = times[times < seconds]
     nev = len(times)
     is_build = rng.random(nev) < args.c4_build_frac
     qpoly = rng.integers(0, len(P), nev)
@@ -517,7 +451,8 @@ def run_c4(args):
     def pct(a, q):
         return round(float(np.percentile(a, q)), 4) if len(a) else None
 
-    print(json.dumps({
+    del pool, lab_pool
+    return {
         "metric": METRIC, "value": round(st["p99_ms"], 3), "unit": "ms (query p99)", "n_gpus": 1,
         "steps": int(st["queries_done"]), "warmup": 0,
         "ms_per_step": round(float(lat.mean()), 4) if len(lat) else None,
@@ -525,7 +460,7 @@ def run_c4(args):
         "config": {"workload": "C4: %d resident C3-style polygons; Poisson arrivals at %g req/s for %g s: %d %% "
                                "queries (uniform polygon, log-uniform 1-1e6 points from pageable host memory), %d %% "
                                "builds of new C3-style polygons admitted by HBM footprint with LRU eviction"
-                               % (len(P), args.c4_rate, args.c4_seconds, round(100 * (1 - args.c4_build_frac)),
+                               % (len(P), args.c4_rate, seconds, round(100 * (1 - args.c4_build_frac)),
                                   round(100 * args.c4_build_frac)),
                    "polygons": len(P), "slots": args.c4_slots, "slot_points": args.c4_slot_points,
                    "build_workers": args.c4_workers, "pool_points_per_polygon": pool_n,
@@ -534,7 +469,7 @@ def run_c4(args):
                        "max": round(st["max_ms"], 3), "build_p50": round(st["build_p50_ms"], 2),
                        "build_p99": round(st["build_p99_ms"], 2)},
         "throughput": {"sustained_mpts_s": round(sustained / 1e6, 3),
-                       "offered_mpts_s": round(offered_pts / args.c4_seconds / 1e6, 3),
+                       "offered_mpts_s": round(offered_pts / seconds / 1e6, 3),
                        "queries": int(st["queries_done"]), "builds_done": int(st["builds_done"]),
                        "builds_failed": int(st["builds_failed"]), "evictions": int(st["evictions"]),
                        "batches": int(st["batches"]), "mean_batch_pieces": round(st["mean_batch_pieces"], 2),
@@ -557,8 +492,7 @@ def run_c4(args):
         "build_ms": {"resident_set_wall": round(resident_build_s * 1e3, 1), "resident_bytes": resident,
                      "generate_s": round(gen_s, 1), "autotune_s": round(tune_s, 1)},
         "tuning": tuning.as_dict(),
-    }))
-    return 0
+    }
 
 
 def main():
@@ -590,13 +524,20 @@ def main():
     ap.add_argument("--c4-pool", type=int, default=1 << 19, help="host points per resident polygon")
     ap.add_argument("--c4-headroom", type=float, default=8.0, help="GB of budget above the resident set")
     ap.add_argument("--c4-trace", default=None, help="save the per-batch trace and latencies (.npz)")
+    ap.add_argument("--no-legs", action="store_true", help="C1 only (no C2/C3/C4 keys in the default run)")
+    ap.add_argument("--leg-c3-polygons", type=int, default=1024)
+    ap.add_argument("--leg-tune-budget", type=float, default=15.0)
+    ap.add_argument("--leg-c4-seconds", type=float, default=10.0)
+    ap.add_argument("--leg-c4-pool", type=int, default=1 << 17)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.config == "c3":
-        return run_c3(args)
+        print(json.dumps(run_c3(args)[0]))
+        return 0
     if args.config == "c4":
-        return run_c4(args)
+        print(json.dumps(run_c4(args)))
+        return 0
 
     import torch
     import torch.distributed as dist
@@ -637,9 +578,9 @@ def main():
     c2 = args.config == "c2"
     n = args.c2_points if c2 else args.points
     if c2:
-        pts = device_c2_points(rings, n, 2222 + rank, "cuda:%d" % local)
+        pts = synth.device_c2_points(rings, n, 2222 + rank, "cuda:%d" % local)
     else:
-        pts = device_points(n, 1234 + rank, "cuda:%d" % local)
+        pts = synth.device_points(n, 1234 + rank, "cuda:%d" % local)
     labels = torch.empty(n, dtype=torch.uint8, device="cuda:%d" % local)
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
@@ -743,6 +684,9 @@ def main():
                      "frac": round(achieved / peak, 4),
                      "traffic": args.traffic if args.traffic is not None else (
                          round(_traffic_per_point() * n) if _traffic_per_point() else None),
+                     "traffic_source": "given on the command line" if args.traffic is not None else
+                                       "scaled ncu capture (profiles/locate_traffic.json: DRAM bytes per point "
+                                       "of one k_locate launch on 1e7 C1 points, times the points per step)",
                      "bytes_per_point": BYTES_PER_POINT, "peak_source": peak_kind},
         "cpu_baseline": cpu,
         "e2e": {"value": round(e2e_rate, 1), "unit": "Mpts/s", "h2d_bytes_per_step": 16 * e2e_n,
@@ -776,8 +720,74 @@ def main():
         "inside_fraction": round(inside / n, 6),
         "lattice_bytes": st_build["lattice_bytes"],
     }
+    if args.config == "c1" and world == 1 and not args.no_legs:
+        # the other configurations as keys of the same line: C2 on the same
+        # polygon and index, then a reduced C3 batch and a shortened C4
+        # serving run on the same 1,024 batch-configuration polygons
+        del pts, labels, host_ll, host_lab
+        torch.cuda.empty_cache()
+        out["c2"] = leg_c2(args, g, gref, rings, stream)
+        del g, gref
+        torch.cuda.empty_cache()
+        out["c3"], polys = run_c3(args, count=args.leg_c3_polygons, tune_budget=args.leg_tune_budget,
+                                  steps=max(3, args.steps // 4))
+        torch.cuda.empty_cache()
+        out["c4"] = run_c4(args, polys=polys, seconds=args.leg_c4_seconds, pool_n=args.leg_c4_pool,
+                           tune_budget=args.leg_tune_budget)
     print(json.dumps(out))
     return 0
+
+
+def leg_c2(args, g, gref, rings, stream):
+    """C2 on the C1 polygon's index: FP32-filtered and FP64-filtered exact
+    query rates and escalation fractions, and the reference algorithm's FP64
+    descent, on `--c2-points` points (half uniform, half within
+    10^U[-15,-3] rad of a random edge) resident in HBM."""
+    import torch
+    import gahhg_b200 as G
+    from gahhg_b200 import synth
+    n = args.c2_points
+    pts = synth.device_c2_points(rings, n, 2222, "cuda:0")
+    labels = torch.empty(n, dtype=torch.uint8, device="cuda:0")
+    sh = stream.cuda_stream
+    lp, pp = labels.data_ptr(), pts.data_ptr()
+    rates, esc = {}, {}
+    steps = max(10, args.steps)
+    for name, prec in (("fp32_filter", G.QUERY_FP32_FILTER), ("fp64_filter", G.QUERY_FP64_FILTER)):
+        g.query_device(pp, n, lp, prec, sh, sync=True)
+        esc[name] = g.stats()
+        for _ in range(max(3, args.warmup)):
+            g.query_device(pp, n, lp, prec, sh)
+        t = timed_loop(lambda: g.query_device(pp, n, lp, prec, sh), steps, stream)
+        rates[name] = n * steps / t / 1e6
+    for _ in range(2):
+        gref.query_device(pp, n, lp, G.QUERY_REFERENCE_FP64, sh)
+    kref = 3
+    tref = timed_loop(lambda: gref.query_device(pp, n, lp, G.QUERY_REFERENCE_FP64, sh), kref, stream) / kref
+    peak, peak_kind = _peaks()
+    e32 = esc["fp32_filter"]
+    per32 = n / (rates["fp32_filter"] * 1e6)
+    del pts, labels
+    return {
+        "workload": "C2: the C1 polygon (1.1M edges); %d FP64 points, half uniform by area, half within "
+                    "10^U[-15,-3] rad of a random edge; exact labels" % n,
+        "points_per_step": n, "steps": steps,
+        "value": round(rates["fp32_filter"], 1), "unit": "Mpts/s",
+        "fp32_filter_mpts": round(rates["fp32_filter"], 1),
+        "fp64_filter_mpts": round(rates["fp64_filter"], 1),
+        "fp32_over_fp64_filter": round(rates["fp32_filter"] / rates["fp64_filter"], 3),
+        "reference_fp64_descent_mpts": round(n / tref / 1e6, 1),
+        "reference_fp64_max_depth": REF_DEPTH_C1,
+        "roofline": {"bound": "hbm", "achieved": round(BYTES_PER_POINT * n / per32 / 1e9, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(BYTES_PER_POINT * n / per32 / 1e9 / peak, 4),
+                     "peak_source": peak_kind},
+        "escalation": {"boundary_points": e32["boundary_points"],
+                       "fp32_to_fp64_points": e32["esc_fp64"], "fp64_to_exact_points": e32["esc_exact"],
+                       "fp32_to_fp64_per_point": round(e32["esc_fp64"] / n, 6),
+                       "fp32_to_fp64_per_boundary_point": round(e32["esc_fp64"] / max(e32["boundary_points"], 1), 4),
+                       "fp64_to_exact_per_point": e32["esc_exact"] / n,
+                       "fp64_filter_mode_exact_points": esc["fp64_filter"]["esc_exact"]},
+    }
 
 
 if __name__ == "__main__":

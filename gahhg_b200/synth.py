@@ -200,3 +200,87 @@ def write_points(path, pts):
     with open(path, "w") as f:
         for lo, la in pts:
             f.write("%.17g,%.17g\n" % (lo, la))
+
+
+# ---- the benchmark's point sets, generated on the device (torch) --------
+
+def device_points(n, seed, device):
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    u = torch.rand((n, 2), generator=g, device=device, dtype=torch.float64)
+    pts = torch.empty((n, 2), device=device, dtype=torch.float64)
+    pts[:, 0] = u[:, 0] * 360.0 - 180.0
+    pts[:, 1] = torch.rad2deg(torch.asin(u[:, 1] * 2.0 - 1.0))
+    return pts
+
+
+def device_c2_points(rings, n, seed, device):
+    """C2 points on the device: half uniform by area, half on a uniform random
+    edge at a uniform arc parameter, offset along the edge-plane normal by
+    +-10^u rad with u ~ U[-15, -3] (the construction of synth.near_edge_points)."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    ll = torch.as_tensor(np.concatenate(rings), dtype=torch.float64, device=device)
+    starts = np.cumsum([0] + [len(r) for r in rings])
+    nxt = np.arange(len(ll)) + 1
+    for a, b in zip(starts[:-1], starts[1:]):
+        nxt[b - 1] = a
+    nxt = torch.as_tensor(nxt, device=device)
+    lo, la = torch.deg2rad(ll[:, 0]), torch.deg2rad(ll[:, 1])
+    xyz = torch.stack([torch.cos(la) * torch.sin(lo), torch.sin(la), torch.cos(la) * torch.cos(lo)], 1)
+    pts = device_points(n, seed + 1, device)
+    m = n // 2
+    e = torch.randint(0, len(ll), (m,), generator=g, device=device)
+    A, B = xyz[e], xyz[nxt[e]]
+    t = torch.rand((m, 1), generator=g, device=device, dtype=torch.float64)
+    P = (1 - t) * A + t * B
+    P = P / torch.linalg.norm(P, dim=1, keepdim=True)
+    N = torch.linalg.cross(A, B)
+    N = N / torch.clamp(torch.linalg.norm(N, dim=1, keepdim=True), min=1e-300)
+    u = torch.rand(m, generator=g, device=device, dtype=torch.float64) * 12.0 - 15.0
+    sign = torch.where(torch.rand(m, generator=g, device=device) < 0.5, -1.0, 1.0).to(torch.float64)
+    Q = P + (torch.pow(10.0, u) * sign)[:, None] * N
+    Q = Q / torch.linalg.norm(Q, dim=1, keepdim=True)
+    pts[m:, 1] = torch.rad2deg(torch.asin(torch.clamp(Q[:, 1], -1.0, 1.0)))
+    pts[m:, 0] = torch.rad2deg(torch.atan2(Q[:, 0], Q[:, 2]))
+    return pts
+
+
+def device_cap_points(lons, lats, radii_deg, counts, seed, device):
+    """Points uniform by area inside each polygon's cap (1.5 x the bounding
+    radius 1.2 r of a star polygon of radius r), generated on the device."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    counts = np.asarray(counts, dtype=np.int64)
+    n = int(counts.sum())
+    pts = torch.empty((n, 2), dtype=torch.float64, device=device)
+    lon_all = torch.as_tensor(lons, dtype=torch.float64, device=device) * (np.pi / 180)
+    lat_all = torch.as_tensor(lats, dtype=torch.float64, device=device) * (np.pi / 180)
+    R_all = torch.clamp(torch.as_tensor(radii_deg, dtype=torch.float64, device=device) * (1.5 * 1.2 * np.pi / 180),
+                        max=np.pi)
+    starts = np.concatenate([[0], np.cumsum(counts)])
+    p0 = 0
+    while p0 < len(counts):  # polygon ranges of about 32M points keep the temporaries small
+        p1 = p0
+        while p1 < len(counts) and (p1 == p0 or starts[p1 + 1] - starts[p0] <= (1 << 25)):
+            p1 += 1
+        cnt = torch.as_tensor(counts[p0:p1], dtype=torch.int64, device=device)
+        idx = torch.repeat_interleave(torch.arange(p0, p1, device=device), cnt)
+        m = int(starts[p1] - starts[p0])
+        lon0, lat0, R = lon_all[idx], lat_all[idx], R_all[idx]
+        u = torch.rand((m, 2), generator=g, device=device, dtype=torch.float64)
+        c = torch.cos(R) + (1.0 - torch.cos(R)) * u[:, 0]
+        d = torch.arccos(torch.clamp(c, -1.0, 1.0))
+        b = u[:, 1] * 2 * np.pi
+        sl = torch.sin(lat0) * torch.cos(d) + torch.cos(lat0) * torch.sin(d) * torch.cos(b)
+        la2 = torch.asin(torch.clamp(sl, -1.0, 1.0))
+        lo2 = lon0 + torch.atan2(torch.sin(b) * torch.sin(d) * torch.cos(lat0), torch.cos(d) - torch.sin(lat0) * sl)
+        out = pts[starts[p0]:starts[p1]]
+        out[:, 0] = torch.remainder(lo2 * (180 / np.pi) + 180.0, 360.0) - 180.0
+        out[:, 1] = la2 * (180 / np.pi)
+        del idx, lon0, lat0, R, u, c, d, b, sl, la2, lo2
+        p0 = p1
+    return pts

@@ -1,6 +1,9 @@
 """ctypes wrapper of the exact oracle (TEST INFRASTRUCTURE).
 
-See oracle/exact_pip.c for the definitions of the exact labels.
+See oracle/exact_pip.c for the definitions of the exact labels, and
+oracle/brute_gpu.cu for the same brute force run on a GPU (for point sets of
+the benchmark configurations' size; points it cannot decide in FP64 go to
+the CPU brute force).
 """
 import ctypes
 import os
@@ -10,6 +13,7 @@ import numpy as np
 from . import build_oracle
 
 _lib = None
+_brute = None
 
 
 def lib():
@@ -32,8 +36,25 @@ def lib():
         L.oracle_crossing.argtypes = [P, P, P, P]
         L.oracle_canon_query_xyz.argtypes = [P, ctypes.c_long, P]
         L.oracle_canon_vertex_xyz.argtypes = [P, ctypes.c_long, P]
+        L.exact_poly_hub_sides.argtypes = [P, P, ctypes.c_int]
         _lib = L
     return _lib
+
+
+def brute_lib():
+    global _brute
+    if _brute is None:
+        path = build_oracle.BRUTE
+        if not os.path.exists(path):
+            path = build_oracle.build_brute()
+        L = ctypes.CDLL(path)
+        P = ctypes.c_void_p
+        L.brute_gpu_label.restype = ctypes.c_longlong
+        L.brute_gpu_label.argtypes = [P, P, ctypes.c_int, P, P, P, P, ctypes.c_longlong, P, ctypes.c_int]
+        L.brute_host_label.restype = ctypes.c_longlong
+        L.brute_host_label.argtypes = [P, P, ctypes.c_int, P, P, P, P, ctypes.c_longlong, P]
+        _brute = L
+    return _brute
 
 
 def _p(a):
@@ -91,6 +112,44 @@ class ExactPolygon:
         out = np.zeros(len(q), dtype=np.uint8)
         lib().exact_poly_query_xyz(self._h, _p(q), len(q), _p(out), threads)
         return out
+
+    def hub_sides(self, threads=os.cpu_count()):
+        """orient(a_e, b_e, hub_k) for every edge e and hub k, (n, 6) int8."""
+        if getattr(self, "_sides", None) is None:
+            side = np.zeros((len(self.pe), 6), dtype=np.int8)
+            lib().exact_poly_hub_sides(self._h, _p(side), threads)
+            self._sides = side
+        return self._sides
+
+    def query_lonlat_gpu(self, lonlat, device=0, threads=os.cpu_count()):
+        """The same labels as query_lonlat, by the GPU brute force
+        (oracle/brute_gpu.cu); the points it leaves undecided are labelled by
+        the CPU brute force.  Returns (labels, number of undecided points)."""
+        ll = np.ascontiguousarray(np.asarray(lonlat, dtype=np.float64).reshape(-1, 2))
+        out = np.zeros(len(ll), dtype=np.uint8)
+        _x, hubs, hl, _e = self.info()
+        side = self.hub_sides(threads)
+        und = brute_lib().brute_gpu_label(_p(self.xyz), _p(self.pe), len(self.pe), _p(side),
+                                          _p(np.ascontiguousarray(hubs)), _p(hl), _p(ll), len(ll), _p(out),
+                                          device)
+        if und < 0:
+            raise RuntimeError("GPU brute force failed (CUDA error)")
+        if und:
+            idx = np.nonzero(out == 0)[0]
+            out[idx] = self.query_lonlat(ll[idx], threads=threads)
+        return out, int(und)
+
+    def query_lonlat_brute_host(self, lonlat, threads=os.cpu_count()):
+        """The GPU brute force's per-point steps run on the host (one thread):
+        its labels, 0 where it is undecided (a check of its logic without a
+        GPU).  Returns (labels, number of undecided points)."""
+        ll = np.ascontiguousarray(np.asarray(lonlat, dtype=np.float64).reshape(-1, 2))
+        out = np.zeros(len(ll), dtype=np.uint8)
+        _x, hubs, hl, _e = self.info()
+        side = self.hub_sides(threads)
+        und = brute_lib().brute_host_label(_p(self.xyz), _p(self.pe), len(self.pe), _p(side),
+                                           _p(np.ascontiguousarray(hubs)), _p(hl), _p(ll), len(ll), _p(out))
+        return out, int(und)
 
     def arc_parity(self, p, q):
         p = np.ascontiguousarray(p, dtype=np.float64)

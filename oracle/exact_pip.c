@@ -416,3 +416,16 @@ void oracle_canon_vertex_xyz(const double* lonlat, long n, double* xyz)
 {
     for (long i = 0; i < n; i++) gahhg_canon_vertex_xyz(lonlat[2 * i], lonlat[2 * i + 1], xyz + 3 * i);
 }
+
+/* side[6 e + k] = orient(a_e, b_e, hub_k) for every edge (the exact signs
+ * the GPU brute force, oracle/brute_gpu.cu, takes as given). */
+void exact_poly_hub_sides(const void* h, signed char* side, int threads)
+{
+    const exact_poly* P = (const exact_poly*)h;
+#pragma omp parallel for schedule(static) num_threads(threads > 0 ? threads : 1)
+    for (int e = 0; e < P->n; e++) {
+        const double* a = P->pv + 3 * P->pe[2 * e];
+        const double* b = P->pv + 3 * P->pe[2 * e + 1];
+        for (int k = 0; k < 6; k++) side[6 * (long)e + k] = (signed char)oracle_orient(a, b, P->hubs[k]);
+    }
+}

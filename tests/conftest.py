@@ -8,6 +8,22 @@ if REPO not in sys.path:
     sys.path.insert(0, REPO)
 
 
+_REPORT = []
+
+
+def report(line):
+    """A line for the session's closing summary (figures of the parity runs:
+    points checked, escalation counts), so that a quiet run shows them."""
+    _REPORT.append(line)
+
+
+def pytest_terminal_summary(terminalreporter, exitstatus, config):
+    if _REPORT:
+        terminalreporter.write_sep("-", "parity figures")
+        for line in _REPORT:
+            terminalreporter.write_line(line)
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (runs on the B200 box)")
     config.addinivalue_line("markers", "slow: long-running")
