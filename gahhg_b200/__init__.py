@@ -328,6 +328,20 @@ def staging_fallbacks(device=0):
     return int(v.value)
 
 
+KNOB_GROUPED_PASS2 = 1
+
+
+def set_knob(knob, value):
+    """Process-wide tuning/test knob (gahhg_set_knob); returns the old value."""
+    old = get_knob(knob)
+    check(_lib.lib().gahhg_set_knob(int(knob), int(value)))
+    return old
+
+
+def get_knob(knob):
+    return int(_lib.lib().gahhg_get_knob(int(knob)))
+
+
 def grid0():
     V = np.zeros((80, 3), dtype=np.float64)
     B = np.zeros(240, dtype=BORDER_DTYPE)

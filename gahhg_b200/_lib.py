@@ -110,6 +110,8 @@ _SIGS = {
     "gahhg_last_error": (ctypes.c_char_p, []),
     "gahhg_abi_version": (ctypes.c_int, []),
     "gahhg_staging_fallbacks": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong)]),
+    "gahhg_set_knob": (ctypes.c_int, [ctypes.c_int, ctypes.c_longlong]),
+    "gahhg_get_knob": (ctypes.c_longlong, [ctypes.c_int]),
     "gahhg_polygon_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_P)]),
     "gahhg_polygon_from_rings": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.POINTER(_P)]),
     "gahhg_polygon_num_edges": (ctypes.c_int, [_P]),

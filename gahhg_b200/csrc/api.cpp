@@ -1,4 +1,5 @@
 // api.cpp - the C ABI (include/gahhg.h) over the host objects.
+#include <atomic>
 #include <chrono>
 #include <cstdarg>
 #include <cstdio>
@@ -175,6 +176,14 @@ static void fill_stats(Grid* g)
     s.lattice_bytes = (long long)lattice_bytes(g->lattice);
 }
 
+// process-wide knobs (gahhg_set_knob)
+namespace {
+constexpr int KNOB_COUNT = 8;
+std::atomic<long long> g_knobs[KNOB_COUNT] = {0, 1, 0, 0, 0, 0, 0, 0};  // index = gahhg_knob
+}  // namespace
+
+long long knob(int k) { return (k > 0 && k < KNOB_COUNT) ? g_knobs[k].load(std::memory_order_relaxed) : 0; }
+
 }  // namespace gahhg
 
 using namespace gahhg;
@@ -196,6 +205,22 @@ void gahhg_build_opts_init(gahhg_build_opts* o)
 
 const char* gahhg_last_error(void) { return last_error(); }
 int gahhg_abi_version(void) { return GAHHG_ABI_VERSION; }
+
+gahhg_status gahhg_set_knob(int k, long long value)
+{
+    if (k != GAHHG_KNOB_GROUPED_PASS2) {
+        set_error("unknown knob %d", k);
+        return GAHHG_ERR_ARG;
+    }
+    if (value != 0 && value != 1) {
+        set_error("knob %d takes 0 or 1, not %lld", k, value);
+        return GAHHG_ERR_ARG;
+    }
+    gahhg::g_knobs[k].store(value, std::memory_order_relaxed);
+    return GAHHG_OK;
+}
+
+long long gahhg_get_knob(int k) { return gahhg::knob(k); }
 
 gahhg_status gahhg_staging_fallbacks(int device, unsigned long long* count)
 {

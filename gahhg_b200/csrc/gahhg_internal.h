@@ -13,6 +13,10 @@
 
 namespace gahhg {
 
+// ----------------------------------------------------------------- knobs --
+// Current value of a gahhg_knob (process-wide, set by gahhg_set_knob).
+long long knob(int k);
+
 // ---------------------------------------------------------------- errors --
 void set_error(const char* fmt, ...);
 const char* last_error();

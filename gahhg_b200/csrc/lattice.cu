@@ -804,7 +804,14 @@ struct QueryView {
     const double2* ends;      // per edge: A.xy, A.z B.x, B.yz (48 B, one aligned load each)
     const D3* pv;
     const int* pe;
+    int nleaves;              // leaves of the index (buckets of 2^GROUP_SHIFT for the grouped pass 2)
+    int nbuckets;             // ceil(nleaves / 2^GROUP_SHIFT)
 };
+
+// Pass 2 groups the queued points by bucket of 2^GROUP_SHIFT consecutive
+// leaves: their records are contiguous in memory, so one bulk copy stages
+// every edge record a bucket's points test.
+constexpr int GROUP_SHIFT = 6;
 
 struct PointCtx {
     double lon, lat;      // input longitude and FakeLL latitude (canonical XYZ)
@@ -1602,13 +1609,425 @@ __global__ void __launch_bounds__(TPB) k_leaf_t3(VS vs, const double2* __restric
     if (ctr) count_inside(inside, ctr + 3);
 }
 
+// ------------------------------------------ pass 2 grouped by leaf bucket --
+//
+// One persistent launch (k_group) replaces the per-point tiers 1 and 2 for a
+// single polygon.  Its blocks take work items in order from a counter:
+//   count items    pass-1 queue entries counted per bucket of 2^GROUP_SHIFT
+//                  consecutive leaves;
+//   scan items     after every count item finished: exclusive scan of the
+//                  bucket counts (decoupled look-back between the items);
+//   scatter items  the pass-1 queue scattered into bucket order (after every
+//                  scan item finished);
+//   bucket items   after every scatter item finished: the bucket's leaf
+//                  records and FP32 edge records (contiguous: leaves and their
+//                  records are stored in leaf order) are staged in shared
+//                  memory by one bulk copy (TMA), every point of the bucket runs
+//                  the FP32 tier against them, and the points it defers run the
+//                  FP64 tier against the bucket's edge ids and FP64 ends,
+//                  gathered into shared memory once per bucket.  Points the FP64
+//                  tier defers go to the tier-3 queue.
+// A block waits only on items that blocks which started before it hold (items
+// are taken in order), and every wait is bounded: a wait that runs out marks
+// the pass failed, the remaining buckets are skipped, and the tier-3 launch
+// sweeps every queued point still unlabelled.  Sparse buckets (fewer than
+// G_STAGE_MIN points) and buckets with more records than fit read the
+// records from global memory instead.
+constexpr int G_TPB = 128;
+constexpr int G_RECS = 1024;              // FP32 records staged per bucket (16 KB)
+constexpr int G_ENDS = 448;               // records whose FP64 ends are staged (21 KB)
+constexpr int G_ROUND = 512;              // bucket entries per round of the FP32 tier
+constexpr int G_SCAN = G_TPB * 8;         // buckets per scan item
+constexpr int G_SCATTER = G_TPB * 16;     // queue entries per scatter item
+constexpr int G_STAGE_MIN = 8;
+constexpr int G_WAIT_LIMIT = 1 << 22;     // polls (about 0.5 s) before a wait gives up
+constexpr int G_BLOCKS_PER_SM = 4;
+
+struct GroupScratch {
+    unsigned int* hist;           // [nb + 1] queued points per bucket (bucket nb: no leaf word); zero
+    unsigned long long* status;   // [nscan] scan look-back words (value | flag << 32); zero
+    unsigned int* boff;           // [nb + 2] bucket offsets in `sorted`
+    uint2* sorted;                // {point, leaf word} per queued point, in bucket order
+    unsigned int* sync;           // [0] next item, [1] count, [2] scan, [3] scatter items done, [4] failed; zero
+    int nb;
+};
+
+__host__ __device__ inline int group_scan_items(int nb) { return (nb + 1 + G_SCAN - 1) / G_SCAN; }
+
+// Thread-0 helpers of k_group.
+__device__ __forceinline__ bool wait_count(const unsigned int* p, unsigned int target)
+{
+    for (int i = 0; i < G_WAIT_LIMIT; i++) {
+        if (*(const volatile unsigned int*)p >= target) {
+            __threadfence();
+            return true;
+        }
+        __nanosleep(128);
+    }
+    return false;
+}
+
+__device__ __forceinline__ uint32_t group_bucket(uint32_t w, int nb)
+{
+    return (w & KIND_MASK) == KIND_LEAF ? min((w & INDEX_MASK) >> GROUP_SHIFT, (uint32_t)nb) : (uint32_t)nb;
+}
+
+__device__ __forceinline__ void group_fail(const GroupScratch& S, const Tiers& T)
+{
+    atomicExch(S.sync + 4, 1u);
+    *(volatile unsigned int*)(T.cnt + 2) = 1u;  // tier 3 sweeps the unlabelled queued points
+}
+
+// FP32 tier on records rec[0 .. L.cnt) (shared or global memory).
+__device__ __forceinline__ uint8_t fp32_records(const LeafRec& L, const float4* rec, const PointCtx& P)
+{
+    local_frame::Offset o;
+    if (!(fabs(P.lon) <= 540.0) || !local_frame::offset(P.lon, P.lat, L.lon, L.lat, o)) return LABEL_DEFER;
+    local_frame::Frame f;
+    local_frame::project(o, f);
+    int par = 0;
+    for (int k = 0; k < L.cnt; k++) {
+        // stored order: orient(A, B, R) = +1, so a crossing needs s2 = -1,
+        // s3 = orient(R, q, A) = -1 and s4 = orient(R, q, B) = +1
+        const float4 r = rec[k];
+        const int s2 = local_frame::sign_edge(f, r.x, r.y, r.z, r.w);
+        if (s2 == 0) return LABEL_DEFER;
+        if (s2 > 0) continue;
+        const int s3 = local_frame::sign_end(f, r.x, r.y);
+        if (s3 == 0) return LABEL_DEFER;
+        if (s3 > 0) continue;
+        const int s4 = local_frame::sign_end(f, r.z, r.w);
+        if (s4 == 0) return LABEL_DEFER;
+        if (s4 > 0) par ^= 1;
+    }
+    return (uint8_t)(par ? 3 - L.label : L.label);
+}
+
+// FP64 tier with the leaf's edge ids eid[0 .. L.cnt) and, when `rec_ends` is
+// set, the records' FP64 ends rec_ends[3k .. 3k + 2] (else from the per-edge
+// table).
+__device__ __forceinline__ uint8_t fp64_records(const QueryView& Q, const LeafRec& L, const uint32_t* eid,
+                                                const double2* rec_ends, PointCtx& P)
+{
+    P.need64();
+    double LR[3];
+    gahhg_canon_vertex_xyz(L.lon, L.lat, LR);
+    int par = 0;
+    for (int k = 0; k < L.cnt; k++) {
+        const uint32_t es = eid[k];
+        double2 e0, e1, e2;
+        if (rec_ends) {
+            e0 = rec_ends[3 * k];
+            e1 = rec_ends[3 * k + 1];
+            e2 = rec_ends[3 * k + 2];
+        } else {
+            const double2* p = Q.ends + 3 * (size_t)(es & 0x7fffffffu);
+            e0 = __ldg(p);
+            e1 = __ldg(p + 1);
+            e2 = __ldg(p + 2);
+        }
+        const int s1 = (es >> 31) ? 1 : -1;
+        const double A[3] = {e0.x, e0.y, e1.x}, B[3] = {e1.y, e2.x, e2.y};
+        if (exact::same(P.q, A) || exact::same(P.q, B)) return CELL_IN;  // vertex rule
+        if (exact::same(P.q, LR)) return L.label;                       // q is the center
+        const int s2 = exact::orient_fp64_near(A, B, P.q);
+        if (s2 == 0) return LABEL_DEFER;
+        if (s2 == s1) continue;
+        const int s3 = exact::orient_fp64_near(LR, P.q, A);
+        if (s3 == 0) return LABEL_DEFER;
+        if (s3 != s2) continue;
+        const int s4 = exact::orient_fp64_near(LR, P.q, B);
+        if (s4 == 0) return LABEL_DEFER;
+        if (s4 == -s2) par ^= 1;
+    }
+    return (uint8_t)(par ? 3 - L.label : L.label);
+}
+
+template <bool FP32, bool STATS>
+__global__ void __launch_bounds__(G_TPB, G_BLOCKS_PER_SM)
+    k_group(QueryView Q, const double2* __restrict__ ll, uint8_t* __restrict__ out,
+            const uint32_t* __restrict__ queue, const uint32_t* __restrict__ l1,
+            const unsigned int* __restrict__ qcount, GroupScratch S, Tiers T, unsigned long long* ctr)
+{
+    __shared__ __align__(16) LeafRec s_leaf[1 << GROUP_SHIFT];
+    __shared__ __align__(16) float4 s_rec[G_RECS];
+    __shared__ __align__(16) uint32_t s_eid[G_ENDS];
+    __shared__ __align__(16) double2 s_end[3 * G_ENDS];
+    __shared__ unsigned short s_def[G_ROUND];
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ unsigned int s_warp[G_TPB / 32];
+    __shared__ unsigned int s_prefix;
+    __shared__ int s_item, s_ok, s_ndef, s_late;
+    wait_for_predecessor();
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned int m = *qcount;
+    const int nb = S.nb;
+    const int nscan = group_scan_items(nb);
+    const int nsc = (int)((m + G_SCATTER - 1) / G_SCATTER);
+    const long long nitems = m ? (long long)2 * nsc + nscan + nb + 1 : 0;
+    if (tid == 0) {
+        s_late = 0;
+        mbar_init(&s_bar);
+    }
+    uint32_t phase = 0;
+    bool pending = false;  // a bulk copy whose wait ran out may still be in flight
+    int inside = 0, boundary = 0, fp64 = 0, exact = 0;
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s_item = (int)atomicAdd(S.sync + 0, 1u);
+        __syncthreads();
+        const long long item = s_item;
+        if (item >= nitems) break;
+        if (item < nsc) {
+            // ---- count item: entries per bucket
+            const unsigned int c = (unsigned int)item;
+            const unsigned int e1 = min(m, (c + 1) * (unsigned int)G_SCATTER);
+            for (unsigned int t = c * G_SCATTER + tid; t < e1; t += G_TPB) atomicAdd(S.hist + group_bucket(l1[t], nb), 1u);
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) atomicAdd(S.sync + 1, 1u);
+        } else if (item < nsc + nscan) {
+            // ---- scan item: buckets [t * G_SCAN, ...) of hist[0 .. nb]
+            const int t = (int)(item - nsc);
+            if (tid == 0) {
+                const bool ok = wait_count(S.sync + 1, (unsigned int)nsc);
+                if (!ok) group_fail(S, T);
+            }
+            __syncthreads();
+            const int base = t * G_SCAN + tid * 8;
+            unsigned int v[8], sum = 0;
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                v[k] = base + k <= nb ? __ldcg(S.hist + base + k) : 0u;
+                sum += v[k];
+            }
+            unsigned int incl = sum;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const unsigned int y = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= d) incl += y;
+            }
+            if (lane == 31) s_warp[warp] = incl;
+            __syncthreads();
+            if (tid == 0) {
+                unsigned int run = 0;
+                for (int w = 0; w < G_TPB / 32; w++) {
+                    const unsigned int x = s_warp[w];
+                    s_warp[w] = run;
+                    run += x;
+                }
+                // run = the item's total; publish it, then look back
+                unsigned int excl = 0;
+                const unsigned long long AGG = 1ull << 32, PRE = 2ull << 32;
+                if (t == 0) {
+                    atomicExch(S.status, PRE | run);
+                } else {
+                    atomicExch(S.status + t, AGG | run);
+                    bool ok = true;
+                    for (int j = t - 1; j >= 0;) {
+                        int spins = 0;
+                        unsigned long long w;
+                        while (((w = *(const volatile unsigned long long*)(S.status + j)) >> 32) == 0ull) {
+                            if (++spins > G_WAIT_LIMIT) break;
+                            __nanosleep(64);
+                        }
+                        if ((w >> 32) == 0ull) {
+                            ok = false;
+                            break;
+                        }
+                        excl += (unsigned int)w;
+                        if ((w >> 32) == 2ull) break;
+                        j--;
+                    }
+                    if (!ok) group_fail(S, T);
+                    atomicExch(S.status + t, PRE | (excl + run));
+                }
+                s_prefix = excl;
+                if (t == nscan - 1) S.boff[nb + 1] = excl + run;  // the total
+            }
+            __syncthreads();
+            unsigned int run = s_prefix + s_warp[warp] + incl - sum;
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                if (base + k <= nb) S.boff[base + k] = run;
+                run += v[k];
+            }
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) atomicAdd(S.sync + 2, 1u);
+        } else if (item < 2 * nsc + nscan) {
+            // ---- scatter item: pass-1 queue entries into bucket order
+            if (tid == 0) {
+                const bool ok = wait_count(S.sync + 2, (unsigned int)nscan);
+                if (!ok) group_fail(S, T);
+                s_ok = ok && *(volatile unsigned int*)(S.sync + 4) == 0u;
+            }
+            __syncthreads();
+            if (s_ok) {
+                const unsigned int c = (unsigned int)(item - nsc - nscan);
+                const unsigned int e1 = min(m, (c + 1) * (unsigned int)G_SCATTER);
+                bool bad = false;
+                for (unsigned int t = c * G_SCATTER + tid; t < e1; t += G_TPB) {
+                    const uint32_t w = l1[t];
+                    const uint32_t b = group_bucket(w, nb);
+                    const unsigned int lo = __ldcg(S.boff + b), hi = __ldcg(S.boff + b + 1);
+                    const unsigned int r = atomicSub(S.hist + b, 1u);
+                    if (r == 0u || lo + r - 1u >= hi || hi > m) {
+                        bad = true;  // counts and entries disagree: never write out of the bucket
+                        continue;
+                    }
+                    S.sorted[lo + r - 1u] = make_uint2(queue[t], w);
+                }
+                if (__syncthreads_or(bad) && tid == 0) group_fail(S, T);
+            }
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) atomicAdd(S.sync + 3, 1u);
+        } else {
+            // ---- bucket item
+            const int b = (int)(item - 2 * nsc - nscan);
+            if (tid == 0) {
+                const bool ok = wait_count(S.sync + 3, (unsigned int)nsc);
+                if (!ok) group_fail(S, T);
+                s_ok = ok && *(volatile unsigned int*)(S.sync + 4) == 0u;
+            }
+            __syncthreads();
+            if (!s_ok) continue;
+            const unsigned int e0 = __ldcg(S.boff + b), E = __ldcg(S.boff + b + 1) - e0;
+            if (E == 0u) continue;
+            if (e0 > m || E > m - e0) {  // offsets beyond the queue: never expected
+                if (tid == 0) group_fail(S, T);
+                continue;
+            }
+            if (b == nb) {
+                // points without a leaf word: the complete test of tier 3
+                for (unsigned int j = tid; j < E; j += G_TPB) {
+                    const uint2 en = __ldcg(S.sorted + e0 + j);
+                    if (!push_deferred(en.x, en.y, T.q3, T.l3, T.cnt + 1, T.cap3)) T.cnt[2] = 1;
+                }
+                continue;
+            }
+            const int l0 = b << GROUP_SHIFT;
+            const int nl = min(1 << GROUP_SHIFT, Q.nleaves - l0);
+            const LeafRec lf = Q.leaves[l0], lz = Q.leaves[l0 + nl - 1];
+            const uint32_t rec0 = lf.off;
+            const uint32_t nrec = lz.off + lz.cnt - rec0;
+            const bool stage = !s_late && E >= (unsigned int)G_STAGE_MIN && nrec <= (uint32_t)G_RECS;
+            if (stage) {
+                if (tid == 0) {
+                    // leaf records in 16-byte units (the leaf array keeps a spare
+                    // record at its end), edge records exactly; both 16-byte aligned
+                    const uint32_t bl = ((uint32_t)nl * (uint32_t)sizeof(LeafRec) + 15u) & ~15u;
+                    const uint32_t br = nrec * (uint32_t)sizeof(float4);
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&s_bar)),
+                                 "r"(bl + br)
+                                 : "memory");
+                    asm volatile(
+                        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                            smem_u32(s_leaf)),
+                        "l"(Q.leaves + l0), "r"(bl), "r"(smem_u32(&s_bar))
+                        : "memory");
+                    if (br)
+                        asm volatile(
+                            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                                smem_u32(s_rec)),
+                            "l"(Q.recs + rec0), "r"(br), "r"(smem_u32(&s_bar))
+                            : "memory");
+                }
+                if (!mbar_wait(&s_bar, phase)) s_late = 1;
+                phase ^= 1u;
+                __syncthreads();
+            }
+            // a copy that ran out of time may still write s_leaf / s_rec: from then
+            // on this block reads global memory only (and waits for the copy at exit)
+            const bool late = s_late != 0;
+            const bool staged = stage && !late;
+            if (stage && late) pending = true;
+            bool ends_ready = false;
+            for (unsigned int r0 = 0; r0 < E; r0 += G_ROUND) {
+                const unsigned int r1 = min(E, r0 + (unsigned int)G_ROUND);
+                if (tid == 0) s_ndef = 0;
+                __syncthreads();
+                for (unsigned int j = r0 + tid; j < r1; j += G_TPB) {
+                    const uint2 en = __ldcg(S.sorted + e0 + j);
+                    const uint32_t leaf = en.y & INDEX_MASK;
+                    const int li = (int)leaf - l0;
+                    if (li < 0 || li >= nl) {  // not this bucket's leaf: never expected
+                        if (!push_deferred(en.x, en.y, T.q3, T.l3, T.cnt + 1, T.cap3)) T.cnt[2] = 1;
+                        continue;
+                    }
+                    boundary++;
+                    uint8_t lab = LABEL_DEFER;
+                    if (FP32) {
+                        PointCtx P;
+                        point_leaf(Q, ll[en.x], P, en.y);
+                        const LeafRec L = staged ? s_leaf[li] : Q.leaves[leaf];
+                        lab = fp32_records(L, staged ? s_rec + (L.off - rec0) : Q.recs + L.off, P);
+                    }
+                    if (lab == LABEL_DEFER) {
+                        if (FP32) fp64++;
+                        s_def[atomicAdd(&s_ndef, 1)] = (unsigned short)(j - r0);
+                    } else {
+                        out[en.x] = lab;
+                        inside += lab == CELL_IN;
+                    }
+                }
+                __syncthreads();
+                const int nd = s_ndef;
+                if (nd == 0) continue;
+                // the bucket's edge ids and FP64 ends, gathered once per bucket when
+                // its deferred points will read them often enough
+                const bool ends_staged = nrec <= (uint32_t)G_ENDS && (ends_ready || (uint32_t)nd * 4u >= nrec);
+                if (ends_staged && !ends_ready) {
+                    for (uint32_t k = tid; k < nrec; k += G_TPB) {
+                        const uint32_t es = __ldg(Q.eids + rec0 + k);
+                        s_eid[k] = es;
+                        const double2* p = Q.ends + 3 * (size_t)(es & 0x7fffffffu);
+                        s_end[3 * k] = __ldg(p);
+                        s_end[3 * k + 1] = __ldg(p + 1);
+                        s_end[3 * k + 2] = __ldg(p + 2);
+                    }
+                    ends_ready = true;
+                    __syncthreads();
+                }
+                for (int d = tid; d < nd; d += G_TPB) {
+                    const uint2 en = __ldcg(S.sorted + e0 + r0 + s_def[d]);
+                    const uint32_t leaf = en.y & INDEX_MASK;
+                    PointCtx P;
+                    point_leaf(Q, ll[en.x], P, en.y);
+                    const LeafRec L = staged ? s_leaf[leaf - l0] : Q.leaves[leaf];
+                    const uint8_t lab =
+                        ends_staged ? fp64_records(Q, L, s_eid + (L.off - rec0), s_end + 3 * (L.off - rec0), P)
+                                    : fp64_records(Q, L, Q.eids + L.off, nullptr, P);
+                    if (lab == LABEL_DEFER) {
+                        exact++;
+                        if (!push_deferred(en.x, en.y, T.q3, T.l3, T.cnt + 1, T.cap3)) T.cnt[2] = 1;
+                    } else {
+                        out[en.x] = lab;
+                        inside += lab == CELL_IN;
+                    }
+                }
+                __syncthreads();
+            }
+        }
+    }
+    if (pending) {
+        // the copy in flight ends before the block does (bounded)
+        if (tid == 0) atomicAdd(&g_tma_timeouts, 1u);
+        mbar_wait(&s_bar, phase ^ 1u);
+    }
+    allow_dependents();
+    if (STATS && ctr) count_stats(ctr, inside, boundary, fp64, exact);
+}
+
 // Launch with programmatic stream serialization (see wait_for_predecessor).
 template <typename... KArgs, typename... Args>
-void launch_dependent(void (*kernel)(KArgs...), int grid, cudaStream_t s, Args... args)
+void launch_dependent_tpb(void (*kernel)(KArgs...), int grid, int tpb, cudaStream_t s, Args... args)
 {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(TPB);
+    cfg.blockDim = dim3(tpb);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
@@ -1617,6 +2036,12 @@ void launch_dependent(void (*kernel)(KArgs...), int grid, cudaStream_t s, Args..
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+template <typename... KArgs, typename... Args>
+void launch_dependent(void (*kernel)(KArgs...), int grid, cudaStream_t s, Args... args)
+{
+    launch_dependent_tpb(kernel, grid, TPB, s, args...);
 }
 
 // Tier counters (T.cnt[0..2]) must be zero.
@@ -2264,7 +2689,8 @@ gahhg_status lattice_build(Grid* g)
         set_error("exact index: too many edge records");
         return GAHHG_ERR_CAPACITY;
     }
-    GAHHG_TRY(L->leaves.reserve(std::max(leaf_total, 1LL), s, false));
+    // one spare leaf: the grouped pass 2 copies leaf records in 16-byte units
+    GAHHG_TRY(L->leaves.reserve(leaf_total + 1, s, false));
     GAHHG_TRY(L->recs.reserve(std::max(rec_total, 1LL), s, false));
     GAHHG_TRY(L->eids.reserve(std::max(rec_total, 1LL), s, false));
     GAHHG_TRY(L->ends.reserve(3 * (size_t)std::max(n, 1), s, false));
@@ -2320,7 +2746,8 @@ gahhg_status lattice_build(Grid* g)
 
 gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long long n, uint8_t* d_labels,
                                 int precision, cudaStream_t s, uint64_t* d_counters, uint32_t* queue,
-                                unsigned int* qcount, long long chunk, int device, const Tiers* tiers);
+                                unsigned int* qcount, long long chunk, int device, const Tiers* tiers,
+                                const GroupScratch* grp = nullptr);
 
 QueryView make_view(const Grid* g)
 {
@@ -2350,6 +2777,8 @@ QueryView make_view(const Grid* g)
     Q.CW = (L->geo.W + (1 << L->cshift) - 1) >> L->cshift;
     Q.swords = L->swords;
     Q.summary = L->summary.ptr;
+    Q.nleaves = (int)L->nleaves;
+    Q.nbuckets = (int)((L->nleaves + (1 << GROUP_SHIFT) - 1) >> GROUP_SHIFT);
     return Q;
 }
 
@@ -2362,25 +2791,45 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
     if (n == 0) return GAHHG_OK;
     const QueryView Q = make_view(g);
     const long long chunk = std::min<long long>((long long)n, QUERY_CHUNK);
-    // [pass-2 queue][counters: queue fill, tier-2 fill, tier-3 fill, overflow]
-    // [pass-2 leaf words][tier-2 queue][its leaf words][tier-3 queue][its leaf words]
+    // Words: [pass-2 queue: chunk][control: 64 (queue fill at +32, tier counters
+    // at +33..35, k_group's sync words at +36..40)][bucket counts: nb + 1]
+    // [pad to 8 bytes][scan look-back words: 2 per scan item][bucket offsets:
+    // nb + 2][pass-2 leaf words: chunk][tier-2 queue][its leaf words][tier-3
+    // queue][its leaf words][pad][bucket-ordered entries: 2 per queued point].
+    // One memset per pass clears the control words, counts and look-back words.
     unsigned int cap2 = 0, cap3 = 0;
     tier_caps(chunk, &cap2, &cap3);
+    const bool grouped = knob(GAHHG_KNOB_GROUPED_PASS2) != 0 && Q.nbuckets > 0;
+    const size_t nb = grouped ? (size_t)Q.nbuckets : 0;
+    const size_t nscan = grouped ? (size_t)group_scan_items((int)nb) : 0;
+    const size_t hist_at = (size_t)chunk + 64;
+    const size_t status_at = (hist_at + (grouped ? nb + 1 : 0) + 1) & ~(size_t)1;
+    const size_t boff_at = status_at + 2 * nscan;
+    const size_t l1_at = boff_at + (grouped ? nb + 2 : 0);
+    const size_t tiers_end = l1_at + (size_t)chunk + 2 * ((size_t)cap2 + cap3);
+    const size_t sorted_at = (tiers_end + 1) & ~(size_t)1;
+    const size_t words = sorted_at + (grouped ? 2 * (size_t)chunk : 0);
     uint32_t* queue = nullptr;
-    GAHHG_TRY(pool_alloc((void**)&queue, sizeof(uint32_t) * (2 * (size_t)chunk + 64 + 2 * ((size_t)cap2 + cap3)),
-                         g->device, s));
+    GAHHG_TRY(pool_alloc((void**)&queue, sizeof(uint32_t) * words, g->device, s));
     unsigned int* qcount = (unsigned int*)(queue + chunk + 32);
     Tiers T;
     T.cnt = qcount + 1;
-    T.l1 = queue + chunk + 64;
+    T.l1 = queue + l1_at;
     T.q2 = T.l1 + chunk;
     T.l2 = T.q2 + cap2;
     T.q3 = T.l2 + cap2;
     T.l3 = T.q3 + cap3;
     T.cap2 = cap2;
     T.cap3 = cap3;
+    GroupScratch G;
+    G.sync = qcount + 4;
+    G.hist = queue + hist_at;
+    G.status = (unsigned long long*)(queue + status_at);
+    G.boff = queue + boff_at;
+    G.sorted = (uint2*)(queue + sorted_at);
+    G.nb = (int)nb;
     const gahhg_status st = lattice_query_with(Q, d_lonlat, (long long)n, d_labels, precision, s, d_counters,
-                                               queue, qcount, chunk, g->device, &T);
+                                               queue, qcount, chunk, g->device, &T, grouped ? &G : nullptr);
     cudaFreeAsync(queue, s);
     return st;
 }
@@ -2389,7 +2838,8 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
 // beyond the pass-2 queue); else qcount[1..3] are the tier counters.
 gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long long n, uint8_t* d_labels,
                                 int precision, cudaStream_t s, uint64_t* d_counters, uint32_t* queue,
-                                unsigned int* qcount, long long chunk, int device, const Tiers* tiers)
+                                unsigned int* qcount, long long chunk, int device, const Tiers* tiers,
+                                const GroupScratch* grp)
 {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -2397,7 +2847,13 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
     for (long long off = 0; off < n; off += chunk) {
         const int m = (int)std::min<long long>(chunk, n - off);
         const double2* ll = (const double2*)d_lonlat + off;
-        GAHHG_CUDA_TRY(cudaMemsetAsync(qcount, 0, sizeof(unsigned int) * (tiers ? 4 : 1), s));
+        // the queue fill, the tier counters and, when grouping, k_group's sync
+        // words, the bucket counts and the look-back words (laid out after them;
+        // the control words run to the counts)
+        const size_t zero_words =
+            grp ? (size_t)((const unsigned int*)(grp->status + group_scan_items(grp->nb)) - qcount)
+                : (tiers ? 4 : 1);
+        GAHHG_CUDA_TRY(cudaMemsetAsync(qcount, 0, sizeof(unsigned int) * zero_words, s));
         const long long tiles = ((long long)m + TPB * LOC_UNROLL - 1) / (TPB * LOC_UNROLL);
         const int grid = (int)std::min<long long>(tiles, (long long)sms * 8);
         uint32_t* leafq = tiers ? tiers->l1 : nullptr;
@@ -2407,7 +2863,27 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
         else
             k_locate<false><<<grid, TPB, summary_bytes(Q.swords), s>>>(ll, m, d_labels + off, Q, queue, leafq,
                                                                        qcount, ctr);
-        if (tiers)
+        if (tiers && grp) {
+            // pass 2 grouped by leaf bucket (tiers 1 and 2), then tier 3
+            const int gg = sms * G_BLOCKS_PER_SM;
+            const bool fp32 = precision != GAHHG_QUERY_FP64_FILTER;
+            const uint32_t* cq = queue;
+            const uint32_t* cl1 = tiers->l1;
+            const unsigned int* cqc = qcount;
+            if (fp32 && ctr)
+                launch_dependent_tpb(k_group<true, true>, gg, G_TPB, s, Q, ll, d_labels + off, cq, cl1, cqc, *grp,
+                                     *tiers, ctr);
+            else if (fp32)
+                launch_dependent_tpb(k_group<true, false>, gg, G_TPB, s, Q, ll, d_labels + off, cq, cl1, cqc, *grp,
+                                     *tiers, ctr);
+            else if (ctr)
+                launch_dependent_tpb(k_group<false, true>, gg, G_TPB, s, Q, ll, d_labels + off, cq, cl1, cqc, *grp,
+                                     *tiers, ctr);
+            else
+                launch_dependent_tpb(k_group<false, false>, gg, G_TPB, s, Q, ll, d_labels + off, cq, cl1, cqc, *grp,
+                                     *tiers, ctr);
+            launch_dependent(k_leaf_t3<OneView>, sms * 2, s, OneView{Q}, ll, d_labels + off, cq, cqc, *tiers, ctr);
+        } else if (tiers)
             leaf_tiers_launch(OneView{Q}, ll, d_labels + off, queue, qcount, *tiers, precision, ctr, sms, s);
         else if (precision == GAHHG_QUERY_FP64_FILTER)
             k_leaf<false><<<sms * 4, TPB, 0, s>>>(ll, d_labels + off, Q, queue, qcount, ctr);

@@ -342,6 +342,17 @@ gahhg_status gahhg_grid0_export(double* v, void* b, void* c);
  * instead, so labels are unaffected; 0 in normal operation. */
 gahhg_status gahhg_staging_fallbacks(int device, unsigned long long* count);
 
+/* Process-wide tuning and test knobs.  No counterpart in the reference.
+ * GAHHG_KNOB_GROUPED_PASS2: 1 (default) runs pass 2 of single-polygon exact
+ * queries grouped by leaf bucket (edge records staged in shared memory once
+ * per bucket); 0 runs the per-point tiers (for A/B measurements).  Values take
+ * effect for work enqueued after the call. */
+typedef enum {
+    GAHHG_KNOB_GROUPED_PASS2 = 1
+} gahhg_knob;
+gahhg_status gahhg_set_knob(int knob, long long value);
+long long gahhg_get_knob(int knob);
+
 const char* gahhg_last_error(void);
 int gahhg_abi_version(void);
 
