@@ -525,6 +525,7 @@ def main():
     ap.add_argument("--c4-headroom", type=float, default=8.0, help="GB of budget above the resident set")
     ap.add_argument("--c4-trace", default=None, help="save the per-batch trace and latencies (.npz)")
     ap.add_argument("--no-legs", action="store_true", help="C1 only (no C2/C3/C4 keys in the default run)")
+    ap.add_argument("--legs", default="c2,c3,c4", help="configurations added as keys of the C1 line")
     ap.add_argument("--leg-c3-polygons", type=int, default=1024)
     ap.add_argument("--leg-tune-budget", type=float, default=15.0)
     ap.add_argument("--leg-c4-seconds", type=float, default=10.0)
@@ -726,14 +727,19 @@ def main():
         # serving run on the same 1,024 batch-configuration polygons
         del pts, labels, host_ll, host_lab
         torch.cuda.empty_cache()
-        out["c2"] = leg_c2(args, g, gref, rings, stream)
+        legs = set(args.legs.split(","))
+        if "c2" in legs:
+            out["c2"] = leg_c2(args, g, gref, rings, stream)
         del g, gref
         torch.cuda.empty_cache()
-        out["c3"], polys = run_c3(args, count=args.leg_c3_polygons, tune_budget=args.leg_tune_budget,
-                                  steps=max(3, args.steps // 4))
-        torch.cuda.empty_cache()
-        out["c4"] = run_c4(args, polys=polys, seconds=args.leg_c4_seconds, pool_n=args.leg_c4_pool,
-                           tune_budget=args.leg_tune_budget)
+        polys = None
+        if "c3" in legs:
+            out["c3"], polys = run_c3(args, count=args.leg_c3_polygons, tune_budget=args.leg_tune_budget,
+                                      steps=max(3, args.steps // 4))
+            torch.cuda.empty_cache()
+        if "c4" in legs:
+            out["c4"] = run_c4(args, polys=polys, seconds=args.leg_c4_seconds, pool_n=args.leg_c4_pool,
+                               tune_budget=args.leg_tune_budget)
     print(json.dumps(out))
     return 0
 

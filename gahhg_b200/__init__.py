@@ -329,6 +329,9 @@ def staging_fallbacks(device=0):
 
 
 KNOB_GROUPED_PASS2 = 1
+KNOB_WALK_STEP_LIMIT = 2
+KNOB_SCAN_SPIN_LIMIT = 3
+KNOB_STAGING_POLL_LIMIT = 4
 
 
 def set_knob(knob, value):

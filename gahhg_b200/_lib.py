@@ -55,7 +55,7 @@ class Stats(ctypes.Structure):
                 ("query_s", ctypes.c_double), ("query_points", ctypes.c_longlong),
                 ("in_count", ctypes.c_longlong), ("esc_fp64", ctypes.c_longlong),
                 ("esc_exact", ctypes.c_longlong), ("boundary_points", ctypes.c_longlong),
-                ("walk_limit_hits", ctypes.c_longlong)]
+                ("walk_limit_hits", ctypes.c_longlong), ("scan_fallbacks", ctypes.c_longlong)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

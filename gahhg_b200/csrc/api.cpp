@@ -179,7 +179,8 @@ static void fill_stats(Grid* g)
 // process-wide knobs (gahhg_set_knob)
 namespace {
 constexpr int KNOB_COUNT = 8;
-std::atomic<long long> g_knobs[KNOB_COUNT] = {0, 1, 0, 0, 0, 0, 0, 0};  // index = gahhg_knob
+constexpr long long KNOB_DEFAULT[KNOB_COUNT] = {0, 1, 1 << 16, 1 << 22, 1 << 20, 0, 0, 0};  // index = gahhg_knob
+std::atomic<long long> g_knobs[KNOB_COUNT] = {0, 1, 1 << 16, 1 << 22, 1 << 20, 0, 0, 0};
 }  // namespace
 
 long long knob(int k) { return (k > 0 && k < KNOB_COUNT) ? g_knobs[k].load(std::memory_order_relaxed) : 0; }
@@ -208,12 +209,13 @@ int gahhg_abi_version(void) { return GAHHG_ABI_VERSION; }
 
 gahhg_status gahhg_set_knob(int k, long long value)
 {
-    if (k != GAHHG_KNOB_GROUPED_PASS2) {
+    if (k < GAHHG_KNOB_GROUPED_PASS2 || k > GAHHG_KNOB_STAGING_POLL_LIMIT) {
         set_error("unknown knob %d", k);
         return GAHHG_ERR_ARG;
     }
-    if (value != 0 && value != 1) {
-        set_error("knob %d takes 0 or 1, not %lld", k, value);
+    if (k == GAHHG_KNOB_GROUPED_PASS2 ? (value != 0 && value != 1) : (value < 0 || value > KNOB_DEFAULT[k])) {
+        set_error("knob %d takes %s, not %lld", k, k == GAHHG_KNOB_GROUPED_PASS2 ? "0 or 1" : "0 .. its default",
+                  value);
         return GAHHG_ERR_ARG;
     }
     gahhg::g_knobs[k].store(value, std::memory_order_relaxed);

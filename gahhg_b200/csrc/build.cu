@@ -371,7 +371,10 @@ gahhg_status check_device_errors(Grid* g, const char* phase)
     // A walk that reaches the step limit is a walk the reference would never
     // finish (its loops are unbounded); the build completes and reports it.
     g->stats.walk_limit_hits = e.walk_step_limit;
-    if (e.scan_lookback_timeout || e.classify_no_converge || e.lattice_overflow || e.other) {
+    // a scan whose look-back ran out of time summed the late tile's inputs
+    // itself: its result is exact, the event is only counted
+    g->stats.scan_fallbacks = e.scan_lookback_timeout;
+    if (e.classify_no_converge || e.lattice_overflow || e.other) {
         set_error("%s: device reported walk_step_limit=%d scan_timeout=%d classify_no_converge=%d "
                   "lattice_overflow=%d other=%d",
                   phase, e.walk_step_limit, e.scan_lookback_timeout, e.classify_no_converge, e.lattice_overflow,
@@ -390,6 +393,7 @@ static GridView view(Grid* g)
     v.C = g->C.ptr;
     v.nb = L.bstart + L.bnum;
     v.nc = L.cstart + L.cnum;
+    v.walk_limit = (int)knob(GAHHG_KNOB_WALK_STEP_LIMIT);
     return v;
 }
 
@@ -416,6 +420,7 @@ static gahhg_status div_grid(Grid* g, int L, bool* more)
     gv.C = g->C.ptr;
     gv.nb = lv.bstart + lv.bnum;
     gv.nc = lv.cstart + lv.cnum;
+    gv.walk_limit = (int)knob(GAHHG_KNOB_WALK_STEP_LIMIT);
     k_mark<<<blocks_for(P->pv_num), TPB, 0, s>>>(P->d_pv, P->d_pe, P->pv_num, gv, L, g->edge_prev.ptr,
                                                  g->edge_cur.ptr, g->d_err);
     GAHHG_TRY(g->cell_a.reserve(lv.cnum, s, false));

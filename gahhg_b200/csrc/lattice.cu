@@ -963,9 +963,9 @@ __device__ __forceinline__ void bulk_stage(void* dst, const void* src, uint32_t 
 }
 
 // Bounded wait for the phase with the given parity; false when it ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int limit = MBAR_POLL_LIMIT)
 {
-    for (int i = 0; i < MBAR_POLL_LIMIT; i++) {
+    for (int i = 0; i < limit; i++) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -1285,7 +1285,7 @@ template <bool STATS>
 __global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, int n, uint8_t* __restrict__ out,
                                                QueryView Q, uint32_t* __restrict__ queue,
                                                uint32_t* __restrict__ leafq, unsigned int* __restrict__ qcount,
-                                               unsigned long long* ctr)
+                                               unsigned long long* ctr, int poll_limit)
 {
     extern __shared__ __align__(16) uint32_t s_sum[];
     __shared__ __align__(8) uint64_t s_bar;
@@ -1296,7 +1296,7 @@ __global__ void __launch_bounds__(TPB) k_locate(const double2* __restrict__ ll, 
         bulk_stage(s_sum, Q.summary, summary_bytes(Q.swords), &s_bar);
     }
     __syncthreads();
-    if (!mbar_wait(&s_bar, 0)) s_late = 1;
+    if (!mbar_wait(&s_bar, 0, poll_limit)) s_late = 1;
     __syncthreads();
     const bool late = s_late != 0;
     // after a wait that ran out the block reads the summary from global
@@ -1392,7 +1392,7 @@ __global__ void __launch_bounds__(TPB) k_batch_locate(const QueryView* __restric
                                                      unsigned int* next_chunk, const double2* __restrict__ ll,
                                                      uint8_t* __restrict__ out, uint32_t* __restrict__ queue,
                                                      uint32_t* __restrict__ leafq, unsigned int* __restrict__ qcount,
-                                                     unsigned long long* ctr)
+                                                     unsigned long long* ctr, int poll_limit)
 {
     // s_sum receives the bulk copies; after a wait runs out the block loads
     // summaries itself into s_own, which no copy writes
@@ -1417,7 +1417,7 @@ __global__ void __launch_bounds__(TPB) k_batch_locate(const QueryView* __restric
         const uint32_t* sum = s_sum;
         if (!late) {
             if (threadIdx.x == 0) bulk_stage(s_sum, Q.summary, summary_bytes(Q.swords), &s_bar);
-            if (!mbar_wait(&s_bar, phase)) s_late = 1;  // any thread's timeout switches the block
+            if (!mbar_wait(&s_bar, phase, poll_limit)) s_late = 1;  // any thread's timeout switches the block
             phase ^= 1u;
             __syncthreads();
             late = s_late != 0;
@@ -1455,7 +1455,22 @@ struct Tiers {
     uint32_t* l3;
     unsigned int* cnt;
     unsigned int cap2, cap3;
+    // the pass-1 queue in leaf-bucket order (k_bucket_sort), used by the first
+    // tier when *sorted == 1
+    const uint32_t* spts = nullptr;
+    const uint32_t* sleaf = nullptr;
+    const unsigned int* sorted = nullptr;
 };
+
+// The pass-1 queue as the first tier reads it: in leaf-bucket order when
+// k_bucket_sort completed, else in pass-1 order.
+__device__ __forceinline__ void first_tier_source(const Tiers& T, const uint32_t*& pts, const uint32_t*& leaf)
+{
+    if (T.sorted && *(const volatile unsigned int*)T.sorted == 1u) {
+        pts = T.spts;
+        leaf = T.sleaf;
+    }
+}
 
 // Where a queued point's index view comes from: one polygon...
 struct OneView {
@@ -1515,12 +1530,15 @@ __global__ void __launch_bounds__(TPB) k_leaf_t1(VS vs, const double2* __restric
 {
     wait_for_predecessor();
     const unsigned int m = *qcount;
+    const uint32_t* src = queue;
+    const uint32_t* src_leaf = T.l1;
+    first_tier_source(T, src, src_leaf);
     int inside = 0, boundary = 0, fp64 = 0;
     for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
-        const uint32_t i = queue[t];
+        const uint32_t i = src[t];
         const QueryView& Q = vs.of(i);
         PointCtx P;
-        const uint32_t w = point_leaf(Q, ll[i], P, T.l1[t]);
+        const uint32_t w = point_leaf(Q, ll[i], P, src_leaf[t]);
         uint8_t lab;
         if ((w & KIND_MASK) == KIND_PURE) {
             lab = (uint8_t)(w & 3u);
@@ -1550,12 +1568,15 @@ __global__ void __launch_bounds__(TPB) k_leaf_t2(VS vs, const double2* __restric
 {
     wait_for_predecessor();
     const unsigned int m = min(*src_count, src_cap);
+    const uint32_t* sp = src;
+    const uint32_t* sl = src_leaf;
+    if (FROM_PASS1) first_tier_source(T, sp, sl);
     int inside = 0, boundary = 0, exact = 0;
     for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
-        const uint32_t i = src[t];
+        const uint32_t i = sp[t];
         const QueryView& Q = vs.of(i);
         PointCtx P;
-        const uint32_t w = point_leaf(Q, ll[i], P, src_leaf[t]);
+        const uint32_t w = point_leaf(Q, ll[i], P, sl[t]);
         uint8_t lab;
         if ((w & KIND_MASK) == KIND_PURE) {
             lab = (uint8_t)(w & 3u);
@@ -1609,55 +1630,59 @@ __global__ void __launch_bounds__(TPB) k_leaf_t3(VS vs, const double2* __restric
     if (ctr) count_inside(inside, ctr + 3);
 }
 
-// ------------------------------------------ pass 2 grouped by leaf bucket --
+// ------------------------------------------- pass-2 queue in leaf order --
 //
-// One persistent launch (k_group) replaces the per-point tiers 1 and 2 for a
-// single polygon.  Its blocks take work items in order from a counter:
-//   count items    pass-1 queue entries counted per bucket of 2^GROUP_SHIFT
-//                  consecutive leaves;
+// Pass 1 queues points in input order, so on inputs without spatial order
+// (C2's near-edge points) neighbouring threads of the tiers test unrelated
+// leaves, and every point gathers its leaf's records from an index larger than
+// L2.  k_bucket_sort puts the queue in order of bucket of 2^GROUP_SHIFT
+// consecutive leaves (whose records are contiguous in memory) before the
+// tiers run, so that a warp's points share a handful of leaves and a block's
+// tile of the queue spans a short, contiguous range of records.  One
+// persistent launch; its blocks take work items in order from a counter:
+//   count items    queue entries counted per bucket;
 //   scan items     after every count item finished: exclusive scan of the
-//                  bucket counts (decoupled look-back between the items);
-//   scatter items  the pass-1 queue scattered into bucket order (after every
-//                  scan item finished);
-//   bucket items   after every scatter item finished: the bucket's leaf
-//                  records and FP32 edge records (contiguous: leaves and their
-//                  records are stored in leaf order) are staged in shared
-//                  memory by one bulk copy (TMA), every point of the bucket runs
-//                  the FP32 tier against them, and the points it defers run the
-//                  FP64 tier against the bucket's edge ids and FP64 ends,
-//                  gathered into shared memory once per bucket.  Points the FP64
-//                  tier defers go to the tier-3 queue.
+//                  counts (decoupled look-back between the items);
+//   scatter items  after every scan item finished: entries written to their
+//                  bucket's range of the sorted point and leaf-word arrays.
 // A block waits only on items that blocks which started before it hold (items
 // are taken in order), and every wait is bounded: a wait that runs out marks
-// the pass failed, the remaining buckets are skipped, and the tier-3 launch
-// sweeps every queued point still unlabelled.  Sparse buckets (fewer than
-// G_STAGE_MIN points) and buckets with more records than fit read the
-// records from global memory instead.
-constexpr int G_TPB = 128;
-constexpr int G_RECS = 1024;              // FP32 records staged per bucket (16 KB)
-constexpr int G_ENDS = 448;               // records whose FP64 ends are staged (21 KB)
-constexpr int G_ROUND = 512;              // bucket entries per round of the FP32 tier
-constexpr int G_SCAN = G_TPB * 8;         // buckets per scan item
-constexpr int G_SCATTER = G_TPB * 16;     // queue entries per scatter item
-constexpr int G_STAGE_MIN = 8;
-constexpr int G_WAIT_LIMIT = 1 << 22;     // polls (about 0.5 s) before a wait gives up
-constexpr int G_BLOCKS_PER_SM = 4;
+// the sort failed and the tiers read the queue in pass-1 order.  The sort is
+// skipped (the tiers read pass-1 order) when the queue holds fewer than
+// SORT_RATIO entries per bucket: sparse buckets gain nothing from it.
+constexpr int S_TPB = 256;
+constexpr int S_SCAN = S_TPB * 8;         // buckets per scan item
+constexpr int S_SCATTER = S_TPB * 16;     // queue entries per count / scatter item
+constexpr int SORT_RATIO = 4;
+constexpr int S_WAIT_LIMIT = 1 << 22;     // polls (about 0.5 s) before a wait gives up
+constexpr int S_BLOCKS_PER_SM = 4;
 
 struct GroupScratch {
     unsigned int* hist;           // [nb + 1] queued points per bucket (bucket nb: no leaf word); zero
     unsigned long long* status;   // [nscan] scan look-back words (value | flag << 32); zero
-    unsigned int* boff;           // [nb + 2] bucket offsets in `sorted`
-    uint2* sorted;                // {point, leaf word} per queued point, in bucket order
-    unsigned int* sync;           // [0] next item, [1] count, [2] scan, [3] scatter items done, [4] failed; zero
+    unsigned int* boff;           // [nb + 2] bucket offsets in the sorted arrays
+    uint32_t* spts;               // sorted point indices
+    uint32_t* sleaf;              // sorted leaf words
+    unsigned int* sync;           // [0] next item, [1] count, [2] scan, [3] scatter items done, [4] failed,
+                                  // [5] 1 when the sorted arrays are complete; zero before the pass
     int nb;
 };
 
-__host__ __device__ inline int group_scan_items(int nb) { return (nb + 1 + G_SCAN - 1) / G_SCAN; }
+__host__ __device__ inline int group_scan_items(int nb) { return (nb + 1 + S_SCAN - 1) / S_SCAN; }
+__host__ __device__ inline bool group_worth_sorting(unsigned int m, int nb)
+{
+    return (unsigned long long)m >= (unsigned long long)SORT_RATIO * (unsigned long long)(nb + 1);
+}
 
-// Thread-0 helpers of k_group.
+__device__ __forceinline__ uint32_t group_bucket(uint32_t w, int nb)
+{
+    return (w & KIND_MASK) == KIND_LEAF ? min((w & INDEX_MASK) >> GROUP_SHIFT, (uint32_t)nb) : (uint32_t)nb;
+}
+
+// Thread 0: bounded wait until *p >= target.
 __device__ __forceinline__ bool wait_count(const unsigned int* p, unsigned int target)
 {
-    for (int i = 0; i < G_WAIT_LIMIT; i++) {
+    for (int i = 0; i < S_WAIT_LIMIT; i++) {
         if (*(const volatile unsigned int*)p >= target) {
             __threadfence();
             return true;
@@ -1667,111 +1692,20 @@ __device__ __forceinline__ bool wait_count(const unsigned int* p, unsigned int t
     return false;
 }
 
-__device__ __forceinline__ uint32_t group_bucket(uint32_t w, int nb)
+__global__ void __launch_bounds__(S_TPB, S_BLOCKS_PER_SM)
+    k_bucket_sort(const uint32_t* __restrict__ queue, const uint32_t* __restrict__ l1,
+                  const unsigned int* __restrict__ qcount, GroupScratch S)
 {
-    return (w & KIND_MASK) == KIND_LEAF ? min((w & INDEX_MASK) >> GROUP_SHIFT, (uint32_t)nb) : (uint32_t)nb;
-}
-
-__device__ __forceinline__ void group_fail(const GroupScratch& S, const Tiers& T)
-{
-    atomicExch(S.sync + 4, 1u);
-    *(volatile unsigned int*)(T.cnt + 2) = 1u;  // tier 3 sweeps the unlabelled queued points
-}
-
-// FP32 tier on records rec[0 .. L.cnt) (shared or global memory).
-__device__ __forceinline__ uint8_t fp32_records(const LeafRec& L, const float4* rec, const PointCtx& P)
-{
-    local_frame::Offset o;
-    if (!(fabs(P.lon) <= 540.0) || !local_frame::offset(P.lon, P.lat, L.lon, L.lat, o)) return LABEL_DEFER;
-    local_frame::Frame f;
-    local_frame::project(o, f);
-    int par = 0;
-    for (int k = 0; k < L.cnt; k++) {
-        // stored order: orient(A, B, R) = +1, so a crossing needs s2 = -1,
-        // s3 = orient(R, q, A) = -1 and s4 = orient(R, q, B) = +1
-        const float4 r = rec[k];
-        const int s2 = local_frame::sign_edge(f, r.x, r.y, r.z, r.w);
-        if (s2 == 0) return LABEL_DEFER;
-        if (s2 > 0) continue;
-        const int s3 = local_frame::sign_end(f, r.x, r.y);
-        if (s3 == 0) return LABEL_DEFER;
-        if (s3 > 0) continue;
-        const int s4 = local_frame::sign_end(f, r.z, r.w);
-        if (s4 == 0) return LABEL_DEFER;
-        if (s4 > 0) par ^= 1;
-    }
-    return (uint8_t)(par ? 3 - L.label : L.label);
-}
-
-// FP64 tier with the leaf's edge ids eid[0 .. L.cnt) and, when `rec_ends` is
-// set, the records' FP64 ends rec_ends[3k .. 3k + 2] (else from the per-edge
-// table).
-__device__ __forceinline__ uint8_t fp64_records(const QueryView& Q, const LeafRec& L, const uint32_t* eid,
-                                                const double2* rec_ends, PointCtx& P)
-{
-    P.need64();
-    double LR[3];
-    gahhg_canon_vertex_xyz(L.lon, L.lat, LR);
-    int par = 0;
-    for (int k = 0; k < L.cnt; k++) {
-        const uint32_t es = eid[k];
-        double2 e0, e1, e2;
-        if (rec_ends) {
-            e0 = rec_ends[3 * k];
-            e1 = rec_ends[3 * k + 1];
-            e2 = rec_ends[3 * k + 2];
-        } else {
-            const double2* p = Q.ends + 3 * (size_t)(es & 0x7fffffffu);
-            e0 = __ldg(p);
-            e1 = __ldg(p + 1);
-            e2 = __ldg(p + 2);
-        }
-        const int s1 = (es >> 31) ? 1 : -1;
-        const double A[3] = {e0.x, e0.y, e1.x}, B[3] = {e1.y, e2.x, e2.y};
-        if (exact::same(P.q, A) || exact::same(P.q, B)) return CELL_IN;  // vertex rule
-        if (exact::same(P.q, LR)) return L.label;                       // q is the center
-        const int s2 = exact::orient_fp64_near(A, B, P.q);
-        if (s2 == 0) return LABEL_DEFER;
-        if (s2 == s1) continue;
-        const int s3 = exact::orient_fp64_near(LR, P.q, A);
-        if (s3 == 0) return LABEL_DEFER;
-        if (s3 != s2) continue;
-        const int s4 = exact::orient_fp64_near(LR, P.q, B);
-        if (s4 == 0) return LABEL_DEFER;
-        if (s4 == -s2) par ^= 1;
-    }
-    return (uint8_t)(par ? 3 - L.label : L.label);
-}
-
-template <bool FP32, bool STATS>
-__global__ void __launch_bounds__(G_TPB, G_BLOCKS_PER_SM)
-    k_group(QueryView Q, const double2* __restrict__ ll, uint8_t* __restrict__ out,
-            const uint32_t* __restrict__ queue, const uint32_t* __restrict__ l1,
-            const unsigned int* __restrict__ qcount, GroupScratch S, Tiers T, unsigned long long* ctr)
-{
-    __shared__ __align__(16) LeafRec s_leaf[1 << GROUP_SHIFT];
-    __shared__ __align__(16) float4 s_rec[G_RECS];
-    __shared__ __align__(16) uint32_t s_eid[G_ENDS];
-    __shared__ __align__(16) double2 s_end[3 * G_ENDS];
-    __shared__ unsigned short s_def[G_ROUND];
-    __shared__ __align__(8) uint64_t s_bar;
-    __shared__ unsigned int s_warp[G_TPB / 32];
+    __shared__ unsigned int s_warp[S_TPB / 32];
     __shared__ unsigned int s_prefix;
-    __shared__ int s_item, s_ok, s_ndef, s_late;
+    __shared__ int s_item, s_ok;
     wait_for_predecessor();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned int m = *qcount;
     const int nb = S.nb;
     const int nscan = group_scan_items(nb);
-    const int nsc = (int)((m + G_SCATTER - 1) / G_SCATTER);
-    const long long nitems = m ? (long long)2 * nsc + nscan + nb + 1 : 0;
-    if (tid == 0) {
-        s_late = 0;
-        mbar_init(&s_bar);
-    }
-    uint32_t phase = 0;
-    bool pending = false;  // a bulk copy whose wait ran out may still be in flight
-    int inside = 0, boundary = 0, fp64 = 0, exact = 0;
+    const int nsc = (int)((m + S_SCATTER - 1) / S_SCATTER);
+    const long long nitems = group_worth_sorting(m, nb) ? (long long)2 * nsc + nscan : 0;
     for (;;) {
         __syncthreads();
         if (tid == 0) s_item = (int)atomicAdd(S.sync + 0, 1u);
@@ -1779,22 +1713,19 @@ __global__ void __launch_bounds__(G_TPB, G_BLOCKS_PER_SM)
         const long long item = s_item;
         if (item >= nitems) break;
         if (item < nsc) {
-            // ---- count item: entries per bucket
+            // ---- count item
             const unsigned int c = (unsigned int)item;
-            const unsigned int e1 = min(m, (c + 1) * (unsigned int)G_SCATTER);
-            for (unsigned int t = c * G_SCATTER + tid; t < e1; t += G_TPB) atomicAdd(S.hist + group_bucket(l1[t], nb), 1u);
+            const unsigned int e1 = min(m, (c + 1) * (unsigned int)S_SCATTER);
+            for (unsigned int t = c * S_SCATTER + tid; t < e1; t += S_TPB) atomicAdd(S.hist + group_bucket(l1[t], nb), 1u);
             __threadfence();
             __syncthreads();
             if (tid == 0) atomicAdd(S.sync + 1, 1u);
         } else if (item < nsc + nscan) {
-            // ---- scan item: buckets [t * G_SCAN, ...) of hist[0 .. nb]
+            // ---- scan item: buckets [t * S_SCAN, ...) of hist[0 .. nb]
             const int t = (int)(item - nsc);
-            if (tid == 0) {
-                const bool ok = wait_count(S.sync + 1, (unsigned int)nsc);
-                if (!ok) group_fail(S, T);
-            }
+            if (tid == 0 && !wait_count(S.sync + 1, (unsigned int)nsc)) atomicExch(S.sync + 4, 1u);
             __syncthreads();
-            const int base = t * G_SCAN + tid * 8;
+            const int base = t * S_SCAN + tid * 8;
             unsigned int v[8], sum = 0;
 #pragma unroll
             for (int k = 0; k < 8; k++) {
@@ -1811,7 +1742,7 @@ __global__ void __launch_bounds__(G_TPB, G_BLOCKS_PER_SM)
             __syncthreads();
             if (tid == 0) {
                 unsigned int run = 0;
-                for (int w = 0; w < G_TPB / 32; w++) {
+                for (int w = 0; w < S_TPB / 32; w++) {
                     const unsigned int x = s_warp[w];
                     s_warp[w] = run;
                     run += x;
@@ -1828,7 +1759,7 @@ __global__ void __launch_bounds__(G_TPB, G_BLOCKS_PER_SM)
                         int spins = 0;
                         unsigned long long w;
                         while (((w = *(const volatile unsigned long long*)(S.status + j)) >> 32) == 0ull) {
-                            if (++spins > G_WAIT_LIMIT) break;
+                            if (++spins > S_WAIT_LIMIT) break;
                             __nanosleep(64);
                         }
                         if ((w >> 32) == 0ull) {
@@ -1839,7 +1770,7 @@ __global__ void __launch_bounds__(G_TPB, G_BLOCKS_PER_SM)
                         if ((w >> 32) == 2ull) break;
                         j--;
                     }
-                    if (!ok) group_fail(S, T);
+                    if (!ok) atomicExch(S.sync + 4, 1u);
                     atomicExch(S.status + t, PRE | (excl + run));
                 }
                 s_prefix = excl;
@@ -1855,19 +1786,19 @@ __global__ void __launch_bounds__(G_TPB, G_BLOCKS_PER_SM)
             __threadfence();
             __syncthreads();
             if (tid == 0) atomicAdd(S.sync + 2, 1u);
-        } else if (item < 2 * nsc + nscan) {
-            // ---- scatter item: pass-1 queue entries into bucket order
+        } else {
+            // ---- scatter item
             if (tid == 0) {
                 const bool ok = wait_count(S.sync + 2, (unsigned int)nscan);
-                if (!ok) group_fail(S, T);
+                if (!ok) atomicExch(S.sync + 4, 1u);
                 s_ok = ok && *(volatile unsigned int*)(S.sync + 4) == 0u;
             }
             __syncthreads();
+            bool bad = false;
             if (s_ok) {
                 const unsigned int c = (unsigned int)(item - nsc - nscan);
-                const unsigned int e1 = min(m, (c + 1) * (unsigned int)G_SCATTER);
-                bool bad = false;
-                for (unsigned int t = c * G_SCATTER + tid; t < e1; t += G_TPB) {
+                const unsigned int e1 = min(m, (c + 1) * (unsigned int)S_SCATTER);
+                for (unsigned int t = c * S_SCATTER + tid; t < e1; t += S_TPB) {
                     const uint32_t w = l1[t];
                     const uint32_t b = group_bucket(w, nb);
                     const unsigned int lo = __ldcg(S.boff + b), hi = __ldcg(S.boff + b + 1);
@@ -1876,149 +1807,21 @@ __global__ void __launch_bounds__(G_TPB, G_BLOCKS_PER_SM)
                         bad = true;  // counts and entries disagree: never write out of the bucket
                         continue;
                     }
-                    S.sorted[lo + r - 1u] = make_uint2(queue[t], w);
+                    S.spts[lo + r - 1u] = queue[t];
+                    S.sleaf[lo + r - 1u] = w;
                 }
-                if (__syncthreads_or(bad) && tid == 0) group_fail(S, T);
             }
+            if (__syncthreads_or(bad) && tid == 0) atomicExch(S.sync + 4, 1u);
             __threadfence();
             __syncthreads();
-            if (tid == 0) atomicAdd(S.sync + 3, 1u);
-        } else {
-            // ---- bucket item
-            const int b = (int)(item - 2 * nsc - nscan);
-            if (tid == 0) {
-                const bool ok = wait_count(S.sync + 3, (unsigned int)nsc);
-                if (!ok) group_fail(S, T);
-                s_ok = ok && *(volatile unsigned int*)(S.sync + 4) == 0u;
-            }
-            __syncthreads();
-            if (!s_ok) continue;
-            const unsigned int e0 = __ldcg(S.boff + b), E = __ldcg(S.boff + b + 1) - e0;
-            if (E == 0u) continue;
-            if (e0 > m || E > m - e0) {  // offsets beyond the queue: never expected
-                if (tid == 0) group_fail(S, T);
-                continue;
-            }
-            if (b == nb) {
-                // points without a leaf word: the complete test of tier 3
-                for (unsigned int j = tid; j < E; j += G_TPB) {
-                    const uint2 en = __ldcg(S.sorted + e0 + j);
-                    if (!push_deferred(en.x, en.y, T.q3, T.l3, T.cnt + 1, T.cap3)) T.cnt[2] = 1;
-                }
-                continue;
-            }
-            const int l0 = b << GROUP_SHIFT;
-            const int nl = min(1 << GROUP_SHIFT, Q.nleaves - l0);
-            const LeafRec lf = Q.leaves[l0], lz = Q.leaves[l0 + nl - 1];
-            const uint32_t rec0 = lf.off;
-            const uint32_t nrec = lz.off + lz.cnt - rec0;
-            const bool stage = !s_late && E >= (unsigned int)G_STAGE_MIN && nrec <= (uint32_t)G_RECS;
-            if (stage) {
-                if (tid == 0) {
-                    // leaf records in 16-byte units (the leaf array keeps a spare
-                    // record at its end), edge records exactly; both 16-byte aligned
-                    const uint32_t bl = ((uint32_t)nl * (uint32_t)sizeof(LeafRec) + 15u) & ~15u;
-                    const uint32_t br = nrec * (uint32_t)sizeof(float4);
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&s_bar)),
-                                 "r"(bl + br)
-                                 : "memory");
-                    asm volatile(
-                        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                            smem_u32(s_leaf)),
-                        "l"(Q.leaves + l0), "r"(bl), "r"(smem_u32(&s_bar))
-                        : "memory");
-                    if (br)
-                        asm volatile(
-                            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                                smem_u32(s_rec)),
-                            "l"(Q.recs + rec0), "r"(br), "r"(smem_u32(&s_bar))
-                            : "memory");
-                }
-                if (!mbar_wait(&s_bar, phase)) s_late = 1;
-                phase ^= 1u;
-                __syncthreads();
-            }
-            // a copy that ran out of time may still write s_leaf / s_rec: from then
-            // on this block reads global memory only (and waits for the copy at exit)
-            const bool late = s_late != 0;
-            const bool staged = stage && !late;
-            if (stage && late) pending = true;
-            bool ends_ready = false;
-            for (unsigned int r0 = 0; r0 < E; r0 += G_ROUND) {
-                const unsigned int r1 = min(E, r0 + (unsigned int)G_ROUND);
-                if (tid == 0) s_ndef = 0;
-                __syncthreads();
-                for (unsigned int j = r0 + tid; j < r1; j += G_TPB) {
-                    const uint2 en = __ldcg(S.sorted + e0 + j);
-                    const uint32_t leaf = en.y & INDEX_MASK;
-                    const int li = (int)leaf - l0;
-                    if (li < 0 || li >= nl) {  // not this bucket's leaf: never expected
-                        if (!push_deferred(en.x, en.y, T.q3, T.l3, T.cnt + 1, T.cap3)) T.cnt[2] = 1;
-                        continue;
-                    }
-                    boundary++;
-                    uint8_t lab = LABEL_DEFER;
-                    if (FP32) {
-                        PointCtx P;
-                        point_leaf(Q, ll[en.x], P, en.y);
-                        const LeafRec L = staged ? s_leaf[li] : Q.leaves[leaf];
-                        lab = fp32_records(L, staged ? s_rec + (L.off - rec0) : Q.recs + L.off, P);
-                    }
-                    if (lab == LABEL_DEFER) {
-                        if (FP32) fp64++;
-                        s_def[atomicAdd(&s_ndef, 1)] = (unsigned short)(j - r0);
-                    } else {
-                        out[en.x] = lab;
-                        inside += lab == CELL_IN;
-                    }
-                }
-                __syncthreads();
-                const int nd = s_ndef;
-                if (nd == 0) continue;
-                // the bucket's edge ids and FP64 ends, gathered once per bucket when
-                // its deferred points will read them often enough
-                const bool ends_staged = nrec <= (uint32_t)G_ENDS && (ends_ready || (uint32_t)nd * 4u >= nrec);
-                if (ends_staged && !ends_ready) {
-                    for (uint32_t k = tid; k < nrec; k += G_TPB) {
-                        const uint32_t es = __ldg(Q.eids + rec0 + k);
-                        s_eid[k] = es;
-                        const double2* p = Q.ends + 3 * (size_t)(es & 0x7fffffffu);
-                        s_end[3 * k] = __ldg(p);
-                        s_end[3 * k + 1] = __ldg(p + 1);
-                        s_end[3 * k + 2] = __ldg(p + 2);
-                    }
-                    ends_ready = true;
-                    __syncthreads();
-                }
-                for (int d = tid; d < nd; d += G_TPB) {
-                    const uint2 en = __ldcg(S.sorted + e0 + r0 + s_def[d]);
-                    const uint32_t leaf = en.y & INDEX_MASK;
-                    PointCtx P;
-                    point_leaf(Q, ll[en.x], P, en.y);
-                    const LeafRec L = staged ? s_leaf[leaf - l0] : Q.leaves[leaf];
-                    const uint8_t lab =
-                        ends_staged ? fp64_records(Q, L, s_eid + (L.off - rec0), s_end + 3 * (L.off - rec0), P)
-                                    : fp64_records(Q, L, Q.eids + L.off, nullptr, P);
-                    if (lab == LABEL_DEFER) {
-                        exact++;
-                        if (!push_deferred(en.x, en.y, T.q3, T.l3, T.cnt + 1, T.cap3)) T.cnt[2] = 1;
-                    } else {
-                        out[en.x] = lab;
-                        inside += lab == CELL_IN;
-                    }
-                }
-                __syncthreads();
-            }
+            // the last scatter item to finish declares the arrays complete (every
+            // failure was flagged before its item was counted)
+            if (tid == 0 && atomicAdd(S.sync + 3, 1u) + 1u == (unsigned int)nsc &&
+                *(volatile unsigned int*)(S.sync + 4) == 0u)
+                atomicExch(S.sync + 5, 1u);
         }
     }
-    if (pending) {
-        // the copy in flight ends before the block does (bounded)
-        if (tid == 0) atomicAdd(&g_tma_timeouts, 1u);
-        mbar_wait(&s_bar, phase ^ 1u);
-    }
     allow_dependents();
-    if (STATS && ctr) count_stats(ctr, inside, boundary, fp64, exact);
 }
 
 // Launch with programmatic stream serialization (see wait_for_predecessor).
@@ -2792,10 +2595,10 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
     const QueryView Q = make_view(g);
     const long long chunk = std::min<long long>((long long)n, QUERY_CHUNK);
     // Words: [pass-2 queue: chunk][control: 64 (queue fill at +32, tier counters
-    // at +33..35, k_group's sync words at +36..40)][bucket counts: nb + 1]
+    // at +33..35, k_bucket_sort's sync words at +36..41)][bucket counts: nb + 1]
     // [pad to 8 bytes][scan look-back words: 2 per scan item][bucket offsets:
     // nb + 2][pass-2 leaf words: chunk][tier-2 queue][its leaf words][tier-3
-    // queue][its leaf words][pad][bucket-ordered entries: 2 per queued point].
+    // queue][its leaf words][sorted points: chunk][sorted leaf words: chunk].
     // One memset per pass clears the control words, counts and look-back words.
     unsigned int cap2 = 0, cap3 = 0;
     tier_caps(chunk, &cap2, &cap3);
@@ -2806,8 +2609,7 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
     const size_t status_at = (hist_at + (grouped ? nb + 1 : 0) + 1) & ~(size_t)1;
     const size_t boff_at = status_at + 2 * nscan;
     const size_t l1_at = boff_at + (grouped ? nb + 2 : 0);
-    const size_t tiers_end = l1_at + (size_t)chunk + 2 * ((size_t)cap2 + cap3);
-    const size_t sorted_at = (tiers_end + 1) & ~(size_t)1;
+    const size_t sorted_at = l1_at + (size_t)chunk + 2 * ((size_t)cap2 + cap3);
     const size_t words = sorted_at + (grouped ? 2 * (size_t)chunk : 0);
     uint32_t* queue = nullptr;
     GAHHG_TRY(pool_alloc((void**)&queue, sizeof(uint32_t) * words, g->device, s));
@@ -2826,7 +2628,8 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
     G.hist = queue + hist_at;
     G.status = (unsigned long long*)(queue + status_at);
     G.boff = queue + boff_at;
-    G.sorted = (uint2*)(queue + sorted_at);
+    G.spts = queue + sorted_at;
+    G.sleaf = queue + sorted_at + chunk;
     G.nb = (int)nb;
     const gahhg_status st = lattice_query_with(Q, d_lonlat, (long long)n, d_labels, precision, s, d_counters,
                                                queue, qcount, chunk, g->device, &T, grouped ? &G : nullptr);
@@ -2847,7 +2650,7 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
     for (long long off = 0; off < n; off += chunk) {
         const int m = (int)std::min<long long>(chunk, n - off);
         const double2* ll = (const double2*)d_lonlat + off;
-        // the queue fill, the tier counters and, when grouping, k_group's sync
+        // the queue fill, the tier counters and, when sorting, k_bucket_sort's sync
         // words, the bucket counts and the look-back words (laid out after them;
         // the control words run to the counts)
         const size_t zero_words =
@@ -2857,34 +2660,25 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
         const long long tiles = ((long long)m + TPB * LOC_UNROLL - 1) / (TPB * LOC_UNROLL);
         const int grid = (int)std::min<long long>(tiles, (long long)sms * 8);
         uint32_t* leafq = tiers ? tiers->l1 : nullptr;
+        const int polls = (int)knob(GAHHG_KNOB_STAGING_POLL_LIMIT);
         if (ctr)
             k_locate<true><<<grid, TPB, summary_bytes(Q.swords), s>>>(ll, m, d_labels + off, Q, queue, leafq, qcount,
-                                                                      ctr);
+                                                                      ctr, polls);
         else
             k_locate<false><<<grid, TPB, summary_bytes(Q.swords), s>>>(ll, m, d_labels + off, Q, queue, leafq,
-                                                                       qcount, ctr);
+                                                                       qcount, ctr, polls);
         if (tiers && grp) {
-            // pass 2 grouped by leaf bucket (tiers 1 and 2), then tier 3
-            const int gg = sms * G_BLOCKS_PER_SM;
-            const bool fp32 = precision != GAHHG_QUERY_FP64_FILTER;
-            const uint32_t* cq = queue;
-            const uint32_t* cl1 = tiers->l1;
-            const unsigned int* cqc = qcount;
-            if (fp32 && ctr)
-                launch_dependent_tpb(k_group<true, true>, gg, G_TPB, s, Q, ll, d_labels + off, cq, cl1, cqc, *grp,
-                                     *tiers, ctr);
-            else if (fp32)
-                launch_dependent_tpb(k_group<true, false>, gg, G_TPB, s, Q, ll, d_labels + off, cq, cl1, cqc, *grp,
-                                     *tiers, ctr);
-            else if (ctr)
-                launch_dependent_tpb(k_group<false, true>, gg, G_TPB, s, Q, ll, d_labels + off, cq, cl1, cqc, *grp,
-                                     *tiers, ctr);
-            else
-                launch_dependent_tpb(k_group<false, false>, gg, G_TPB, s, Q, ll, d_labels + off, cq, cl1, cqc, *grp,
-                                     *tiers, ctr);
-            launch_dependent(k_leaf_t3<OneView>, sms * 2, s, OneView{Q}, ll, d_labels + off, cq, cqc, *tiers, ctr);
-        } else if (tiers)
+            // the pass-1 queue in leaf-bucket order, then the tiers over it
+            launch_dependent_tpb(k_bucket_sort, sms * S_BLOCKS_PER_SM, S_TPB, s, (const uint32_t*)queue,
+                                 (const uint32_t*)tiers->l1, (const unsigned int*)qcount, *grp);
+            Tiers T = *tiers;
+            T.spts = grp->spts;
+            T.sleaf = grp->sleaf;
+            T.sorted = grp->sync + 5;
+            leaf_tiers_launch(OneView{Q}, ll, d_labels + off, queue, qcount, T, precision, ctr, sms, s);
+        } else if (tiers) {
             leaf_tiers_launch(OneView{Q}, ll, d_labels + off, queue, qcount, *tiers, precision, ctr, sms, s);
+        }
         else if (precision == GAHHG_QUERY_FP64_FILTER)
             k_leaf<false><<<sms * 4, TPB, 0, s>>>(ll, d_labels + off, Q, queue, qcount, ctr);
         else
@@ -3042,12 +2836,13 @@ gahhg_status batch_query_launch(const void* d_views, const void* d_chunks, int n
     T.q3 = T.l2 + T.cap2;
     T.l3 = T.q3 + T.cap3;
     T.cnt = counters + 2;
+    const int polls = (int)knob(GAHHG_KNOB_STAGING_POLL_LIMIT);
     if (ctr)
         k_batch_locate<true><<<grid, TPB, 0, s>>>(views, chunks, nchunks, counters + 1, (const double2*)d_lonlat,
-                                                  d_labels, queue, T.l1, counters, ctr);
+                                                  d_labels, queue, T.l1, counters, ctr, polls);
     else
         k_batch_locate<false><<<grid, TPB, 0, s>>>(views, chunks, nchunks, counters + 1, (const double2*)d_lonlat,
-                                                   d_labels, queue, T.l1, counters, ctr);
+                                                   d_labels, queue, T.l1, counters, ctr, polls);
     leaf_tiers_launch(ChunkViews{views, chunks, nchunks}, (const double2*)d_lonlat, d_labels, queue, counters, T,
                       precision, ctr, sms, s);
     GAHHG_CUDA_TRY(cudaGetLastError());

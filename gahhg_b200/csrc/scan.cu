@@ -13,7 +13,9 @@
 // older call has a different epoch and reads as "not ready", so the status
 // array never needs clearing.  Tiles take their index from an atomic counter
 // in launch order, so every tile a look-back waits on has already started;
-// each wait is still bounded and reports through DeviceErrors if it expires.
+// each wait is still bounded (spin_limit polls): when it runs out, the tile
+// sums the late tile's inputs itself and goes on looking back, so the result
+// stays exact, and the event is counted in DeviceErrors (scan fallbacks).
 #include "gahhg_internal.h"
 
 namespace gahhg {
@@ -23,7 +25,6 @@ namespace {
 constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_ITEMS = 8;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
-constexpr long long SCAN_SPIN_LIMIT = 1ll << 22;
 
 struct ScanState {
     unsigned long long* status;
@@ -41,7 +42,7 @@ __device__ __forceinline__ unsigned long long load_status(const unsigned long lo
 __global__ void __launch_bounds__(SCAN_THREADS)
 k_scan_exclusive(const int* __restrict__ in, int* __restrict__ out, int n, int* total,
                  unsigned long long* status, unsigned int* counter, unsigned int tile_base,
-                 unsigned int epoch, int ntiles, DeviceErrors* err)
+                 unsigned int epoch, int ntiles, DeviceErrors* err, long long spin_limit)
 {
     __shared__ int s_tile;
     __shared__ int s_prefix;
@@ -98,9 +99,17 @@ k_scan_exclusive(const int* __restrict__ in, int* __restrict__ out, int n, int* 
                 unsigned int hi = (unsigned int)(w >> 32);
                 unsigned int state = hi & 3u;
                 if ((hi >> 2) != (epoch & 0x3fffffffu) || state == 0u) {
-                    if (++spins > SCAN_SPIN_LIMIT) {
+                    if (++spins > spin_limit) {
+                        // tile j is late: add its inputs directly and look further back
                         atomicAdd(&err->scan_lookback_timeout, 1);
-                        break;
+                        const long long j0 = (long long)j * SCAN_TILE;
+                        const long long j1 = j0 + SCAN_TILE < n ? j0 + SCAN_TILE : n;
+                        int agg_j = 0;
+                        for (long long idx = j0; idx < j1; idx++) agg_j += in[idx];
+                        excl += agg_j;
+                        spins = 0;
+                        j--;
+                        continue;
                     }
                     if (spins > 64) __nanosleep(64);
                     continue;
@@ -208,7 +217,8 @@ gahhg_status scan_exclusive(const int* d_in, int* d_out, int n, int* d_total, vo
     }
     const unsigned int epoch = st->epoch & 0x3fffffffu;
     k_scan_exclusive<<<ntiles, SCAN_THREADS, 0, s>>>(d_in, d_out, n, d_total, st->status, st->counter,
-                                                     st->tile_base, epoch, ntiles, err);
+                                                     st->tile_base, epoch, ntiles, err,
+                                                     knob(GAHHG_KNOB_SCAN_SPIN_LIMIT));
     GAHHG_CUDA_TRY(cudaGetLastError());
     st->tile_base += (unsigned int)ntiles;
     st->epoch = (st->epoch + 1) & 0x3fffffffu;

@@ -11,7 +11,8 @@
 // grid, a walk that returns to a state it was in before (the next step
 // depends only on the current cell and the border it entered by, so such a
 // walk would repeat forever; Brent's cycle test finds it within a few times
-// the cycle's length) or a walk longer than WALK_STEP_LIMIT ends the walk and
+// the cycle's length) or a walk longer than the step limit (GridView::
+// walk_limit, default WALK_STEP_LIMIT, gahhg_set_knob) ends the walk and
 // is counted in DeviceErrors instead of reading garbage or spinning.  A walk
 // that ends in the reference never repeats a state, so none of these changes
 // a walk the reference completes.
@@ -29,6 +30,7 @@ struct GridView {
     Cell* C;
     int nb;  // borders in use (valid indices [0, nb))
     int nc;  // cells in use
+    int walk_limit = WALK_STEP_LIMIT;  // steps before a walk gives up
 };
 
 __device__ __forceinline__ int inside_cell(D3 p, int cid, const GridView& g)
@@ -150,7 +152,7 @@ __device__ __forceinline__ int walk_edge(D3 p0, D3 p1, int cur, const GridView& 
     int steps = 0;
     int seen_cur = cur, seen_in = in, window = 1, since = 0;  // Brent's cycle test
     while (true) {
-        if (steps >= WALK_STEP_LIMIT || (steps > 0 && cur == seen_cur && in == seen_in)) {
+        if (steps >= g.walk_limit || (steps > 0 && cur == seen_cur && in == seen_in)) {
             atomicAdd(&err->walk_step_limit, 1);
             return steps;
         }

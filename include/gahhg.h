@@ -87,6 +87,8 @@ typedef struct {
     long long boundary_points; /* exact query: points that ran crossing tests */
     long long walk_limit_hits; /* edge walks stopped on a repeated state or at the step limit (the reference
                                   would not terminate) */
+    long long scan_fallbacks;  /* build scans whose bounded look-back ran out and summed the late tile's
+                                  inputs instead (exact either way; 0 in normal operation) */
 } gahhg_stats;
 
 /* Defaults as in GPISPParam::GPISPParam (source/GPISPParam.h:64-77). */
@@ -343,12 +345,26 @@ gahhg_status gahhg_grid0_export(double* v, void* b, void* c);
 gahhg_status gahhg_staging_fallbacks(int device, unsigned long long* count);
 
 /* Process-wide tuning and test knobs.  No counterpart in the reference.
- * GAHHG_KNOB_GROUPED_PASS2: 1 (default) runs pass 2 of single-polygon exact
- * queries grouped by leaf bucket (edge records staged in shared memory once
- * per bucket); 0 runs the per-point tiers (for A/B measurements).  Values take
- * effect for work enqueued after the call. */
+ * GAHHG_KNOB_GROUPED_PASS2: 1 (default) puts the points that pass 1 of a
+ * single-polygon exact query could not label in order of their leaves before
+ * the crossing tests run (when there are enough of them); 0 keeps them in
+ * input order (for A/B measurements).  Labels are the same either way.
+ * Values take effect for work enqueued after the call. */
 typedef enum {
-    GAHHG_KNOB_GROUPED_PASS2 = 1
+    GAHHG_KNOB_GROUPED_PASS2 = 1,
+    /* Bounded waits and loops, lowered by tests to make them run out (never
+     * needed otherwise; 0 or more, defaults in brackets):
+     * WALK_STEP_LIMIT     cells an edge walk of the hierarchy visits before it
+     *                     stops and counts a walk_limit_hit [65,536];
+     * SCAN_SPIN_LIMIT     polls a build scan's look-back waits for an earlier
+     *                     tile before summing that tile's inputs itself
+     *                     (counted in scan_fallbacks) [4,194,304];
+     * STAGING_POLL_LIMIT  polls a pass-1 block waits for the bulk copy of the
+     *                     coarse summary before reading it from global memory
+     *                     (counted by gahhg_staging_fallbacks) [1,048,576]. */
+    GAHHG_KNOB_WALK_STEP_LIMIT = 2,
+    GAHHG_KNOB_SCAN_SPIN_LIMIT = 3,
+    GAHHG_KNOB_STAGING_POLL_LIMIT = 4
 } gahhg_knob;
 gahhg_status gahhg_set_knob(int knob, long long value);
 long long gahhg_get_knob(int knob);

@@ -150,3 +150,20 @@ def test_exact_oracle_agrees_with_reference_on_shipped_queries(oracle_ref, input
         lab = e.query_lonlat(q)
         want = ref_outputs.get("labels", name)
         assert int(((lab == 2) != (want == 2)).sum()) == known.get(name, 0), name
+
+
+def test_knobs_host_side():
+    """gahhg_set_knob: defaults, accepted ranges, refusals (host only)."""
+    import gahhg_b200 as G
+    assert G.get_knob(G.KNOB_GROUPED_PASS2) == 1
+    assert G.get_knob(G.KNOB_WALK_STEP_LIMIT) == 1 << 16
+    assert G.get_knob(G.KNOB_SCAN_SPIN_LIMIT) == 1 << 22
+    assert G.get_knob(G.KNOB_STAGING_POLL_LIMIT) == 1 << 20
+    for k, bad in [(G.KNOB_GROUPED_PASS2, 2), (G.KNOB_WALK_STEP_LIMIT, -1), (G.KNOB_SCAN_SPIN_LIMIT, 1 << 23),
+                   (0, 1), (99, 1)]:
+        with pytest.raises(G.GahhgError):
+            G.set_knob(k, bad)
+    old = G.set_knob(G.KNOB_WALK_STEP_LIMIT, 1)
+    assert G.get_knob(G.KNOB_WALK_STEP_LIMIT) == 1
+    G.set_knob(G.KNOB_WALK_STEP_LIMIT, old)
+    assert G.get_knob(G.KNOB_WALK_STEP_LIMIT) == 1 << 16

@@ -1,11 +1,11 @@
-"""Pass 2 grouped by leaf bucket (k_group: bucket counts, scan, scatter, then
-each bucket's edge records staged in shared memory by one bulk copy) against
-the per-point tiers it replaces (knob GAHHG_KNOB_GROUPED_PASS2 = 0): the same
-labels and the same per-tier escalation counts, for both precisions, on
-near-edge points of the 1.1M-edge C1 polygon (dense buckets, staged records)
-and on uniform points (sparse buckets, records from global memory), and on
-the shipped NA0 polygon.  Labels are also checked against the exact oracle
-where it is cheap.  Reference boundary loop: source/GPISPAHHG.cu:1481-1501.
+"""The pass-1 queue put in leaf-bucket order before the tiers run
+(k_bucket_sort: counts per bucket of 64 leaves, scan, scatter) against the
+tiers over the queue in pass-1 order (knob GAHHG_KNOB_GROUPED_PASS2 = 0): the
+same labels and the same per-tier escalation counts, for both precisions, on
+near-edge points of the 1.1M-edge C1 polygon (dense buckets: sorted) and on
+uniform points and the shipped NA0 polygon (sparse: the sort is skipped).
+Labels are also checked against the exact oracle where it is cheap.
+Reference boundary loop: source/GPISPAHHG.cu:1481-1501.
 """
 import numpy as np
 import pytest
@@ -41,14 +41,15 @@ def c1_grid():
 def test_grouped_equals_per_point_c2(c1_grid, prec):
     rings, _P, g = c1_grid
     pts = synth.device_c2_points(rings, 2_000_000, 7, "cuda:0")
+    fallbacks = G.staging_fallbacks(0)
     a, sa = _run(g, pts, prec, True)
     b, sb = _run(g, pts, prec, False)
     assert np.array_equal(a, b), "%d labels differ" % int((a != b).sum())
     assert set(np.unique(a)) <= {1, 2}
     for k in ("boundary_points", "esc_fp64", "esc_exact", "in_count"):
         assert sa[k] == sb[k], (k, sa[k], sb[k])
-    assert G.staging_fallbacks(0) == 0
-    report("grouped pass 2 == per-point tiers on 2e6 C2 points (%s): boundary %d, FP32->FP64 %d, FP64->exact %d"
+    assert G.staging_fallbacks(0) == fallbacks
+    report("tiers over the leaf-ordered queue == pass-1 order on 2e6 C2 points (%s): boundary %d, FP32->FP64 %d, FP64->exact %d"
            % ("FP32 filter" if prec == G.QUERY_FP32_FILTER else "FP64 filter", sa["boundary_points"],
               sa["esc_fp64"], sa["esc_exact"]))
 
