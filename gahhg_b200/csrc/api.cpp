@@ -161,6 +161,9 @@ Grid::~Grid()
 static void fill_stats(Grid* g)
 {
     gahhg_stats& s = g->stats;
+    s.pv_num = g->poly->pv_num;
+    s.lattice_bytes = (long long)lattice_bytes(g->lattice);
+    if (!g->hierarchy) return;
     const Level& L = g->levels[g->gnum - 1];
     s.depth = g->gnum;
     s.pv_num = g->poly->pv_num;
@@ -173,7 +176,23 @@ static void fill_stats(Grid* g)
     s.cpu_space = 792 + 28 * g->gnum;
     s.gpu_min_space = 24 * s.vnum + 48 * s.bnum + 28 * s.cnum + 4 * s.rnum;
     s.gamma = g->gamma;
-    s.lattice_bytes = (long long)lattice_bytes(g->lattice);
+}
+
+// The hexagon hierarchy of an exact grid, built (and classified, when the
+// grid was) the first time something needs it; exact queries never do.
+static gahhg_status ensure_hierarchy(Grid* g)
+{
+    std::lock_guard<std::mutex> lock(g->hierarchy_mu);
+    if (g->hierarchy) return GAHHG_OK;
+    GAHHG_CUDA_TRY(cudaSetDevice(g->device));
+    GAHHG_TRY(grid_build(g));
+    g->hierarchy = true;
+    if (g->classified) {
+        GAHHG_TRY(grid_classify(g));
+        GAHHG_TRY(grid_prepare_query(g));
+    }
+    fill_stats(g);
+    return GAHHG_OK;
 }
 
 // process-wide knobs (gahhg_set_knob)
@@ -336,11 +355,16 @@ gahhg_status gahhg_build(const gahhg_polygon* poly, const gahhg_build_opts* opts
         delete G;
         return GAHHG_ERR_CUDA;
     }
-    gahhg_status s = grid_build(g);
-    if (s == GAHHG_OK && o.semantics == GAHHG_SEMANTICS_EXACT) {
+    gahhg_status s = GAHHG_OK;
+    if (o.semantics == GAHHG_SEMANTICS_EXACT) {
+        // the exact index alone: the hierarchy waits until something needs it
         const double t0 = now_seconds();
-        s = lattice_build(g);
+        s = grid_alloc_common(g);
+        if (s == GAHHG_OK) s = lattice_build(g);
         g->stats.lattice_s = now_seconds() - t0;
+    } else {
+        s = grid_build(g);
+        g->hierarchy = s == GAHHG_OK;
     }
     if (s != GAHHG_OK) {
         delete G;
@@ -355,8 +379,14 @@ gahhg_status gahhg_classify(gahhg_grid* G)
 {
     if (!G) return GAHHG_ERR_ARG;
     GAHHG_CUDA_TRY(cudaSetDevice(G->g.device));
-    GAHHG_TRY(grid_classify(&G->g));
-    GAHHG_TRY(grid_prepare_query(&G->g));
+    {
+        std::lock_guard<std::mutex> lock(G->g.hierarchy_mu);
+        if (G->g.hierarchy) {
+            GAHHG_TRY(grid_classify(&G->g));
+            GAHHG_TRY(grid_prepare_query(&G->g));
+        }
+        G->g.classified = true;  // an exact grid without its hierarchy is query-ready
+    }
     fill_stats(&G->g);
     return GAHHG_OK;
 }
@@ -377,7 +407,10 @@ static gahhg_status run_query(Grid* g, const double* d_lonlat, size_t n, uint8_t
     }
     if (precision == GAHHG_QUERY_AUTO)
         precision = g->lattice ? GAHHG_QUERY_FP32_FILTER : GAHHG_QUERY_REFERENCE_FP64;
-    if (precision == GAHHG_QUERY_REFERENCE_FP64) return grid_query_ref(g, d_lonlat, n, d_labels, s, d_counters);
+    if (precision == GAHHG_QUERY_REFERENCE_FP64) {
+        GAHHG_TRY(ensure_hierarchy(g));
+        return grid_query_ref(g, d_lonlat, n, d_labels, s, d_counters);
+    }
     if (precision == GAHHG_QUERY_FP32_FILTER || precision == GAHHG_QUERY_FP64_FILTER) {
         if (!g->lattice) {
             set_error("exact precision needs a grid built with GAHHG_SEMANTICS_EXACT");
@@ -548,11 +581,16 @@ gahhg_status gahhg_stats_get(const gahhg_grid* G, gahhg_stats* s)
     return GAHHG_OK;
 }
 
-int gahhg_grid_depth(const gahhg_grid* G) { return G ? G->g.gnum : 0; }
+int gahhg_grid_depth(const gahhg_grid* G)
+{
+    if (!G || ensure_hierarchy(const_cast<Grid*>(&G->g)) != GAHHG_OK) return 0;
+    return G->g.gnum;
+}
 
 gahhg_status gahhg_grid_export(const gahhg_grid* G, int* levels, double* v, void* b, void* c, int* refs)
 {
     if (!G) return GAHHG_ERR_ARG;
+    GAHHG_TRY(ensure_hierarchy(const_cast<Grid*>(&G->g)));
     const Grid* g = &G->g;
     const Level& L = g->levels[g->gnum - 1];
     GAHHG_CUDA_TRY(cudaSetDevice(g->device));
@@ -580,6 +618,7 @@ gahhg_status gahhg_report_append(const gahhg_grid* G, const char* polyfile, cons
                                  const char* path, int dest_stdout)
 {
     if (!G) return GAHHG_ERR_ARG;
+    GAHHG_TRY(ensure_hierarchy(const_cast<Grid*>(&G->g)));
     const gahhg_stats& s = G->g.stats;
     FILE* fp = stdout;
     if (!dest_stdout) {

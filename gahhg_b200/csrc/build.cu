@@ -532,6 +532,15 @@ static gahhg_status dispatch_last(Grid* g)
     return GAHHG_OK;
 }
 
+gahhg_status grid_alloc_common(Grid* g)
+{
+    if (!g->d_err) GAHHG_CUDA_TRY(cudaMalloc(&g->d_err, sizeof(DeviceErrors)));
+    if (!g->d_counts) GAHHG_CUDA_TRY(cudaMalloc(&g->d_counts, 64 * sizeof(int)));
+    if (!g->h_counts) GAHHG_CUDA_TRY(cudaMallocHost(&g->h_counts, 64 * sizeof(int)));
+    GAHHG_CUDA_TRY(cudaMemsetAsync(g->d_err, 0, sizeof(DeviceErrors), g->stream));
+    return GAHHG_OK;
+}
+
 gahhg_status grid_build(Grid* g)
 {
     cudaStream_t s = g->stream;

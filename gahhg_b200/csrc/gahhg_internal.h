@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -192,10 +193,15 @@ struct Grid {
     gahhg_stats stats{};
     bool classified = false;
     bool borrowed = false;        // stream and scan state belong to a batch worker
+    // the hexagon hierarchy exists (always for reference semantics; for exact
+    // semantics built on first need: report, export, depth, FP64 reference query)
+    bool hierarchy = false;
+    std::mutex hierarchy_mu;
 
     ~Grid();
 };
 
+gahhg_status grid_alloc_common(Grid* g);  // device error word and count buffers
 gahhg_status grid_build(Grid* g);
 gahhg_status grid_classify(Grid* g);
 gahhg_status grid_query_ref(Grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels, cudaStream_t s,

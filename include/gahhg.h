@@ -128,9 +128,12 @@ void gahhg_points_free(gahhg_points* p);
 /* ---- build / classify --------------------------------------------------- */
 
 /* GPISP::createAHHGInit + createAHHG (source/GPISPAHHG.cu:1947-2015): the
- * level-synchronous refinement on the GPU plus the bottom-level edge lists;
- * for GAHHG_SEMANTICS_EXACT also the exact-label lattice.  The polygon must
- * outlive the grid. */
+ * level-synchronous refinement on the GPU plus the bottom-level edge lists.
+ * For GAHHG_SEMANTICS_EXACT the build makes the exact-label lattice, which
+ * exact queries use alone; the hexagon hierarchy is then built (and
+ * classified) the first time gahhg_report_append, gahhg_grid_export,
+ * gahhg_grid_depth or a GAHHG_QUERY_REFERENCE_FP64 query needs it, and until
+ * then its fields of gahhg_stats are 0.  The polygon must outlive the grid. */
 gahhg_status gahhg_build(const gahhg_polygon* poly, const gahhg_build_opts* opts, gahhg_grid** out);
 /* GPISP::classifyAHHG (source/GPISPAHHG.cu:2018-2059). */
 gahhg_status gahhg_classify(gahhg_grid* g);

@@ -2,9 +2,10 @@
 gahhg_set_knob lowered), on the GPU, without a fault:
 
   walk step limit      every edge walk of the hierarchy stops after one cell:
-                       the build completes and counts the walks
-                       (walk_limit_hits); the exact labels do not depend on
-                       the hierarchy and stay equal to the exact oracle's;
+                       the build completes, counts the walks (walk_limit_hits)
+                       and still answers reference-precision queries; an
+                       exact grid's labels do not depend on the hierarchy and
+                       stay equal to the exact oracle's;
   scan look-back       every build scan's look-back gives up at once on a late
                        tile and sums that tile's inputs itself: the grids are
                        bit-identical to a normal build's (scan_fallbacks
@@ -42,13 +43,15 @@ def knob(k, v):
 def test_walk_step_limit_runs_out(inputs, tmp_path):
     path = inputs.polygon_file("various/NA0.txt", tmp_path)
     P = G.Polygon.from_file(path)
-    g0 = G.Grid(P, semantics=G.SEMANTICS_EXACT, device=0).classify()
+    q = inputs.query("uniform")
+    g0 = G.Grid(P, semantics=G.SEMANTICS_REFERENCE, device=0).classify()
     assert g0.stats()["walk_limit_hits"] == 0
     with knob(G.KNOB_WALK_STEP_LIMIT, 1):
+        gr = G.Grid(P, semantics=G.SEMANTICS_REFERENCE, device=0).classify()
         g = G.Grid(P, semantics=G.SEMANTICS_EXACT, device=0).classify()
-    st = g.stats()
-    assert st["walk_limit_hits"] > 0
-    q = inputs.query("uniform")
+        assert g.depth > 0  # the exact grid's hierarchy, built now, under the same limit
+    assert gr.stats()["walk_limit_hits"] > 0 and g.stats()["walk_limit_hits"] > 0
+    assert set(np.unique(gr.query(q, G.QUERY_REFERENCE_FP64))) <= {0, 1, 2}
     xyz, pe = P.export()
     want = exact.ExactPolygon(xyz, pe, len(inputs.rings_deg("various/NA0.txt")[0])).query_lonlat(q)
     assert np.array_equal(g.query(q, G.QUERY_FP32_FILTER), want)
