@@ -696,7 +696,8 @@ __global__ void k_leaf_flags(int nn, const int* cnt, const int* child_base, int*
 __global__ void k_leaf_records(BuildView v, int lvl, int nn, const int* is_leaf, const int* leaf_off,
                                const int* rec_off, int leaf_base, long long rec_base, const long long* ix,
                                const long long* iy, const int* cnt, const int* off, const int* list,
-                               const uint8_t* label, LeafRec* leaves, float4* recs, uint32_t* eids, int* bad)
+                               const uint8_t* label, LeafRec* leaves, float4* recs, uint32_t* eids, double* leafR,
+                               int* bad)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nn || !is_leaf[p]) return;
@@ -711,6 +712,15 @@ __global__ void k_leaf_records(BuildView v, int lvl, int nn, const int* is_leaf,
     L.label = label[p];
     L.pad = 0;
     leaves[leaf_base + leaf_off[p]] = L;
+    {
+        // the center's canonical XYZ, bit for bit as the query would compute it
+        double Rq[3];
+        gahhg_canon_vertex_xyz(L.lon, L.lat, Rq);
+        double* dst = leafR + 3 * (size_t)(leaf_base + leaf_off[p]);
+        dst[0] = Rq[0];
+        dst[1] = Rq[1];
+        dst[2] = Rq[2];
+    }
     if (cnt[p] > 65535) atomicAdd(bad + 2, 1);
     local_frame::Basis fb;
     local_frame::basis_at(c.lonc, c.latc, fb);
@@ -802,6 +812,7 @@ struct QueryView {
     const float4* recs;       // per record: the FP32 tier's tangent-frame ends
     const uint32_t* eids;     // per record: edge id | (orient(A, B, R) > 0) << 31
     const double2* ends;      // per edge: A.xy, A.z B.x, B.yz (48 B, one aligned load each)
+    const double* leafR;      // per leaf: the center's canonical XYZ (3 doubles), as leaf_label computes it
     const D3* pv;
     const int* pe;
     int nleaves;              // leaves of the index (buckets of 2^GROUP_SHIFT for the grouped pass 2)
@@ -996,27 +1007,53 @@ __host__ __device__ __forceinline__ uint32_t summary_bytes(int swords) { return 
 // that produced it.
 constexpr uint8_t LABEL_DEFER = 0xFF;
 
-__device__ uint8_t leaf_label_fp32(const QueryView& Q, uint32_t leaf, const PointCtx& P)
+// Tier 1 runs every edge of the leaf: a decided edge adds its crossing to
+// the parity, an undecided one is noted in `mask` (bit k for record k < 31)
+// and the FP64 tier evaluates only those, starting from the parity of the
+// decided ones (bit 31).  The label is exact either way: the crossing parity
+// is the XOR of independent per-edge tests.  MASK_ALL asks tier 2 for every
+// edge (a record beyond the 31st undecided, or the offset refused).
+constexpr uint32_t MASK_ALL = 0xFFFFFFFFu;
+
+__device__ uint8_t leaf_label_fp32(const QueryView& Q, uint32_t leaf, const PointCtx& P, uint32_t& mask)
 {
     const LeafRec L = Q.leaves[leaf];
     local_frame::Offset o;
-    if (!(fabs(P.lon) <= 540.0) || !local_frame::offset(P.lon, P.lat, L.lon, L.lat, o)) return LABEL_DEFER;
+    if (!(fabs(P.lon) <= 540.0) || !local_frame::offset(P.lon, P.lat, L.lon, L.lat, o)) {
+        mask = MASK_ALL;
+        return LABEL_DEFER;
+    }
     local_frame::Frame f;
     local_frame::project(o, f);
     int par = 0;
+    uint32_t und = 0;
+    bool all = false;
     for (int k = 0; k < L.cnt; k++) {
         // stored order: orient(A, B, R) = +1, so a crossing needs s2 = -1,
         // s3 = orient(R, q, A) = -1 and s4 = orient(R, q, B) = +1
         const float4 r = __ldg(Q.recs + L.off + k);
-        const int s2 = local_frame::sign_edge(f, r.x, r.y, r.z, r.w);
-        if (s2 == 0) return LABEL_DEFER;
-        if (s2 > 0) continue;
-        const int s3 = local_frame::sign_end(f, r.x, r.y);
-        if (s3 == 0) return LABEL_DEFER;
-        if (s3 > 0) continue;
-        const int s4 = local_frame::sign_end(f, r.z, r.w);
-        if (s4 == 0) return LABEL_DEFER;
-        if (s4 > 0) par ^= 1;
+        int s = local_frame::sign_edge(f, r.x, r.y, r.z, r.w);
+        if (s < 0) {
+            s = local_frame::sign_end(f, r.x, r.y);
+            if (s < 0) {
+                s = local_frame::sign_end(f, r.z, r.w);
+                if (s > 0) par ^= 1;
+            }
+        }
+        if (s == 0) {
+            if (k < 31)
+                und |= 1u << k;
+            else
+                all = true;
+        }
+    }
+    if (all) {
+        mask = MASK_ALL;
+        return LABEL_DEFER;
+    }
+    if (und) {
+        mask = und | ((uint32_t)par << 31);
+        return LABEL_DEFER;
     }
     return (uint8_t)(par ? 3 - L.label : L.label);
 }
@@ -1026,22 +1063,39 @@ __device__ uint8_t leaf_label_fp32(const QueryView& Q, uint32_t leaf, const Poin
 // before the first sign is evaluated, instead of one dependent chain per edge.
 constexpr int T2_GROUP = 4;
 
-__device__ uint8_t leaf_label_fp64(const QueryView& Q, uint32_t leaf, PointCtx& P)
+// FP64 tier on the leaf's records selected by `mask` (MASK_ALL: every record,
+// parity from 0; else the records of bits 0..30, parity from bit 31).
+__device__ uint8_t leaf_label_fp64(const QueryView& Q, uint32_t leaf, PointCtx& P, uint32_t mask = MASK_ALL)
 {
     const LeafRec L = Q.leaves[leaf];
     P.need64();
-    double LR[3];
-    gahhg_canon_vertex_xyz(L.lon, L.lat, LR);
+    const double LR[3] = {__ldg(Q.leafR + 3 * (size_t)leaf), __ldg(Q.leafR + 3 * (size_t)leaf + 1),
+                          __ldg(Q.leafR + 3 * (size_t)leaf + 2)};
+    const bool all = mask == MASK_ALL;
     const int cnt = L.cnt;
-    int par = 0;
-    for (int k0 = 0; k0 < cnt; k0 += T2_GROUP) {
+    int par = all ? 0 : (int)(mask >> 31);
+    uint32_t sel = all ? 0u : (mask & 0x7fffffffu);
+    for (int k0 = 0; all ? k0 < cnt : sel != 0u; k0 += T2_GROUP) {
+        // the next T2_GROUP records: consecutive ones, or the next set bits of sel
+        int kk[T2_GROUP];
+#pragma unroll
+        for (int j = 0; j < T2_GROUP; j++) {
+            if (all) {
+                kk[j] = k0 + j < cnt ? k0 + j : -1;
+            } else if (sel) {
+                kk[j] = __ffs(sel) - 1;
+                sel &= sel - 1u;
+            } else {
+                kk[j] = -1;
+            }
+        }
         uint32_t es[T2_GROUP];
         double2 e[T2_GROUP][3];
 #pragma unroll
-        for (int j = 0; j < T2_GROUP; j++) es[j] = k0 + j < cnt ? __ldg(Q.eids + L.off + k0 + j) : 0u;
+        for (int j = 0; j < T2_GROUP; j++) es[j] = kk[j] >= 0 ? __ldg(Q.eids + L.off + kk[j]) : 0u;
 #pragma unroll
         for (int j = 0; j < T2_GROUP; j++) {
-            if (k0 + j < cnt) {
+            if (kk[j] >= 0) {
                 const double2* p = Q.ends + 3 * (size_t)(es[j] & 0x7fffffffu);
                 e[j][0] = __ldg(p);
                 e[j][1] = __ldg(p + 1);
@@ -1050,7 +1104,7 @@ __device__ uint8_t leaf_label_fp64(const QueryView& Q, uint32_t leaf, PointCtx& 
         }
 #pragma unroll
         for (int j = 0; j < T2_GROUP; j++) {
-            if (k0 + j >= cnt) break;
+            if (kk[j] < 0) break;
             const int s1 = (es[j] >> 31) ? 1 : -1;
             const double A[3] = {e[j][0].x, e[j][0].y, e[j][1].x}, B[3] = {e[j][1].y, e[j][2].x, e[j][2].y};
             if (exact::same(P.q, A) || exact::same(P.q, B)) return CELL_IN;  // vertex rule
@@ -1453,6 +1507,7 @@ struct Tiers {
     uint32_t* l1;
     uint32_t* l2;
     uint32_t* l3;
+    uint32_t* m2;   // per tier-2 entry: tier 1's mask of undecided records (leaf_label_fp32)
     unsigned int* cnt;
     unsigned int cap2, cap3;
     // the pass-1 queue in leaf-bucket order (k_bucket_sort), used by the first
@@ -1498,7 +1553,7 @@ struct ChunkViews {
 // Appends i to q through counter *c, one atomic per group of converged
 // threads; false when the queue is full.
 __device__ __forceinline__ bool push_deferred(uint32_t i, uint32_t w, uint32_t* q, uint32_t* l, unsigned int* c,
-                                              unsigned int cap)
+                                              unsigned int cap, uint32_t* extra = nullptr, uint32_t x = 0u)
 {
     const unsigned int act = __activemask();
     const int lane = threadIdx.x & 31;
@@ -1510,6 +1565,7 @@ __device__ __forceinline__ bool push_deferred(uint32_t i, uint32_t w, uint32_t* 
     if (pos >= cap) return false;
     q[pos] = i;
     l[pos] = w;
+    if (extra) extra[pos] = x;
     return true;
 }
 
@@ -1544,10 +1600,11 @@ __global__ void __launch_bounds__(TPB) k_leaf_t1(VS vs, const double2* __restric
             lab = (uint8_t)(w & 3u);
         } else {
             boundary++;
-            lab = leaf_label_fp32(Q, w & INDEX_MASK, P);
+            uint32_t mask = 0;
+            lab = leaf_label_fp32(Q, w & INDEX_MASK, P, mask);
             if (lab == LABEL_DEFER) {
                 fp64++;
-                if (!push_deferred(i, w, T.q2, T.l2, T.cnt, T.cap2)) T.cnt[2] = 1;
+                if (!push_deferred(i, w, T.q2, T.l2, T.cnt, T.cap2, T.m2, mask)) T.cnt[2] = 1;
                 continue;
             }
         }
@@ -1582,7 +1639,7 @@ __global__ void __launch_bounds__(TPB) k_leaf_t2(VS vs, const double2* __restric
             lab = (uint8_t)(w & 3u);
         } else {
             if (FROM_PASS1) boundary++;
-            lab = leaf_label_fp64(Q, w & INDEX_MASK, P);
+            lab = leaf_label_fp64(Q, w & INDEX_MASK, P, FROM_PASS1 ? MASK_ALL : T.m2[t]);
             if (lab == LABEL_DEFER) {
                 exact++;
                 if (!push_deferred(i, w, T.q3, T.l3, T.cnt + 1, T.cap3)) T.cnt[2] = 1;
@@ -1796,19 +1853,39 @@ __global__ void __launch_bounds__(S_TPB, S_BLOCKS_PER_SM)
             __syncthreads();
             bool bad = false;
             if (s_ok) {
+                // S_SCATTER / S_TPB entries per thread, every load and atomic of
+                // the batch issued before the first result is used
+                constexpr int PER = 8;
                 const unsigned int c = (unsigned int)(item - nsc - nscan);
-                const unsigned int e1 = min(m, (c + 1) * (unsigned int)S_SCATTER);
-                for (unsigned int t = c * S_SCATTER + tid; t < e1; t += S_TPB) {
-                    const uint32_t w = l1[t];
-                    const uint32_t b = group_bucket(w, nb);
-                    const unsigned int lo = __ldcg(S.boff + b), hi = __ldcg(S.boff + b + 1);
-                    const unsigned int r = atomicSub(S.hist + b, 1u);
-                    if (r == 0u || lo + r - 1u >= hi || hi > m) {
+                for (int half = 0; half < S_SCATTER / S_TPB; half += PER) {
+                const unsigned int t0 = c * S_SCATTER + (unsigned int)half * S_TPB + tid;
+                uint32_t w[PER], b[PER];
+                unsigned int r[PER], lo[PER], hi[PER];
+#pragma unroll
+                for (int k = 0; k < PER; k++) {
+                    const unsigned int t = t0 + (unsigned int)k * S_TPB;
+                    w[k] = t < m ? l1[t] : 0u;
+                    b[k] = group_bucket(w[k], nb);
+                }
+#pragma unroll
+                for (int k = 0; k < PER; k++)
+                    r[k] = t0 + (unsigned int)k * S_TPB < m ? atomicSub(S.hist + b[k], 1u) : 0u;
+#pragma unroll
+                for (int k = 0; k < PER; k++) {
+                    lo[k] = __ldcg(S.boff + b[k]);
+                    hi[k] = __ldcg(S.boff + b[k] + 1);
+                }
+#pragma unroll
+                for (int k = 0; k < PER; k++) {
+                    const unsigned int t = t0 + (unsigned int)k * S_TPB;
+                    if (t >= m) continue;
+                    if (r[k] == 0u || lo[k] + r[k] - 1u >= hi[k] || hi[k] > m) {
                         bad = true;  // counts and entries disagree: never write out of the bucket
                         continue;
                     }
-                    S.spts[lo + r - 1u] = queue[t];
-                    S.sleaf[lo + r - 1u] = w;
+                    S.spts[lo[k] + r[k] - 1u] = queue[t];
+                    S.sleaf[lo[k] + r[k] - 1u] = w[k];
+                }
                 }
             }
             if (__syncthreads_or(bad) && tid == 0) atomicExch(S.sync + 4, 1u);
@@ -1884,6 +1961,7 @@ struct Lattice {
     DevArray<float4> recs;
     DevArray<uint32_t> eids;
     DevArray<double2> ends;
+    DevArray<double> leafR;
     DevArray<uint32_t> summary;
     int cshift = 0, swords = 0;
     long long nedges = 0;
@@ -1901,6 +1979,7 @@ void lattice_free(Lattice* L)
     L->recs.release();
     L->eids.release();
     L->ends.release();
+    L->leafR.release();
     L->summary.release();
     delete L;
 }
@@ -1908,7 +1987,7 @@ void lattice_free(Lattice* L)
 size_t lattice_bytes(const Lattice* L)
 {
     if (!L) return 0;
-    return L->nnodes * sizeof(uint32_t) + L->nleaves * sizeof(LeafRec) +
+    return L->nnodes * sizeof(uint32_t) + L->nleaves * (sizeof(LeafRec) + 3 * sizeof(double)) +
            L->nrecs * (sizeof(float4) + sizeof(uint32_t)) + L->nedges * 3 * sizeof(double2);
 }
 
@@ -1916,7 +1995,8 @@ size_t lattice_device_bytes(const Lattice* L)
 {
     if (!L) return 0;
     return L->nodes.cap * sizeof(uint32_t) + L->leaves.cap * sizeof(LeafRec) + L->recs.cap * sizeof(float4) +
-           L->eids.cap * sizeof(uint32_t) + L->ends.cap * sizeof(double2) + L->summary.cap * sizeof(uint32_t);
+           L->eids.cap * sizeof(uint32_t) + L->ends.cap * sizeof(double2) + L->summary.cap * sizeof(uint32_t) +
+           L->leafR.cap * sizeof(double);
 }
 
 namespace {
@@ -2496,6 +2576,7 @@ gahhg_status lattice_build(Grid* g)
     GAHHG_TRY(L->leaves.reserve(leaf_total + 1, s, false));
     GAHHG_TRY(L->recs.reserve(std::max(rec_total, 1LL), s, false));
     GAHHG_TRY(L->eids.reserve(std::max(rec_total, 1LL), s, false));
+    GAHHG_TRY(L->leafR.reserve(3 * (size_t)std::max(leaf_total, 1LL), s, false));
     GAHHG_TRY(L->ends.reserve(3 * (size_t)std::max(n, 1), s, false));
     L->nleaves = leaf_total;
     L->nrecs = rec_total;
@@ -2506,7 +2587,8 @@ gahhg_status lattice_build(Grid* g)
         k_leaf_records<<<blocks_for(b.nn), TPB, 0, s>>>(bv, lvl, b.nn, is_leaf[lvl].ptr, leaf_off[lvl].ptr,
                                                         rec_off[lvl].ptr, leaf_base[lvl], rec_base[lvl], b.ix.ptr,
                                                         b.iy.ptr, b.cnt.ptr, b.off.ptr, b.list.ptr, b.label.ptr,
-                                                        L->leaves.ptr, L->recs.ptr, L->eids.ptr, d_bad);
+                                                        L->leaves.ptr, L->recs.ptr, L->eids.ptr, L->leafR.ptr,
+                                                        d_bad);
     }
     GAHHG_CUDA_TRY(cudaGetLastError());
     GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
@@ -2574,6 +2656,7 @@ QueryView make_view(const Grid* g)
     Q.recs = L->recs.ptr;
     Q.eids = L->eids.ptr;
     Q.ends = L->ends.ptr;
+    Q.leafR = L->leafR.ptr;
     Q.pv = g->poly->d_pv;
     Q.pe = g->poly->d_pe;
     Q.cshift = L->cshift;
@@ -2598,7 +2681,8 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
     // at +33..35, k_bucket_sort's sync words at +36..41)][bucket counts: nb + 1]
     // [pad to 8 bytes][scan look-back words: 2 per scan item][bucket offsets:
     // nb + 2][pass-2 leaf words: chunk][tier-2 queue][its leaf words][tier-3
-    // queue][its leaf words][sorted points: chunk][sorted leaf words: chunk].
+    // queue][its leaf words][tier-2 masks][sorted points: chunk][sorted leaf
+    // words: chunk].
     // One memset per pass clears the control words, counts and look-back words.
     unsigned int cap2 = 0, cap3 = 0;
     tier_caps(chunk, &cap2, &cap3);
@@ -2609,7 +2693,7 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
     const size_t status_at = (hist_at + (grouped ? nb + 1 : 0) + 1) & ~(size_t)1;
     const size_t boff_at = status_at + 2 * nscan;
     const size_t l1_at = boff_at + (grouped ? nb + 2 : 0);
-    const size_t sorted_at = l1_at + (size_t)chunk + 2 * ((size_t)cap2 + cap3);
+    const size_t sorted_at = l1_at + (size_t)chunk + 3 * (size_t)cap2 + 2 * (size_t)cap3;
     const size_t words = sorted_at + (grouped ? 2 * (size_t)chunk : 0);
     uint32_t* queue = nullptr;
     GAHHG_TRY(pool_alloc((void**)&queue, sizeof(uint32_t) * words, g->device, s));
@@ -2621,6 +2705,7 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
     T.l2 = T.q2 + cap2;
     T.q3 = T.l2 + cap2;
     T.l3 = T.q3 + cap3;
+    T.m2 = T.l3 + cap3;
     T.cap2 = cap2;
     T.cap3 = cap3;
     GroupScratch G;
@@ -2801,7 +2886,7 @@ size_t batch_queue_words(long long queue_cap)
 {
     unsigned int cap2 = 0, cap3 = 0;
     tier_caps(queue_cap, &cap2, &cap3);
-    return 2 * ((size_t)queue_cap + cap2 + cap3);
+    return 2 * ((size_t)queue_cap + cap2 + cap3) + cap2;
 }
 
 // counters: [0] queue count, [1] next chunk, [2..4] tier counters.  The
@@ -2835,6 +2920,7 @@ gahhg_status batch_query_launch(const void* d_views, const void* d_chunks, int n
     T.l2 = T.q2 + T.cap2;
     T.q3 = T.l2 + T.cap2;
     T.l3 = T.q3 + T.cap3;
+    T.m2 = T.l3 + T.cap3;
     T.cnt = counters + 2;
     const int polls = (int)knob(GAHHG_KNOB_STAGING_POLL_LIMIT);
     if (ctr)
