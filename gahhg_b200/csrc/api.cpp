@@ -198,8 +198,10 @@ static gahhg_status ensure_hierarchy(Grid* g)
 // process-wide knobs (gahhg_set_knob)
 namespace {
 constexpr int KNOB_COUNT = 8;
-constexpr long long KNOB_DEFAULT[KNOB_COUNT] = {0, 1, 1 << 16, 1 << 22, 1 << 20, 0, 0, 0};  // index = gahhg_knob
-std::atomic<long long> g_knobs[KNOB_COUNT] = {0, 1, 1 << 16, 1 << 22, 1 << 20, 0, 0, 0};
+constexpr long long KNOB_DEFAULT[KNOB_COUNT] = {0, 0, 1 << 16, 1 << 22, 1 << 20, 0, 0, 0};  // index = gahhg_knob
+std::atomic<long long> g_knobs[KNOB_COUNT] = {0, 0, 1 << 16, 1 << 22, 1 << 20, 0, 0, 0};
+// on/off knobs (0 or 1) rather than limits
+inline bool knob_is_switch(int k) { return k == GAHHG_KNOB_GROUPED_PASS2; }
 }  // namespace
 
 long long knob(int k) { return (k > 0 && k < KNOB_COUNT) ? g_knobs[k].load(std::memory_order_relaxed) : 0; }
@@ -232,9 +234,8 @@ gahhg_status gahhg_set_knob(int k, long long value)
         set_error("unknown knob %d", k);
         return GAHHG_ERR_ARG;
     }
-    if (k == GAHHG_KNOB_GROUPED_PASS2 ? (value != 0 && value != 1) : (value < 0 || value > KNOB_DEFAULT[k])) {
-        set_error("knob %d takes %s, not %lld", k, k == GAHHG_KNOB_GROUPED_PASS2 ? "0 or 1" : "0 .. its default",
-                  value);
+    if (knob_is_switch(k) ? (value != 0 && value != 1) : (value < 0 || value > KNOB_DEFAULT[k])) {
+        set_error("knob %d takes %s, not %lld", k, knob_is_switch(k) ? "0 or 1" : "0 .. its default", value);
         return GAHHG_ERR_ARG;
     }
     gahhg::g_knobs[k].store(value, std::memory_order_relaxed);

@@ -1310,20 +1310,25 @@ __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t*
             }
         }
         if (__any_sync(0xffffffffu, any)) {
+            // one atomic on the queue counter per warp and tile: every thread of
+            // the grid pushes through this one counter, and where most points
+            // are queued (points near the edges) the counter itself limits pass 1
+            unsigned int total = 0;
+#pragma unroll
+            for (int k = 0; k < UNROLL; k++) total += __popc(__ballot_sync(0xffffffffu, push[k]));
+            unsigned int pos = 0;
+            if (lane == 0) pos = atomicAdd(qcount, total);
+            pos = __shfl_sync(0xffffffffu, pos, 0);
 #pragma unroll
             for (int k = 0; k < UNROLL; k++) {
-                const unsigned int mask = __ballot_sync(0xffffffffu, push[k]);
-                if (!mask) continue;
-                unsigned int pos = 0;
-                const int leader = __ffs(mask) - 1;
-                if (lane == leader) pos = atomicAdd(qcount, (unsigned int)__popc(mask));
-                pos = __shfl_sync(0xffffffffu, pos, leader);
+                const unsigned int mk = __ballot_sync(0xffffffffu, push[k]);
                 if (push[k]) {
-                    const unsigned int at = pos + __popc(mask & ((1u << lane) - 1u));
+                    const unsigned int at = pos + __popc(mk & ((1u << lane) - 1u));
                     queue[at] = (uint32_t)(first + base + k * TPB + threadIdx.x);
                     // w is the leaf word, or KIND_PURE (LEAF_UNKNOWN) for an unlocated point
                     if (leafq) leafq[at] = w[k];
                 }
+                pos += __popc(mk);
             }
         }
 #pragma unroll
@@ -1579,37 +1584,71 @@ __device__ __forceinline__ void count_stats(unsigned long long* ctr, int inside,
 
 // Tier 1 over the pass-1 queue.
 template <class VS>
-__global__ void __launch_bounds__(TPB) k_leaf_t1(VS vs, const double2* __restrict__ ll, uint8_t* __restrict__ out,
+__global__ void __launch_bounds__(TPB, 5) k_leaf_t1(VS vs, const double2* __restrict__ ll, uint8_t* __restrict__ out,
                                                 const uint32_t* __restrict__ queue,
                                                 const unsigned int* __restrict__ qcount, Tiers T,
                                                 unsigned long long* ctr)
 {
+    __shared__ unsigned int s_wcnt[TPB / 32];
+    __shared__ unsigned int s_base;
     wait_for_predecessor();
     const unsigned int m = *qcount;
     const uint32_t* src = queue;
     const uint32_t* src_leaf = T.l1;
     first_tier_source(T, src, src_leaf);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int inside = 0, boundary = 0, fp64 = 0;
-    for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
-        const uint32_t i = src[t];
-        const QueryView& Q = vs.of(i);
-        PointCtx P;
-        const uint32_t w = point_leaf(Q, ll[i], P, src_leaf[t]);
-        uint8_t lab;
-        if ((w & KIND_MASK) == KIND_PURE) {
-            lab = (uint8_t)(w & 3u);
-        } else {
-            boundary++;
-            uint32_t mask = 0;
-            lab = leaf_label_fp32(Q, w & INDEX_MASK, P, mask);
+    // block-uniform loop: the deferred points of a block's round take one
+    // atomic on the tier-2 counter (about half the points defer on near-edge
+    // inputs, and one counter serves the whole grid)
+    for (unsigned int b0 = blockIdx.x * blockDim.x; b0 < m; b0 += gridDim.x * blockDim.x) {
+        const unsigned int t = b0 + threadIdx.x;
+        bool defer = false;
+        uint32_t i = 0, w = 0, mask = 0;
+        if (t < m) {
+            i = src[t];
+            const QueryView& Q = vs.of(i);
+            PointCtx P;
+            w = point_leaf(Q, ll[i], P, src_leaf[t]);
+            uint8_t lab;
+            if ((w & KIND_MASK) == KIND_PURE) {
+                lab = (uint8_t)(w & 3u);
+            } else {
+                boundary++;
+                lab = leaf_label_fp32(Q, w & INDEX_MASK, P, mask);
+            }
             if (lab == LABEL_DEFER) {
                 fp64++;
-                if (!push_deferred(i, w, T.q2, T.l2, T.cnt, T.cap2, T.m2, mask)) T.cnt[2] = 1;
-                continue;
+                defer = true;
+            } else {
+                out[i] = lab;
+                inside += lab == CELL_IN;
             }
         }
-        out[i] = lab;
-        inside += lab == CELL_IN;
+        const unsigned int bal = __ballot_sync(0xffffffffu, defer);
+        if (lane == 0) s_wcnt[warp] = __popc(bal);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned int tot = 0;
+            for (int k = 0; k < TPB / 32; k++) {
+                const unsigned int c = s_wcnt[k];
+                s_wcnt[k] = tot;
+                tot += c;
+            }
+            s_base = tot ? atomicAdd(T.cnt, tot) : 0u;
+        }
+        __syncthreads();
+        if (defer) {
+            const unsigned int pos = s_base + s_wcnt[warp] + __popc(bal & ((1u << lane) - 1u));
+            if (pos < T.cap2) {
+                T.q2[pos] = i;
+                T.l2[pos] = w;
+                T.m2[pos] = mask;
+            } else {
+                T.cnt[2] = 1;  // the tier-3 sweep labels it
+            }
+        }
+        __syncthreads();  // s_wcnt / s_base are rewritten next round
     }
     allow_dependents();
     if (ctr) count_stats(ctr, inside, boundary, fp64, 0);
@@ -2746,12 +2785,8 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
         const int grid = (int)std::min<long long>(tiles, (long long)sms * 8);
         uint32_t* leafq = tiers ? tiers->l1 : nullptr;
         const int polls = (int)knob(GAHHG_KNOB_STAGING_POLL_LIMIT);
-        if (ctr)
-            k_locate<true><<<grid, TPB, summary_bytes(Q.swords), s>>>(ll, m, d_labels + off, Q, queue, leafq, qcount,
-                                                                      ctr, polls);
-        else
-            k_locate<false><<<grid, TPB, summary_bytes(Q.swords), s>>>(ll, m, d_labels + off, Q, queue, leafq,
-                                                                       qcount, ctr, polls);
+        auto kl = ctr ? k_locate<true> : k_locate<false>;
+        kl<<<grid, TPB, summary_bytes(Q.swords), s>>>(ll, m, d_labels + off, Q, queue, leafq, qcount, ctr, polls);
         if (tiers && grp) {
             // the pass-1 queue in leaf-bucket order, then the tiers over it
             launch_dependent_tpb(k_bucket_sort, sms * S_BLOCKS_PER_SM, S_TPB, s, (const uint32_t*)queue,

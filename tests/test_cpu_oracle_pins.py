@@ -155,7 +155,7 @@ def test_exact_oracle_agrees_with_reference_on_shipped_queries(oracle_ref, input
 def test_knobs_host_side():
     """gahhg_set_knob: defaults, accepted ranges, refusals (host only)."""
     import gahhg_b200 as G
-    assert G.get_knob(G.KNOB_GROUPED_PASS2) == 1
+    assert G.get_knob(G.KNOB_GROUPED_PASS2) == 0
     assert G.get_knob(G.KNOB_WALK_STEP_LIMIT) == 1 << 16
     assert G.get_knob(G.KNOB_SCAN_SPIN_LIMIT) == 1 << 22
     assert G.get_knob(G.KNOB_STAGING_POLL_LIMIT) == 1 << 20
