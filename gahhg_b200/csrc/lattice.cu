@@ -82,15 +82,18 @@ constexpr long long NODE_BUDGET = 1LL << 27;
 constexpr long long PAIR_BUDGET = 1LL << 30;
 
 // Leaf: its center as the lon/lat it was placed at (R = their canonical XYZ,
-// recomputed where needed), its edge records and its center's label.
-struct __align__(8) LeafRec {
+// recomputed where needed), its edge records, its center's label, and the
+// sine and cosine of the center's canonical latitude rounded to float (the
+// FP32 tier's frame, local_frame::frame_at).  32 bytes: one sector.
+struct __align__(16) LeafRec {
     double lon, lat;
     uint32_t off;
     uint16_t cnt;
     uint8_t label;
     uint8_t pad;
+    float sb, cb;
 };
-static_assert(sizeof(LeafRec) == 24, "LeafRec");
+static_assert(sizeof(LeafRec) == 32, "LeafRec");
 
 // (leaf, edge) records of the FP32 tier: float4 (a1, a2, b1, b2), the edge's
 // ends in the leaf's tangent frame (local_frame::edge_record), ordered so that
@@ -711,6 +714,12 @@ __global__ void k_leaf_records(BuildView v, int lvl, int nn, const int* is_leaf,
     L.cnt = (uint16_t)min(cnt[p], 65535);
     L.label = label[p];
     L.pad = 0;
+    {
+        double sb, cb;
+        gahhg_canon_sincos(gahhg_canon_rad(L.lat), &sb, &cb);
+        L.sb = (float)sb;
+        L.cb = (float)cb;
+    }
     leaves[leaf_base + leaf_off[p]] = L;
     {
         // the center's canonical XYZ, bit for bit as the query would compute it
@@ -856,11 +865,7 @@ __device__ uint8_t leaf_label(const QueryView& Q, uint32_t leaf, PointCtx& P, bo
     double LR[3];
     gahhg_canon_vertex_xyz(L.lon, L.lat, LR);
     local_frame::Frame f;
-    if (fp32) {
-        local_frame::Offset o;
-        fp32 = fabs(P.lon) <= 540.0 && local_frame::offset(P.lon, P.lat, L.lon, L.lat, o);
-        if (fp32) local_frame::project(o, f);
-    }
+    if (fp32) fp32 = fabs(P.lon) <= 540.0 && local_frame::frame_at(P.lon, P.lat, L.lon, L.lat, L.sb, L.cb, f);
     if (!fp32) P.need64();
     unsigned long long* c64 = ctr ? ctr + 0 : nullptr;
     unsigned long long* cx = ctr ? ctr + 1 : nullptr;
@@ -1015,36 +1020,54 @@ constexpr uint8_t LABEL_DEFER = 0xFF;
 // edge (a record beyond the 31st undecided, or the offset refused).
 constexpr uint32_t MASK_ALL = 0xFFFFFFFFu;
 
-__device__ uint8_t leaf_label_fp32(const QueryView& Q, uint32_t leaf, const PointCtx& P, uint32_t& mask)
+// Records whose loads tier 1 issues together (one group covers a leaf of
+// the default leaf size): the first group goes out before the offset's
+// arithmetic, so its latency hides behind the sines and cosines.
+constexpr int T1_GROUP = 4;
+constexpr int T1_BLOCKS = 5;  // blocks per SM of tier 1 (registers)
+
+__device__ __forceinline__ uint8_t leaf_label_fp32(const QueryView& Q, const LeafRec& L, const PointCtx& P,
+                                                 uint32_t& mask)
 {
-    const LeafRec L = Q.leaves[leaf];
-    local_frame::Offset o;
-    if (!(fabs(P.lon) <= 540.0) || !local_frame::offset(P.lon, P.lat, L.lon, L.lat, o)) {
+    const float4* rec = Q.recs + L.off;
+    const int cnt = L.cnt;
+    float4 r[T1_GROUP];
+#pragma unroll
+    for (int j = 0; j < T1_GROUP; j++) r[j] = j < cnt ? __ldg(rec + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+    local_frame::Frame f;
+    if (!(fabs(P.lon) <= 540.0) || !local_frame::frame_at(P.lon, P.lat, L.lon, L.lat, L.sb, L.cb, f)) {
         mask = MASK_ALL;
         return LABEL_DEFER;
     }
-    local_frame::Frame f;
-    local_frame::project(o, f);
     int par = 0;
     uint32_t und = 0;
     bool all = false;
-    for (int k = 0; k < L.cnt; k++) {
-        // stored order: orient(A, B, R) = +1, so a crossing needs s2 = -1,
-        // s3 = orient(R, q, A) = -1 and s4 = orient(R, q, B) = +1
-        const float4 r = __ldg(Q.recs + L.off + k);
-        int s = local_frame::sign_edge(f, r.x, r.y, r.z, r.w);
-        if (s < 0) {
-            s = local_frame::sign_end(f, r.x, r.y);
-            if (s < 0) {
-                s = local_frame::sign_end(f, r.z, r.w);
-                if (s > 0) par ^= 1;
-            }
+    for (int k0 = 0; k0 < cnt; k0 += T1_GROUP) {
+        if (k0 > 0) {
+#pragma unroll
+            for (int j = 0; j < T1_GROUP; j++)
+                r[j] = k0 + j < cnt ? __ldg(rec + k0 + j) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        if (s == 0) {
-            if (k < 31)
-                und |= 1u << k;
-            else
-                all = true;
+#pragma unroll
+        for (int j = 0; j < T1_GROUP; j++) {
+            const int k = k0 + j;
+            if (k >= cnt) break;
+            // stored order: orient(A, B, R) = +1, so a crossing needs s2 = -1,
+            // s3 = orient(R, q, A) = -1 and s4 = orient(R, q, B) = +1
+            int sg = local_frame::sign_edge(f, r[j].x, r[j].y, r[j].z, r[j].w);
+            if (sg < 0) {
+                sg = local_frame::sign_end(f, r[j].x, r[j].y);
+                if (sg < 0) {
+                    sg = local_frame::sign_end(f, r[j].z, r[j].w);
+                    if (sg > 0) par ^= 1;
+                }
+            }
+            if (sg == 0) {
+                if (k < 31)
+                    und |= 1u << k;
+                else
+                    all = true;
+            }
         }
     }
     if (all) {
@@ -1313,6 +1336,8 @@ __device__ __forceinline__ void locate_range(const QueryView& Q, const uint32_t*
             // one atomic on the queue counter per warp and tile: every thread of
             // the grid pushes through this one counter, and where most points
             // are queued (points near the edges) the counter itself limits pass 1
+            // (one per block and tile, which takes block-wide barriers, made
+            // uniform points 14 % slower and near-edge points 2 % faster)
             unsigned int total = 0;
 #pragma unroll
             for (int k = 0; k < UNROLL; k++) total += __popc(__ballot_sync(0xffffffffu, push[k]));
@@ -1584,10 +1609,10 @@ __device__ __forceinline__ void count_stats(unsigned long long* ctr, int inside,
 
 // Tier 1 over the pass-1 queue.
 template <class VS>
-__global__ void __launch_bounds__(TPB, 5) k_leaf_t1(VS vs, const double2* __restrict__ ll, uint8_t* __restrict__ out,
-                                                const uint32_t* __restrict__ queue,
-                                                const unsigned int* __restrict__ qcount, Tiers T,
-                                                unsigned long long* ctr)
+__global__ void __launch_bounds__(TPB, T1_BLOCKS) k_leaf_t1(VS vs, const double2* __restrict__ ll,
+                                                         uint8_t* __restrict__ out, const uint32_t* __restrict__ queue,
+                                                         const unsigned int* __restrict__ qcount, Tiers T,
+                                                         unsigned long long* ctr)
 {
     __shared__ unsigned int s_wcnt[TPB / 32];
     __shared__ unsigned int s_base;
@@ -1615,7 +1640,7 @@ __global__ void __launch_bounds__(TPB, 5) k_leaf_t1(VS vs, const double2* __rest
                 lab = (uint8_t)(w & 3u);
             } else {
                 boundary++;
-                lab = leaf_label_fp32(Q, w & INDEX_MASK, P, mask);
+                lab = leaf_label_fp32(Q, Q.leaves[w & INDEX_MASK], P, mask);
             }
             if (lab == LABEL_DEFER) {
                 fp64++;
@@ -1973,8 +1998,7 @@ void leaf_tiers_launch(const VS& vs, const double2* ll, uint8_t* out, const uint
         launch_dependent(k_leaf_t2<VS, true>, sms * 4, s, vs, ll, out, queue, (const uint32_t*)T.l1, qcount,
                          0xffffffffu, T, ctr);
     } else {
-        // tier 1 (46 registers) fills five blocks per SM: +7 % on near-edge points
-        launch_dependent(k_leaf_t1<VS>, sms * 5, s, vs, ll, out, queue, qcount, T, ctr);
+        launch_dependent(k_leaf_t1<VS>, sms * T1_BLOCKS, s, vs, ll, out, queue, qcount, T, ctr);
         launch_dependent(k_leaf_t2<VS, false>, sms * 4, s, vs, ll, out, (const uint32_t*)T.q2,
                          (const uint32_t*)T.l2, (const unsigned int*)T.cnt, T.cap2, T, ctr);
     }

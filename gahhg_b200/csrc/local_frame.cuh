@@ -5,24 +5,32 @@
 // on the canonical FP64 XYZ of the query q, the leaf center R and the edge
 // (A, B).  Evaluating them on an FP32 copy of q bounds the error by FP32's
 // resolution on the unit sphere (~1e-7 rad), so every point closer than that
-// to an edge would escalate.  Here the offset d = q - R is computed in FP32
-// from the differences of the canonical radians (sum-to-product identities
-// with accurate sines of the half differences), so its error is relative to
-// |d|, about the leaf's size; the three determinants are then evaluated in
-// the tangent frame of R (see edge_record below), where an edge is four
-// floats and the query two coordinates and q . R.
+// to an edge would escalate.  Here q is expressed in the tangent frame of R
+// (see edge_record below) directly from the angle differences to R, so the
+// error of its frame coordinates is relative to their size (about the leaf's
+// size); an edge is four floats in the same frame.
 //
-// Error bound of the offset (u = 2^-24).  With h = half the canonical
-// differences, m the midpoints reduced to [-pi, pi]: |fl(m) - m| <= u pi;
-// sinf/cosf are within 2 ulp (CUDA's documented bound; the host functions are
-// tighter), so each of sin/cos(m) and of sin(a), cos(a), cos(b0) is within
-// 7.2e-7 absolutely, sin(h) within 3u relatively; each component of d is then
-// within KAPPA * (|hA| + |hB|) + DELTA of the offset of the canonical points
-// (worst case about 2e-6 * (|hA| + |hB|)), where DELTA covers the FP64
-// rounding of the radian differences (up to +-2 pi wraps, about 6e-15) and
-// the canonical conversion's own errors.  A product of floats each rounded
-// from a value within a few FP64 ulp adds REL * (sum of |terms|).  The
-// constants carry a margin of two or more.
+// The frame coordinates (frame_at).  With canonical radians (a, b) of q and
+// (a0, b0) of R, dl = a - a0 (reduced by 2 pi), dp = b - b0 and phi = b:
+//   p1 = q.e1 = cos phi sin dl
+//   p2 = q.e2 = sin dp + sin b0 cos phi (1 - cos dl)
+//   w  = q.R  = cos dp - cos b0 cos phi (1 - cos dl)
+//   cos phi   = cos b0 cos dp - sin b0 sin dp
+// The differences dl, dp come from the degree differences in FP64 (one
+// multiplication by pi'/180, no division), so they carry an absolute error
+// E_RAD against the canonical radians' difference besides their rounding to
+// FP32.  sin, cos and 1 - cos of |x| <= 0.5 are Taylor polynomials in FP32
+// (coefficients 1/n! rounded to float, Horner's rule with explicit fmaf,
+// truncated where the next term is below 1e-11 relative).  sin b0 and cos b0
+// are stored per leaf (FP64 canonical values rounded to float).  Every step
+// is one or two FP32 roundings, and frame_at evaluates, per point, a bound on
+// each coordinate's error from the magnitudes it computed (the derivation is
+// beside the code); the bound is doubled to cover its own FP32 evaluation and
+// the second-order terms left out.
+//
+// Only explicit fmaf() calls fuse (nvcc --fmad=false, host -ffp-contract=off),
+// so the host build of this header that the soundness tests run gives the
+// device's bits.
 #pragma once
 
 #include <math.h>
@@ -38,101 +46,102 @@
 namespace gahhg {
 namespace local_frame {
 
-constexpr float KAPPA = 8.0e-6f;   // per component of d, per radian of |hA| + |hB|
-constexpr float DELTA = 3.0e-14f;  // absolute, per component of d
-constexpr float REL = 1.0e-6f;     // relative, per term of a dot product (rounding of terms and sums)
+constexpr float EPS = 5.9604645e-8f;                      // 2^-24, FP32 unit roundoff
+constexpr double RAD_PER_DEG = GAHHG_PI_TRUNC / 180.0;    // the canonical conversion's pi' / 180, rounded
 constexpr double TWO_PI_HI = 6.283185307179586;          // 2 pi rounded to double
 constexpr double TWO_PI_LO = 2.4492935982947064e-16;     // 2 pi - TWO_PI_HI
 constexpr double INV_TWO_PI = 0.15915494309189535;       // 1 / (2 pi) rounded to double
+// Absolute error of the FP64 differences against the canonical radians'
+// difference, for |lon|, |lonR| <= 540 deg: each canonical radian value is
+// within 2 ulp of x pi' / 180 (|a| <= 9.43: 4.2e-15 for both), the
+// difference and product add 3 ulp of the result, the reduction by 2 pi
+// (|k| <= 3, two-part constant) about 4e-15; 1.1e-14 in all, 3e-14 here.
+constexpr float E_RAD = 3.0e-14f;
+// Absolute floor added to each coordinate's bound: the canonical XYZ of q
+// and R differ from the exact sine/cosine points at their canonical radians
+// by a few 1e-16 per component, which moves each determinant by at most that
+// times the norm of the other rows' cross product.
+constexpr float DELTA = 3.0e-14f;
+// Relative error per term of the determinants in sign_edge / sign_end: the
+// records' rounding to float (2 eps per coordinate product) and the fmaf
+// evaluation (4 eps for sign_edge, 2 for sign_end); 10 eps here.
+constexpr float REL = 6.0e-7f;
 
-struct Offset {
-    float d[3];
-    float err;             // bound on |d_i - (q - R)_i| for each component
-    float cl, sl, cp, sp;  // cos/sin of R's longitude and latitude, each within BASIS_ERR
-};
-
-// q from (lon, lat) and R from (lonR, latR), degrees, as the canonical
-// conversion takes them (lat is the query's FakeLL latitude).  False when the
-// offset is not small (|half differences| above ~0.5 rad): the caller defers.
-LFHD bool offset(double lon, double lat, double lonR, double latR, Offset& o)
+// Taylor polynomials for |x| <= 0.5 (FP32, explicit fmaf).
+//   taylor_sin: |S - sin x| <= 2 eps |x|   (x^3 term: x3 rounded twice, P within 1.1 eps)
+//   taylor_vers: 1 - cos x, |H - (1 - cos x)| <= 5 eps H
+LFHD float taylor_sin(float x)
 {
-    const double a = gahhg_canon_rad(lon), a0 = gahhg_canon_rad(lonR);
-    const double b = gahhg_canon_rad(lat), b0 = gahhg_canon_rad(latR);
-    // the nearest multiple of 2 pi by a reciprocal product: where it can differ
-    // from the quotient's (a half-integer number of turns) |ha| ~ pi / 2, and
-    // the offset is refused below; the midpoint lands in [-pi, pi] up to ulps
-    double ta = a - a0;
-    const double k = rint(ta * INV_TWO_PI);
-    ta = (ta - k * TWO_PI_HI) - k * TWO_PI_LO;
-    const double ha = 0.5 * ta, hb = 0.5 * (b - b0);
-    if (!(fabs(ha) < 0.5 && fabs(hb) < 0.5)) return false;
-    double ma = a0 + ha;
-    ma -= TWO_PI_HI * rint(ma * INV_TWO_PI);
-    const double mb = b0 + hb;
-    const float fha = (float)ha, fhb = (float)hb, fma_ = (float)ma, fmb = (float)mb;
-    const float sma = sinf(fma_), cma = cosf(fma_);
-    const float smb = sinf(fmb), cmb = cosf(fmb);
-    const float sha = sinf(fha), shb = sinf(fhb);
-    const float cha = cosf(fha), chb = cosf(fhb);
-    const float sin_a = sma * cha + cma * sha;  // a = ma + ha
-    const float cos_a = cma * cha - sma * sha;
-    const float cos_b0 = cmb * chb + smb * shb;  // b0 = mb - hb
-    const float dc = -2.0f * smb * shb;          // cos b - cos b0
-    const float dsa = 2.0f * cma * sha;          // sin a - sin a0
-    const float dca = -2.0f * sma * sha;         // cos a - cos a0
-    o.d[0] = dc * sin_a + cos_b0 * dsa;          // cos b sin a - cos b0 sin a0
-    o.d[1] = 2.0f * cmb * shb;                   // sin b - sin b0
-    o.d[2] = dc * cos_a + cos_b0 * dca;          // cos b cos a - cos b0 cos a0
-    o.err = KAPPA * (fabsf(fha) + fabsf(fhb)) + DELTA;
-    o.sl = sma * cha - cma * sha;  // a0 = ma - ha
-    o.cl = cma * cha + sma * sha;
-    o.sp = smb * chb - cmb * shb;  // b0 = mb - hb
-    o.cp = cos_b0;
-    return true;
+    const float x2 = x * x;
+    float p = fmaf(x2, 2.7557319e-6f, -1.9841270e-4f);  //  1/9!, -1/7!
+    p = fmaf(p, x2, 8.3333333e-3f);                      //  1/5!
+    p = fmaf(p, x2, -1.6666667e-1f);                     // -1/3!
+    return fmaf(x * x2, p, x);
 }
 
-LFHD int sign_bounded(float v, float bound) { return v > bound ? 1 : (v < -bound ? -1 : 0); }
+LFHD float taylor_vers(float x)
+{
+    const float x2 = x * x;
+    float p = fmaf(x2, 2.7557319e-7f, -2.4801587e-5f);  //  1/10!, -1/8!
+    p = fmaf(p, x2, 1.3888889e-3f);                      //  1/6!
+    p = fmaf(p, x2, -4.1666667e-2f);                     // -1/4!
+    p = fmaf(p, x2, 0.5f);                               //  1/2!
+    return x2 * p;
+}
 
-// ---- the leaf's tangent frame -------------------------------------------
-//
-// With R at canonical radians (a0, b0), e1 = (cos a0, 0, -sin a0) (east) and
-// e2 = (-sin b0 sin a0, cos b0, -sin b0 cos a0) (north) complete R to a
-// right-handed orthonormal basis (det[R; e1; e2] = 1).  In it a point X has
-// coordinates (X.R, X.e1, X.e2); an edge end A with A.R > 0 is stored as its
-// gnomonic coordinates a = (A.e1, A.e2) / (A.R), and the query as
-// w = q.R = 1 + d.R and p = (d.e1, d.e2) (R.e1 = R.e2 = 0).  Then, exactly,
-//   det[A; B; q] = (A.R)(B.R) (w (a1 b2 - a2 b1) + (b1 - a1) p2 - (b2 - a2) p1)
-//   det[R; q; A] = (A.R) (p1 a2 - p2 a1)
-// (rows expanded in the basis), so an edge needs four floats.  Records are
-// stored in the order that makes orient(A, B, R) = +1; swapping A and B
-// negates det[A; B; q] and exchanges the two end tests, and the crossing test
-// (s2 != s1, s3 == s2, s4 == -s2) is symmetric under that exchange.
-//
-// Error terms beyond the offset's: the basis computed in FP32 from the sines
-// and cosines of the offset (BASIS_ERR absolutely per component) perturbs p
-// and w by BASIS_ERR (|d0| + |d1| + |d2|) each, three times over; the stored
-// coordinates are rounded from FP64 values within ~1e-16 relatively (REL per
-// product covers them and the FP32 arithmetic); R's canonical FP64 point
-// differs from the exact one at (a0, b0) by ~1e-16, which adds at most
-// 1e-16 (|p| + |a|) to an end test (END_DELTA, with a large margin) and is
-// inside the offset's DELTA for p and w.
-constexpr float BASIS_ERR = 2.0e-6f;
-constexpr float END_DELTA = 1.0e-14f;
-
+// The query's coordinates in the leaf's frame and bounds on their errors:
+// |p_i - exact| <= errp, |w - exact| <= errw.
 struct Frame {
     float p1, p2, w;
-    float errp, errw;  // bounds on |p_i - exact| and |w - exact|
+    float errp, errw;
 };
 
-LFHD void project(const Offset& o, Frame& f)
+// q at (lon, lat) degrees (lat: the query's FakeLL latitude, as the canonical
+// conversion takes it), the leaf center at (lonR, latR) degrees with sb, cb =
+// sin and cos of its canonical latitude rounded to float.  False when an
+// angle difference exceeds 0.5 rad (the caller defers to FP64); then q.R >=
+// cos 0.5 - (1 - cos 0.5) > 0.75.
+LFHD bool frame_at(double lon, double lat, double lonR, double latR, float sb, float cb, Frame& f)
 {
-    const float t = o.d[0] * o.sl + o.d[2] * o.cl;
-    f.p1 = o.d[0] * o.cl - o.d[2] * o.sl;
-    f.p2 = o.d[1] * o.cp - o.sp * t;
-    f.w = 1.0f + (o.cp * t + o.sp * o.d[1]);
-    const float dn = fabsf(o.d[0]) + fabsf(o.d[1]) + fabsf(o.d[2]);
-    f.errp = 2.0f * o.err + (3.0f * BASIS_ERR + REL) * dn;
-    f.errw = f.errp + 1.0e-7f;
+    double dl = (lon - lonR) * RAD_PER_DEG;
+    const double k = rint(dl * INV_TWO_PI);
+    dl = (dl - k * TWO_PI_HI) - k * TWO_PI_LO;
+    const double dp = (lat - latR) * RAD_PER_DEG;
+    if (!(fabs(dl) <= 0.5 && fabs(dp) <= 0.5)) return false;
+    const float xl = (float)dl, xp = (float)dp;
+    const float axl = fabsf(xl), axp = fabsf(xp);
+    // input errors against the canonical differences: rounding to float and E_RAD
+    const float etal = fmaf(axl, 1.0000001f * EPS, E_RAD), etap = fmaf(axp, 1.0000001f * EPS, E_RAD);
+    const float sp = taylor_sin(xp), hp = taylor_vers(xp), cp = 1.0f - hp;
+    const float sl = taylor_sin(xl), hl = taylor_vers(xl);
+    // cos phi = cos b0 cos dp - sin b0 sin dp
+    const float m1 = sb * sp;
+    const float cf = fmaf(cb, cp, -m1);
+    const float t = cf * hl;  // cos phi (1 - cos dl)
+    f.p1 = cf * sl;
+    f.p2 = fmaf(sb, t, sp);
+    f.w = fmaf(-cb, t, cp);
+    // Error bounds (first order; |sb|, |cb| <= 1, |xl|, |xp| <= 0.5):
+    //  es_p = |sp - sin dp| <= 2 eps |xp| + etap     (sin is 1-Lipschitz)
+    //  ec_p = |cp - cos dp| <= 2 eps + |xp| etap     (1 - hp: one rounding, 5 eps hp <= 0.62 eps)
+    //  es_l = |sl - sin dl| <= 2 eps |xl| + etal
+    //  eh_l = |hl - (1 - cos dl)| <= 5 eps hl + |xl| etal
+    //  stored sb, cb: within eps |.| + 3e-16 of sin b0, cos b0
+    //  E_cf = |cf - cos phi| <= eps |cf| + eps |m1| + (eps |cb| + |cb| ec_p) + (eps |sb sp| + |sb| es_p)
+    //       <= eps (|cf| + 2 |m1| + 3 |cb| + 2 |xp|) + 1.5 etap + 1e-15
+    //  |p1 - p1*| <= eps |p1| + E_cf |sl| + |cf| es_l
+    //  |t - t*|   <= eps |t| + E_cf hl + |cf| eh_l
+    //  |p2 - p2*| <= eps |p2| + eps |t| + |t - t*| + es_p
+    //  |w - w*|   <= eps |w| + ec_p + eps |t| + |t - t*|
+    const float acf = fabsf(cf), at = fabsf(t);
+    const float ecf = fmaf(EPS, acf + 2.0f * fabsf(m1) + 3.0f * fabsf(cb) + 2.0f * axp, fmaf(1.5f, etap, 1.0e-15f));
+    const float ep1 = EPS * fabsf(f.p1) + ecf * fabsf(sl) + acf * fmaf(2.0f * EPS, axl, etal);
+    const float et = EPS * at + ecf * hl + acf * fmaf(5.0f * EPS, hl, axl * etal);
+    const float ep2 = EPS * (fabsf(f.p2) + at) + et + fmaf(2.0f * EPS, axp, etap);
+    const float ew = EPS * (fabsf(f.w) + at) + et + fmaf(axp, etap, 2.0f * EPS);
+    f.errp = fmaf(2.0f, fmaxf(ep1, ep2), DELTA);
+    f.errw = fmaf(2.0f, ew, DELTA);
+    return true;
 }
 
 // The tangent frame at the center (canonical radians of its degrees), FP64.
@@ -174,25 +183,39 @@ LFHD void edge_record(const double* A, const double* B, const Basis& f, bool swa
     }
 }
 
-// sign det[A; B; q] for a record (a1, a2, b1, b2) in its stored order.
+LFHD int sign_bounded(float v, float bound) { return v > bound ? 1 : (v < -bound ? -1 : 0); }
+
+// sign det[A; B; q] for a record (a1, a2, b1, b2) in its stored order:
+// v = w (a1 b2 - a2 b1) + (b1 - a1) p2 - (b2 - a2) p1.  Its error: the
+// frame's, errp (|u1| + |u2|) + errw |c|, and REL times
+// S = |w| (|a1 b2| + |a2 b1|) + (|a1| + |b1|) |p2| + (|a2| + |b2|) |p1|
+// (|a1 b2| + |a2 b1| <= |c| + 2 |a2 b1| up to a rounding).
 LFHD int sign_edge(const Frame& f, float a1, float a2, float b1, float b2)
 {
     const float u1 = b1 - a1, u2 = b2 - a2;
-    const float c = a1 * b2 - a2 * b1;
-    const float v = f.w * c + (u1 * f.p2 - u2 * f.p1);
-    const float bound = f.errp * (fabsf(u1) + fabsf(u2)) + f.errw * fabsf(c) +
-                        REL * (fabsf(f.w) * (fabsf(a1 * b2) + fabsf(a2 * b1)) + (fabsf(a1) + fabsf(b1)) * fabsf(f.p2) +
-                               (fabsf(a2) + fabsf(b2)) * fabsf(f.p1)) +
-                        1e-30f;
+    const float m = a2 * b1;
+    const float c = fmaf(a1, b2, -m);
+    const float n = u2 * f.p1;
+    const float v = fmaf(f.w, c, fmaf(u1, f.p2, -n));
+    const float S = fmaf(fabsf(f.w), fmaf(2.0f, fabsf(m), fabsf(c)),
+                         fmaf(fabsf(f.p2), fabsf(a1) + fabsf(b1), fabsf(f.p1) * (fabsf(a2) + fabsf(b2))));
+    const float bound = fmaf(f.errp, fabsf(u1) + fabsf(u2), fmaf(f.errw, fabsf(c), fmaf(REL, S, 1e-30f)));
     return sign_bounded(v, bound);
 }
 
-// sign det[R; q; X] for an end (x1, x2) of a record.
+// Canonical R against the exact frame point: at most a few 1e-16 per
+// component, which moves det[R; q; X] / (X.R) by about that times
+// |p1| + |p2| + |x1| + |x2|; END_DELTA carries a margin above 30.
+constexpr float END_DELTA = 1.0e-14f;
+
+// sign det[R; q; X] for an end (x1, x2) of a record: v = p1 x2 - p2 x1
+// (|p1 x2| + |p2 x1| <= |v| + 2 |p2 x1| up to a rounding).
 LFHD int sign_end(const Frame& f, float x1, float x2)
 {
-    const float v = f.p1 * x2 - f.p2 * x1;
-    const float bound = f.errp * (fabsf(x1) + fabsf(x2)) + REL * (fabsf(f.p1 * x2) + fabsf(f.p2 * x1)) +
-                        END_DELTA * (fabsf(x1) + fabsf(x2) + fabsf(f.p1) + fabsf(f.p2)) + 1e-30f;
+    const float n = f.p2 * x1;
+    const float v = fmaf(f.p1, x2, -n);
+    const float bound = fmaf(f.errp + END_DELTA, fabsf(x1) + fabsf(x2),
+                             fmaf(REL, fmaf(2.0f, fabsf(n), fabsf(v)), END_DELTA * (fabsf(f.p1) + fabsf(f.p2)) + 1e-30f));
     return sign_bounded(v, bound);
 }
 

@@ -35,14 +35,16 @@ extern "C" void local_signs(const double* cfg, long n, int* out)
         local_frame::Basis fb;
         local_frame::basis_at(c[2], c[3], fb);
         local_frame::edge_record(A, B, fb, swap, r);
-        local_frame::Offset o;
+        // the leaf record's sine and cosine of the center's canonical latitude
+        double sb, cb;
+        gahhg_canon_sincos(gahhg_canon_rad(c[3]), &sb, &cb);
+        local_frame::Frame f;
         int* s = out + 3 * i;
-        if (s1 == 0 || !local_frame::offset(c[0], gahhg_canon_query_lat(c[1]), c[2], c[3], o)) {
+        if (s1 == 0 || !(fabs(c[0]) <= 540.0) ||
+            !local_frame::frame_at(c[0], gahhg_canon_query_lat(c[1]), c[2], c[3], (float)sb, (float)cb, f)) {
             s[0] = s[1] = s[2] = 9;
             continue;
         }
-        local_frame::Frame f;
-        local_frame::project(o, f);
         const int e = local_frame::sign_edge(f, r[0], r[1], r[2], r[3]);
         const int ea = local_frame::sign_end(f, r[0], r[1]), eb = local_frame::sign_end(f, r[2], r[3]);
         s[0] = swap ? -e : e;
