@@ -824,14 +824,9 @@ struct QueryView {
     const double* leafR;      // per leaf: the center's canonical XYZ (3 doubles), as leaf_label computes it
     const D3* pv;
     const int* pe;
-    int nleaves;              // leaves of the index (buckets of 2^GROUP_SHIFT for the grouped pass 2)
-    int nbuckets;             // ceil(nleaves / 2^GROUP_SHIFT)
+    int nparts;               // windows of consecutive leaves the pass-2 queue is ordered by (1: none)
+    float part_scale;         // window of leaf i: floor(i * part_scale), clamped to nparts - 1
 };
-
-// Pass 2 groups the queued points by bucket of 2^GROUP_SHIFT consecutive
-// leaves: their records are contiguous in memory, so one bulk copy stages
-// every edge record a bucket's points test.
-constexpr int GROUP_SHIFT = 6;
 
 struct PointCtx {
     double lon, lat;      // input longitude and FakeLL latitude (canonical XYZ)
@@ -865,7 +860,9 @@ __device__ uint8_t leaf_label(const QueryView& Q, uint32_t leaf, PointCtx& P, bo
     double LR[3];
     gahhg_canon_vertex_xyz(L.lon, L.lat, LR);
     local_frame::Frame f;
+    local_frame::Tests ft;
     if (fp32) fp32 = fabs(P.lon) <= 540.0 && local_frame::frame_at(P.lon, P.lat, L.lon, L.lat, L.sb, L.cb, f);
+    if (fp32) local_frame::tests_of(f, ft);
     if (!fp32) P.need64();
     unsigned long long* c64 = ctr ? ctr + 0 : nullptr;
     unsigned long long* cx = ctr ? ctr + 1 : nullptr;
@@ -878,11 +875,11 @@ __device__ uint8_t leaf_label(const QueryView& Q, uint32_t leaf, PointCtx& P, bo
         int s2 = 0, ea = 0, eb = 0;
         if (fp32) {
             const float4 r = __ldg(Q.recs + L.off + k);
-            s2 = s1 * local_frame::sign_edge(f, r.x, r.y, r.z, r.w);
+            s2 = s1 * local_frame::sign_edge(ft, r.x, r.y, r.z, r.w);
             const float x1 = s1 > 0 ? r.x : r.z, x2 = s1 > 0 ? r.y : r.w;
             const float y1 = s1 > 0 ? r.z : r.x, y2 = s1 > 0 ? r.w : r.y;
-            ea = local_frame::sign_end(f, x1, x2);
-            eb = local_frame::sign_end(f, y1, y2);
+            ea = local_frame::sign_end(ft, x1, x2);
+            eb = local_frame::sign_end(ft, y1, y2);
         }
         double A[3], B[3];
         bool haveAB = false;
@@ -1024,7 +1021,7 @@ constexpr uint32_t MASK_ALL = 0xFFFFFFFFu;
 // the default leaf size): the first group goes out before the offset's
 // arithmetic, so its latency hides behind the sines and cosines.
 constexpr int T1_GROUP = 4;
-constexpr int T1_BLOCKS = 5;  // blocks per SM of tier 1 (registers)
+constexpr int T1_BLOCKS = 4;  // blocks per SM of tier 1 (registers)
 
 __device__ __forceinline__ uint8_t leaf_label_fp32(const QueryView& Q, const LeafRec& L, const PointCtx& P,
                                                  uint32_t& mask)
@@ -1039,6 +1036,8 @@ __device__ __forceinline__ uint8_t leaf_label_fp32(const QueryView& Q, const Lea
         mask = MASK_ALL;
         return LABEL_DEFER;
     }
+    local_frame::Tests t;
+    local_frame::tests_of(f, t);
     int par = 0;
     uint32_t und = 0;
     bool all = false;
@@ -1052,17 +1051,9 @@ __device__ __forceinline__ uint8_t leaf_label_fp32(const QueryView& Q, const Lea
         for (int j = 0; j < T1_GROUP; j++) {
             const int k = k0 + j;
             if (k >= cnt) break;
-            // stored order: orient(A, B, R) = +1, so a crossing needs s2 = -1,
-            // s3 = orient(R, q, A) = -1 and s4 = orient(R, q, B) = +1
-            int sg = local_frame::sign_edge(f, r[j].x, r[j].y, r[j].z, r[j].w);
-            if (sg < 0) {
-                sg = local_frame::sign_end(f, r[j].x, r[j].y);
-                if (sg < 0) {
-                    sg = local_frame::sign_end(f, r[j].z, r[j].w);
-                    if (sg > 0) par ^= 1;
-                }
-            }
-            if (sg == 0) {
+            const int x = local_frame::record_crossing(t, r[j].x, r[j].y, r[j].z, r[j].w);
+            if (x > 0) par ^= 1;
+            if (x < 0) {
                 if (k < 31)
                     und |= 1u << k;
                 else
@@ -1540,15 +1531,15 @@ struct Tiers {
     uint32_t* m2;   // per tier-2 entry: tier 1's mask of undecided records (leaf_label_fp32)
     unsigned int* cnt;
     unsigned int cap2, cap3;
-    // the pass-1 queue in leaf-bucket order (k_bucket_sort), used by the first
+    // the pass-1 queue in window order (k_part_scatter), used by the first
     // tier when *sorted == 1
     const uint32_t* spts = nullptr;
     const uint32_t* sleaf = nullptr;
     const unsigned int* sorted = nullptr;
 };
 
-// The pass-1 queue as the first tier reads it: in leaf-bucket order when
-// k_bucket_sort completed, else in pass-1 order.
+// The pass-1 queue as the first tier reads it: in window order when
+// k_part_scatter ran, else in pass-1 order.
 __device__ __forceinline__ void first_tier_source(const Tiers& T, const uint32_t*& pts, const uint32_t*& leaf)
 {
     if (T.sorted && *(const volatile unsigned int*)T.sorted == 1u) {
@@ -1751,218 +1742,137 @@ __global__ void __launch_bounds__(TPB) k_leaf_t3(VS vs, const double2* __restric
     if (ctr) count_inside(inside, ctr + 3);
 }
 
-// ------------------------------------------- pass-2 queue in leaf order --
+// ------------------------------------- pass-2 queue in leaf-window order --
 //
 // Pass 1 queues points in input order, so on inputs without spatial order
-// (C2's near-edge points) neighbouring threads of the tiers test unrelated
-// leaves, and every point gathers its leaf's records from an index larger than
-// L2.  k_bucket_sort puts the queue in order of bucket of 2^GROUP_SHIFT
-// consecutive leaves (whose records are contiguous in memory) before the
-// tiers run, so that a warp's points share a handful of leaves and a block's
-// tile of the queue spans a short, contiguous range of records.  One
-// persistent launch; its blocks take work items in order from a counter:
-//   count items    queue entries counted per bucket;
-//   scan items     after every count item finished: exclusive scan of the
-//                  counts (decoupled look-back between the items);
-//   scatter items  after every scan item finished: entries written to their
-//                  bucket's range of the sorted point and leaf-word arrays.
-// A block waits only on items that blocks which started before it hold (items
-// are taken in order), and every wait is bounded: a wait that runs out marks
-// the sort failed and the tiers read the queue in pass-1 order.  The sort is
-// skipped (the tiers read pass-1 order) when the queue holds fewer than
-// SORT_RATIO entries per bucket: sparse buckets gain nothing from it.
-constexpr int S_TPB = 256;
-constexpr int S_SCAN = S_TPB * 8;         // buckets per scan item
-constexpr int S_SCATTER = S_TPB * 16;     // queue entries per count / scatter item
-constexpr int SORT_RATIO = 4;
-constexpr int S_WAIT_LIMIT = 1 << 22;     // polls (about 0.5 s) before a wait gives up
-constexpr int S_BLOCKS_PER_SM = 4;
+// (C2's near-edge points) the tiers' gathers of leaf and edge records sweep
+// the whole index, which is larger than L2 (350-400 MB on the C1 polygon):
+// nearly every record comes from DRAM, once per point.  Leaves are numbered
+// so that their records are contiguous, so a window of consecutive leaves is
+// a contiguous slice of the index.  Two launches put the queue in window
+// order (a counting sort with a few dozen bins, block-aggregated):
+//   k_part_count    entries per window (shared-memory counts, one global
+//                   atomic per window and block);
+//   k_part_scatter  each block ranks a tile's entries per window in shared
+//                   memory, takes the tile's place in each window with one
+//                   global atomic per window, and writes them there.
+// The tiers' grid-stride loops then sweep the queue in order, so at any time
+// the grid works in one or two windows whose records stay in L2, and tier 1
+// writes the tier-2 queue in the same order.  Windows are sized at about
+// PART_BYTES of index; queues below PART_MIN_QUEUE entries keep pass-1 order
+// (both kernels return at once and the tiers read the pass-1 queue).
+constexpr int PART_MAX = 64;
+constexpr long long PART_BYTES = 24LL << 20;
+constexpr unsigned int PART_MIN_QUEUE = 1u << 18;
+constexpr int P_TPB = 256;
+constexpr int P_ITEMS = 8;
 
-struct GroupScratch {
-    unsigned int* hist;           // [nb + 1] queued points per bucket (bucket nb: no leaf word); zero
-    unsigned long long* status;   // [nscan] scan look-back words (value | flag << 32); zero
-    unsigned int* boff;           // [nb + 2] bucket offsets in the sorted arrays
-    uint32_t* spts;               // sorted point indices
-    uint32_t* sleaf;              // sorted leaf words
-    unsigned int* sync;           // [0] next item, [1] count, [2] scan, [3] scatter items done, [4] failed,
-                                  // [5] 1 when the sorted arrays are complete; zero before the pass
-    int nb;
+struct PartScratch {
+    unsigned int* total;   // [PART_MAX] entries per window; zero before the pass
+    unsigned int* cursor;  // [PART_MAX] entries placed per window; zero before the pass
+    unsigned int* done;    // set to 1 when the window-ordered arrays are complete; zero before the pass
+    uint32_t* spts;        // point indices in window order
+    uint32_t* sleaf;       // their leaf words
+    int np;                // windows (>= 2)
+    float scale;           // QueryView::part_scale
 };
 
-__host__ __device__ inline int group_scan_items(int nb) { return (nb + 1 + S_SCAN - 1) / S_SCAN; }
-__host__ __device__ inline bool group_worth_sorting(unsigned int m, int nb)
+__device__ __forceinline__ int part_of(uint32_t w, int np, float scale)
 {
-    return (unsigned long long)m >= (unsigned long long)SORT_RATIO * (unsigned long long)(nb + 1);
+    if ((w & KIND_MASK) != KIND_LEAF) return np - 1;  // a point pass 1 did not locate
+    return min((int)(__uint2float_rz(w & INDEX_MASK) * scale), np - 1);
 }
 
-__device__ __forceinline__ uint32_t group_bucket(uint32_t w, int nb)
+// Adds one per active lane to cnt[b] in shared memory, one atomic per group
+// of lanes with the same b; returns the lane's rank (old value + position).
+__device__ __forceinline__ unsigned int smem_rank(unsigned int* cnt, int b)
 {
-    return (w & KIND_MASK) == KIND_LEAF ? min((w & INDEX_MASK) >> GROUP_SHIFT, (uint32_t)nb) : (uint32_t)nb;
+    const unsigned int act = __activemask();
+    const unsigned int same = __match_any_sync(act, b);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(same) - 1;
+    unsigned int base = 0;
+    if (lane == leader) base = atomicAdd(cnt + b, (unsigned int)__popc(same));
+    base = __shfl_sync(same, base, leader);
+    return base + __popc(same & ((1u << lane) - 1u));
 }
 
-// Thread 0: bounded wait until *p >= target.
-__device__ __forceinline__ bool wait_count(const unsigned int* p, unsigned int target)
+__global__ void __launch_bounds__(P_TPB) k_part_count(const uint32_t* __restrict__ l1,
+                                                      const unsigned int* __restrict__ qcount, PartScratch S)
 {
-    for (int i = 0; i < S_WAIT_LIMIT; i++) {
-        if (*(const volatile unsigned int*)p >= target) {
-            __threadfence();
-            return true;
-        }
-        __nanosleep(128);
-    }
-    return false;
-}
-
-__global__ void __launch_bounds__(S_TPB, S_BLOCKS_PER_SM)
-    k_bucket_sort(const uint32_t* __restrict__ queue, const uint32_t* __restrict__ l1,
-                  const unsigned int* __restrict__ qcount, GroupScratch S)
-{
-    __shared__ unsigned int s_warp[S_TPB / 32];
-    __shared__ unsigned int s_prefix;
-    __shared__ int s_item, s_ok;
+    __shared__ unsigned int s_cnt[PART_MAX];
     wait_for_predecessor();
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned int m = *qcount;
-    const int nb = S.nb;
-    const int nscan = group_scan_items(nb);
-    const int nsc = (int)((m + S_SCATTER - 1) / S_SCATTER);
-    const long long nitems = group_worth_sorting(m, nb) ? (long long)2 * nsc + nscan : 0;
-    for (;;) {
+    if (m < PART_MIN_QUEUE) {
+        allow_dependents();
+        return;
+    }
+    for (int k = threadIdx.x; k < S.np; k += P_TPB) s_cnt[k] = 0;
+    __syncthreads();
+    for (unsigned int t = blockIdx.x * P_TPB + threadIdx.x; t < m; t += gridDim.x * P_TPB)
+        smem_rank(s_cnt, part_of(l1[t], S.np, S.scale));
+    __syncthreads();
+    allow_dependents();
+    for (int k = threadIdx.x; k < S.np; k += P_TPB)
+        if (s_cnt[k]) atomicAdd(S.total + k, s_cnt[k]);
+}
+
+__global__ void __launch_bounds__(P_TPB) k_part_scatter(const uint32_t* __restrict__ queue,
+                                                        const uint32_t* __restrict__ l1,
+                                                        const unsigned int* __restrict__ qcount, PartScratch S)
+{
+    __shared__ unsigned int s_start[PART_MAX], s_cnt[PART_MAX], s_base[PART_MAX];
+    wait_for_predecessor();
+    const unsigned int m = *qcount;
+    if (m < PART_MIN_QUEUE) {
+        allow_dependents();
+        return;
+    }
+    if (threadIdx.x == 0) {
+        unsigned int run = 0;
+        for (int k = 0; k < S.np; k++) {
+            s_start[k] = run;
+            run += S.total[k];
+        }
+    }
+    for (int k = threadIdx.x; k < S.np; k += P_TPB) s_cnt[k] = 0;
+    __syncthreads();
+    constexpr int TILE = P_TPB * P_ITEMS;
+    // block-uniform loop; per tile: ranks (s_cnt), barrier, the tile's place
+    // in each window (s_base; s_cnt cleared), barrier, writes
+    for (unsigned int base = blockIdx.x * TILE; base < m; base += gridDim.x * TILE) {
+        uint32_t q[P_ITEMS], w[P_ITEMS];
+        unsigned int r[P_ITEMS];
+        int b[P_ITEMS];
+#pragma unroll
+        for (int k = 0; k < P_ITEMS; k++) {
+            const unsigned int t = base + k * P_TPB + threadIdx.x;
+            q[k] = t < m ? queue[t] : 0u;
+            w[k] = t < m ? l1[t] : 0u;
+            b[k] = part_of(w[k], S.np, S.scale);
+        }
+#pragma unroll
+        for (int k = 0; k < P_ITEMS; k++)
+            if (base + k * P_TPB + threadIdx.x < m) r[k] = smem_rank(s_cnt, b[k]);
         __syncthreads();
-        if (tid == 0) s_item = (int)atomicAdd(S.sync + 0, 1u);
+        for (int j = threadIdx.x; j < S.np; j += P_TPB) {
+            const unsigned int c = s_cnt[j];
+            if (c) s_base[j] = s_start[j] + atomicAdd(S.cursor + j, c);
+            s_cnt[j] = 0;
+        }
         __syncthreads();
-        const long long item = s_item;
-        if (item >= nitems) break;
-        if (item < nsc) {
-            // ---- count item
-            const unsigned int c = (unsigned int)item;
-            const unsigned int e1 = min(m, (c + 1) * (unsigned int)S_SCATTER);
-            for (unsigned int t = c * S_SCATTER + tid; t < e1; t += S_TPB) atomicAdd(S.hist + group_bucket(l1[t], nb), 1u);
-            __threadfence();
-            __syncthreads();
-            if (tid == 0) atomicAdd(S.sync + 1, 1u);
-        } else if (item < nsc + nscan) {
-            // ---- scan item: buckets [t * S_SCAN, ...) of hist[0 .. nb]
-            const int t = (int)(item - nsc);
-            if (tid == 0 && !wait_count(S.sync + 1, (unsigned int)nsc)) atomicExch(S.sync + 4, 1u);
-            __syncthreads();
-            const int base = t * S_SCAN + tid * 8;
-            unsigned int v[8], sum = 0;
 #pragma unroll
-            for (int k = 0; k < 8; k++) {
-                v[k] = base + k <= nb ? __ldcg(S.hist + base + k) : 0u;
-                sum += v[k];
+        for (int k = 0; k < P_ITEMS; k++) {
+            if (base + k * P_TPB + threadIdx.x >= m) continue;
+            const unsigned int at = s_base[b[k]] + r[k];
+            if (at < m) {  // counts and entries agree; never write past the queue
+                S.spts[at] = q[k];
+                S.sleaf[at] = w[k];
             }
-            unsigned int incl = sum;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const unsigned int y = __shfl_up_sync(0xffffffffu, incl, d);
-                if (lane >= d) incl += y;
-            }
-            if (lane == 31) s_warp[warp] = incl;
-            __syncthreads();
-            if (tid == 0) {
-                unsigned int run = 0;
-                for (int w = 0; w < S_TPB / 32; w++) {
-                    const unsigned int x = s_warp[w];
-                    s_warp[w] = run;
-                    run += x;
-                }
-                // run = the item's total; publish it, then look back
-                unsigned int excl = 0;
-                const unsigned long long AGG = 1ull << 32, PRE = 2ull << 32;
-                if (t == 0) {
-                    atomicExch(S.status, PRE | run);
-                } else {
-                    atomicExch(S.status + t, AGG | run);
-                    bool ok = true;
-                    for (int j = t - 1; j >= 0;) {
-                        int spins = 0;
-                        unsigned long long w;
-                        while (((w = *(const volatile unsigned long long*)(S.status + j)) >> 32) == 0ull) {
-                            if (++spins > S_WAIT_LIMIT) break;
-                            __nanosleep(64);
-                        }
-                        if ((w >> 32) == 0ull) {
-                            ok = false;
-                            break;
-                        }
-                        excl += (unsigned int)w;
-                        if ((w >> 32) == 2ull) break;
-                        j--;
-                    }
-                    if (!ok) atomicExch(S.sync + 4, 1u);
-                    atomicExch(S.status + t, PRE | (excl + run));
-                }
-                s_prefix = excl;
-                if (t == nscan - 1) S.boff[nb + 1] = excl + run;  // the total
-            }
-            __syncthreads();
-            unsigned int run = s_prefix + s_warp[warp] + incl - sum;
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-                if (base + k <= nb) S.boff[base + k] = run;
-                run += v[k];
-            }
-            __threadfence();
-            __syncthreads();
-            if (tid == 0) atomicAdd(S.sync + 2, 1u);
-        } else {
-            // ---- scatter item
-            if (tid == 0) {
-                const bool ok = wait_count(S.sync + 2, (unsigned int)nscan);
-                if (!ok) atomicExch(S.sync + 4, 1u);
-                s_ok = ok && *(volatile unsigned int*)(S.sync + 4) == 0u;
-            }
-            __syncthreads();
-            bool bad = false;
-            if (s_ok) {
-                // S_SCATTER / S_TPB entries per thread, every load and atomic of
-                // the batch issued before the first result is used
-                constexpr int PER = 8;
-                const unsigned int c = (unsigned int)(item - nsc - nscan);
-                for (int half = 0; half < S_SCATTER / S_TPB; half += PER) {
-                const unsigned int t0 = c * S_SCATTER + (unsigned int)half * S_TPB + tid;
-                uint32_t w[PER], b[PER];
-                unsigned int r[PER], lo[PER], hi[PER];
-#pragma unroll
-                for (int k = 0; k < PER; k++) {
-                    const unsigned int t = t0 + (unsigned int)k * S_TPB;
-                    w[k] = t < m ? l1[t] : 0u;
-                    b[k] = group_bucket(w[k], nb);
-                }
-#pragma unroll
-                for (int k = 0; k < PER; k++)
-                    r[k] = t0 + (unsigned int)k * S_TPB < m ? atomicSub(S.hist + b[k], 1u) : 0u;
-#pragma unroll
-                for (int k = 0; k < PER; k++) {
-                    lo[k] = __ldcg(S.boff + b[k]);
-                    hi[k] = __ldcg(S.boff + b[k] + 1);
-                }
-#pragma unroll
-                for (int k = 0; k < PER; k++) {
-                    const unsigned int t = t0 + (unsigned int)k * S_TPB;
-                    if (t >= m) continue;
-                    if (r[k] == 0u || lo[k] + r[k] - 1u >= hi[k] || hi[k] > m) {
-                        bad = true;  // counts and entries disagree: never write out of the bucket
-                        continue;
-                    }
-                    S.spts[lo[k] + r[k] - 1u] = queue[t];
-                    S.sleaf[lo[k] + r[k] - 1u] = w[k];
-                }
-                }
-            }
-            if (__syncthreads_or(bad) && tid == 0) atomicExch(S.sync + 4, 1u);
-            __threadfence();
-            __syncthreads();
-            // the last scatter item to finish declares the arrays complete (every
-            // failure was flagged before its item was counted)
-            if (tid == 0 && atomicAdd(S.sync + 3, 1u) + 1u == (unsigned int)nsc &&
-                *(volatile unsigned int*)(S.sync + 4) == 0u)
-                atomicExch(S.sync + 5, 1u);
         }
     }
     allow_dependents();
+    if (blockIdx.x == 0 && threadIdx.x == 0) *S.done = 1u;
 }
 
 // Launch with programmatic stream serialization (see wait_for_predecessor).
@@ -2695,7 +2605,7 @@ gahhg_status lattice_build(Grid* g)
 gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long long n, uint8_t* d_labels,
                                 int precision, cudaStream_t s, uint64_t* d_counters, uint32_t* queue,
                                 unsigned int* qcount, long long chunk, int device, const Tiers* tiers,
-                                const GroupScratch* grp = nullptr);
+                                const PartScratch* part = nullptr);
 
 QueryView make_view(const Grid* g)
 {
@@ -2726,8 +2636,12 @@ QueryView make_view(const Grid* g)
     Q.CW = (L->geo.W + (1 << L->cshift) - 1) >> L->cshift;
     Q.swords = L->swords;
     Q.summary = L->summary.ptr;
-    Q.nleaves = (int)L->nleaves;
-    Q.nbuckets = (int)((L->nleaves + (1 << GROUP_SHIFT) - 1) >> GROUP_SHIFT);
+    // windows of about PART_BYTES of the records the tiers gather per leaf
+    const long long tier_bytes = L->nrecs * (long long)(sizeof(float4) + sizeof(uint32_t)) +
+                                 L->nleaves * (long long)(sizeof(LeafRec) + 3 * sizeof(double));
+    Q.nparts = (int)std::min<long long>(PART_MAX, std::max<long long>(1, (tier_bytes + PART_BYTES - 1) / PART_BYTES));
+    if (L->nleaves < 2 * PART_MAX) Q.nparts = 1;
+    Q.part_scale = Q.nparts > 1 ? (float)((double)Q.nparts / (double)L->nleaves) : 0.0f;
     return Q;
 }
 
@@ -2740,24 +2654,18 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
     if (n == 0) return GAHHG_OK;
     const QueryView Q = make_view(g);
     const long long chunk = std::min<long long>((long long)n, QUERY_CHUNK);
-    // Words: [pass-2 queue: chunk][control: 64 (queue fill at +32, tier counters
-    // at +33..35, k_bucket_sort's sync words at +36..41)][bucket counts: nb + 1]
-    // [pad to 8 bytes][scan look-back words: 2 per scan item][bucket offsets:
-    // nb + 2][pass-2 leaf words: chunk][tier-2 queue][its leaf words][tier-3
-    // queue][its leaf words][tier-2 masks][sorted points: chunk][sorted leaf
-    // words: chunk].
-    // One memset per pass clears the control words, counts and look-back words.
+    // Words: [pass-2 queue: chunk][control: 192 (queue fill at +32, tier
+    // counters at +33..35, window-order flag at +36, entries per window at
+    // +64, windows' cursors at +128)][pass-2 leaf words: chunk][tier-2 queue]
+    // [its leaf words][tier-3 queue][its leaf words][tier-2 masks][queue in
+    // window order: points, leaf words (chunk each)].
+    // One memset per pass clears the control words from the queue fill on.
     unsigned int cap2 = 0, cap3 = 0;
     tier_caps(chunk, &cap2, &cap3);
-    const bool grouped = knob(GAHHG_KNOB_GROUPED_PASS2) != 0 && Q.nbuckets > 0;
-    const size_t nb = grouped ? (size_t)Q.nbuckets : 0;
-    const size_t nscan = grouped ? (size_t)group_scan_items((int)nb) : 0;
-    const size_t hist_at = (size_t)chunk + 64;
-    const size_t status_at = (hist_at + (grouped ? nb + 1 : 0) + 1) & ~(size_t)1;
-    const size_t boff_at = status_at + 2 * nscan;
-    const size_t l1_at = boff_at + (grouped ? nb + 2 : 0);
+    const bool windows = knob(GAHHG_KNOB_GROUPED_PASS2) != 0 && Q.nparts > 1 && chunk >= PART_MIN_QUEUE;
+    const size_t l1_at = (size_t)chunk + 192;
     const size_t sorted_at = l1_at + (size_t)chunk + 3 * (size_t)cap2 + 2 * (size_t)cap3;
-    const size_t words = sorted_at + (grouped ? 2 * (size_t)chunk : 0);
+    const size_t words = sorted_at + (windows ? 2 * (size_t)chunk : 0);
     uint32_t* queue = nullptr;
     GAHHG_TRY(pool_alloc((void**)&queue, sizeof(uint32_t) * words, g->device, s));
     unsigned int* qcount = (unsigned int*)(queue + chunk + 32);
@@ -2771,16 +2679,16 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
     T.m2 = T.l3 + cap3;
     T.cap2 = cap2;
     T.cap3 = cap3;
-    GroupScratch G;
-    G.sync = qcount + 4;
-    G.hist = queue + hist_at;
-    G.status = (unsigned long long*)(queue + status_at);
-    G.boff = queue + boff_at;
-    G.spts = queue + sorted_at;
-    G.sleaf = queue + sorted_at + chunk;
-    G.nb = (int)nb;
+    PartScratch W;
+    W.done = qcount + 4;
+    W.total = queue + chunk + 64;
+    W.cursor = queue + chunk + 128;
+    W.spts = queue + sorted_at;
+    W.sleaf = queue + sorted_at + chunk;
+    W.np = Q.nparts;
+    W.scale = Q.part_scale;
     const gahhg_status st = lattice_query_with(Q, d_lonlat, (long long)n, d_labels, precision, s, d_counters,
-                                               queue, qcount, chunk, g->device, &T, grouped ? &G : nullptr);
+                                               queue, qcount, chunk, g->device, &T, windows ? &W : nullptr);
     cudaFreeAsync(queue, s);
     return st;
 }
@@ -2790,7 +2698,7 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
 gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long long n, uint8_t* d_labels,
                                 int precision, cudaStream_t s, uint64_t* d_counters, uint32_t* queue,
                                 unsigned int* qcount, long long chunk, int device, const Tiers* tiers,
-                                const GroupScratch* grp)
+                                const PartScratch* part)
 {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -2798,12 +2706,9 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
     for (long long off = 0; off < n; off += chunk) {
         const int m = (int)std::min<long long>(chunk, n - off);
         const double2* ll = (const double2*)d_lonlat + off;
-        // the queue fill, the tier counters and, when sorting, k_bucket_sort's sync
-        // words, the bucket counts and the look-back words (laid out after them;
-        // the control words run to the counts)
-        const size_t zero_words =
-            grp ? (size_t)((const unsigned int*)(grp->status + group_scan_items(grp->nb)) - qcount)
-                : (tiers ? 4 : 1);
+        // the queue fill, the tier counters and, when ordering by window, the
+        // flag, the counts and the cursors (the control words run up to them)
+        const size_t zero_words = part ? (size_t)(part->cursor + PART_MAX - qcount) : (tiers ? 4 : 1);
         GAHHG_CUDA_TRY(cudaMemsetAsync(qcount, 0, sizeof(unsigned int) * zero_words, s));
         const long long tiles = ((long long)m + TPB * LOC_UNROLL - 1) / (TPB * LOC_UNROLL);
         const int grid = (int)std::min<long long>(tiles, (long long)sms * 8);
@@ -2811,14 +2716,16 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
         const int polls = (int)knob(GAHHG_KNOB_STAGING_POLL_LIMIT);
         auto kl = ctr ? k_locate<true> : k_locate<false>;
         kl<<<grid, TPB, summary_bytes(Q.swords), s>>>(ll, m, d_labels + off, Q, queue, leafq, qcount, ctr, polls);
-        if (tiers && grp) {
-            // the pass-1 queue in leaf-bucket order, then the tiers over it
-            launch_dependent_tpb(k_bucket_sort, sms * S_BLOCKS_PER_SM, S_TPB, s, (const uint32_t*)queue,
-                                 (const uint32_t*)tiers->l1, (const unsigned int*)qcount, *grp);
+        if (tiers && part) {
+            // the pass-1 queue in window order, then the tiers over it
+            launch_dependent_tpb(k_part_count, sms * 4, P_TPB, s, (const uint32_t*)tiers->l1,
+                                 (const unsigned int*)qcount, *part);
+            launch_dependent_tpb(k_part_scatter, sms * 4, P_TPB, s, (const uint32_t*)queue,
+                                 (const uint32_t*)tiers->l1, (const unsigned int*)qcount, *part);
             Tiers T = *tiers;
-            T.spts = grp->spts;
-            T.sleaf = grp->sleaf;
-            T.sorted = grp->sync + 5;
+            T.spts = part->spts;
+            T.sleaf = part->sleaf;
+            T.sorted = part->done;
             leaf_tiers_launch(OneView{Q}, ll, d_labels + off, queue, qcount, T, precision, ctr, sms, s);
         } else if (tiers) {
             leaf_tiers_launch(OneView{Q}, ll, d_labels + off, queue, qcount, *tiers, precision, ctr, sms, s);

@@ -183,40 +183,81 @@ LFHD void edge_record(const double* A, const double* B, const Basis& f, bool swa
     }
 }
 
-LFHD int sign_bounded(float v, float bound) { return v > bound ? 1 : (v < -bound ? -1 : 0); }
-
-// sign det[A; B; q] for a record (a1, a2, b1, b2) in its stored order:
-// v = w (a1 b2 - a2 b1) + (b1 - a1) p2 - (b2 - a2) p1.  Its error: the
-// frame's, errp (|u1| + |u2|) + errw |c|, and REL times
-// S = |w| (|a1 b2| + |a2 b1|) + (|a1| + |b1|) |p2| + (|a2| + |b2|) |p1|
-// (|a1 b2| + |a2 b1| <= |c| + 2 |a2 b1| up to a rounding).
-LFHD int sign_edge(const Frame& f, float a1, float a2, float b1, float b2)
-{
-    const float u1 = b1 - a1, u2 = b2 - a2;
-    const float m = a2 * b1;
-    const float c = fmaf(a1, b2, -m);
-    const float n = u2 * f.p1;
-    const float v = fmaf(f.w, c, fmaf(u1, f.p2, -n));
-    const float S = fmaf(fabsf(f.w), fmaf(2.0f, fabsf(m), fabsf(c)),
-                         fmaf(fabsf(f.p2), fabsf(a1) + fabsf(b1), fabsf(f.p1) * (fabsf(a2) + fabsf(b2))));
-    const float bound = fmaf(f.errp, fabsf(u1) + fabsf(u2), fmaf(f.errw, fabsf(c), fmaf(REL, S, 1e-30f)));
-    return sign_bounded(v, bound);
-}
-
 // Canonical R against the exact frame point: at most a few 1e-16 per
 // component, which moves det[R; q; X] / (X.R) by about that times
 // |p1| + |p2| + |x1| + |x2|; END_DELTA carries a margin above 30.
 constexpr float END_DELTA = 1.0e-14f;
 
-// sign det[R; q; X] for an end (x1, x2) of a record: v = p1 x2 - p2 x1
-// (|p1 x2| + |p2 x1| <= |v| + 2 |p2 x1| up to a rounding).
-LFHD int sign_end(const Frame& f, float x1, float x2)
+// The record tests' per-point constants.  For a record (a1, a2, b1, b2) with
+// T = |a1| + |a2| + |b1| + |b2|:
+//   s2 = sign det[A; B; q]: v2 = w c + (b1 - a1) p2 - (b2 - a2) p1,
+//        c = a1 b2 - a2 b1 = fl(a1 b2 - m), m = fl(a2 b1).  Its error is the
+//        frame's, errp (|u1| + |u2|) + errw |c|, plus REL times
+//        S = |w| (|a1 b2| + |a2 b1|) + (|a1| + |b1|) |p2| + (|a2| + |b2|) |p1|;
+//        with |u1| + |u2| <= T, |a1 b2| + |a2 b1| <= |c| + 2 |m| and
+//        S <= |w| (|c| + 2 |m|) + max(|p1|, |p2|) T (each up to a rounding,
+//        inside REL's margin) it is at most K1 T + K2 |c| + K3 |m|.
+//   s3 = sign det[R; q; A]: v3 = p1 a2 - p2 a1, error at most
+//        errp (|a1| + |a2|) + REL (|p1 a2| + |p2 a1|) + END_DELTA (|a1| + |a2| + |p1| + |p2|)
+//        <= KE (|a1| + |a2|) + DE; s4 likewise for B.
+struct Tests {
+    float p1, p2, w;
+    float K1, K2, K3;  // s2 bound: K1 T + K2 |c| + K3 |m|
+    float KE, DE;      // end bound: KE (|x1| + |x2|) + DE
+};
+
+LFHD void tests_of(const Frame& f, Tests& t)
 {
-    const float n = f.p2 * x1;
-    const float v = fmaf(f.p1, x2, -n);
-    const float bound = fmaf(f.errp + END_DELTA, fabsf(x1) + fabsf(x2),
-                             fmaf(REL, fmaf(2.0f, fabsf(n), fabsf(v)), END_DELTA * (fabsf(f.p1) + fabsf(f.p2)) + 1e-30f));
-    return sign_bounded(v, bound);
+    const float P = fmaxf(fabsf(f.p1), fabsf(f.p2)), P1 = fabsf(f.p1) + fabsf(f.p2), aw = fabsf(f.w);
+    t.p1 = f.p1;
+    t.p2 = f.p2;
+    t.w = f.w;
+    t.K1 = fmaf(REL, P, f.errp);
+    t.K2 = fmaf(REL, aw, f.errw);
+    t.K3 = 2.0f * REL * aw;
+    t.KE = fmaf(REL, P1, f.errp + END_DELTA);
+    t.DE = fmaf(END_DELTA, P1, 1e-30f);
+}
+
+LFHD int sign_bounded(float v, float bound) { return v > bound ? 1 : (v < -bound ? -1 : 0); }
+
+// sign det[A; B; q] for a record (a1, a2, b1, b2) in its stored order.
+LFHD int sign_edge(const Tests& t, float a1, float a2, float b1, float b2)
+{
+    const float u1 = b1 - a1, u2 = b2 - a2;
+    const float m = a2 * b1;
+    const float c = fmaf(a1, b2, -m);
+    const float v = fmaf(t.w, c, fmaf(u1, t.p2, -(u2 * t.p1)));
+    const float T = (fabsf(a1) + fabsf(a2)) + (fabsf(b1) + fabsf(b2));
+    return sign_bounded(v, fmaf(t.K1, T, fmaf(t.K2, fabsf(c), t.K3 * fabsf(m))));
+}
+
+// sign det[R; q; X] for an end (x1, x2) of a record.
+LFHD int sign_end(const Tests& t, float x1, float x2)
+{
+    const float v = fmaf(t.p1, x2, -(t.p2 * x1));
+    return sign_bounded(v, fmaf(t.KE, fabsf(x1) + fabsf(x2), t.DE));
+}
+
+// The crossing test of one record in its stored order (orient(A, B, R) = +1):
+// arc(R, q) crosses the edge when s2 = -1, s3 = -1 and s4 = +1.  Returns 1
+// (crossing), 0 (none: some sign rules it out, decided even when another is
+// not) or -1 (undecided).  All three signs are evaluated without branches,
+// with the bounds of sign_edge / sign_end.
+LFHD int record_crossing(const Tests& t, float a1, float a2, float b1, float b2)
+{
+    const float v3 = fmaf(t.p1, a2, -(t.p2 * a1));
+    const float v4 = fmaf(t.p1, b2, -(t.p2 * b1));
+    const float na = fabsf(a1) + fabsf(a2), nb = fabsf(b1) + fabsf(b2);
+    const float B3 = fmaf(t.KE, na, t.DE), B4 = fmaf(t.KE, nb, t.DE);
+    const float u1 = b1 - a1, u2 = b2 - a2;
+    const float m = a2 * b1;
+    const float c = fmaf(a1, b2, -m);
+    const float v2 = fmaf(t.w, c, fmaf(u1, t.p2, -(u2 * t.p1)));
+    const float B2 = fmaf(t.K1, na + nb, fmaf(t.K2, fabsf(c), t.K3 * fabsf(m)));
+    const bool none = (v2 > B2) | (v3 > B3) | (v4 < -B4);
+    const bool cross = (v2 < -B2) & (v3 < -B3) & (v4 > B4);
+    return cross ? 1 : (none ? 0 : -1);
 }
 
 }  // namespace local_frame

@@ -349,10 +349,12 @@ gahhg_status gahhg_staging_fallbacks(int device, unsigned long long* count);
 
 /* Process-wide tuning and test knobs.  No counterpart in the reference.
  * GAHHG_KNOB_GROUPED_PASS2: 1 puts the points that pass 1 of a
- * single-polygon exact query could not label in order of their leaves before
- * the crossing tests run (when there are enough of them); 0 (default) keeps
- * them in input order.  Labels are the same either way; on a B200 the sort
- * costs more than the locality it buys (measured on near-edge points).
+ * single-polygon exact query could not label in order of windows of
+ * consecutive leaves (about 24 MB of index each) before the crossing tests
+ * run, when there are enough of them and the index spans several windows;
+ * 0 (default) keeps them in input order.  Labels are the same either way; on
+ * a B200 the ordering costs more than the locality it buys (measured on
+ * near-edge points).
  * Values take effect for work enqueued after the call. */
 typedef enum {
     GAHHG_KNOB_GROUPED_PASS2 = 1,

@@ -17,7 +17,8 @@ extern "C" void filter_signs(const double* xyz, long n, int near, int* out)
 // doubles): query lon, lat (raw; the FakeLL round trip is applied here),
 // center lon, lat, then A lon, lat and B lon, lat.  out: s2 = orient(A, B, q),
 // s3 = orient(R, q, A), s4 = orient(R, q, B) in the given order of A and B
-// (0 = undecided), or 9 9 9 when the offset is not small.
+// (0 = undecided), then the tier's crossing test of the record (1 crossing,
+// 0 none, -1 undecided), or 9 9 9 9 when the offset is not small.
 #include "../../gahhg_b200/csrc/local_frame.cuh"
 
 extern "C" void local_signs(const double* cfg, long n, int* out)
@@ -39,16 +40,20 @@ extern "C" void local_signs(const double* cfg, long n, int* out)
         double sb, cb;
         gahhg_canon_sincos(gahhg_canon_rad(c[3]), &sb, &cb);
         local_frame::Frame f;
-        int* s = out + 3 * i;
+        int* s = out + 4 * i;
         if (s1 == 0 || !(fabs(c[0]) <= 540.0) ||
             !local_frame::frame_at(c[0], gahhg_canon_query_lat(c[1]), c[2], c[3], (float)sb, (float)cb, f)) {
-            s[0] = s[1] = s[2] = 9;
+            s[0] = s[1] = s[2] = s[3] = 9;
             continue;
         }
-        const int e = local_frame::sign_edge(f, r[0], r[1], r[2], r[3]);
-        const int ea = local_frame::sign_end(f, r[0], r[1]), eb = local_frame::sign_end(f, r[2], r[3]);
+        local_frame::Tests t;
+        local_frame::tests_of(f, t);
+        const int e = local_frame::sign_edge(t, r[0], r[1], r[2], r[3]);
+        const int ea = local_frame::sign_end(t, r[0], r[1]), eb = local_frame::sign_end(t, r[2], r[3]);
         s[0] = swap ? -e : e;
         s[1] = swap ? eb : ea;
         s[2] = swap ? ea : eb;
+        // the tier's combined test, on the stored order
+        s[3] = local_frame::record_crossing(t, r[0], r[1], r[2], r[3]);
     }
 }

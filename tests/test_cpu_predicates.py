@@ -41,7 +41,7 @@ def probe(tmp_path_factory):
 
     def local(cfg):
         cfg = np.ascontiguousarray(cfg, dtype=np.float64)
-        res = np.zeros((len(cfg), 3), dtype=np.int32)
+        res = np.zeros((len(cfg), 4), dtype=np.int32)
         lib.local_signs(cfg.ctypes.data, len(cfg), res.ctypes.data)
         return res
 
@@ -128,14 +128,30 @@ def test_fp32_local_frame_is_sound(probe, seed, polar):
     # near a pole cells span wide longitude differences, and more offsets are
     # refused (those points defer to the FP64 tier)
     assert ok.mean() > (0.99 if polar < 0.5 else 0.95)
-    want = np.zeros_like(got)
+    want = np.zeros((len(cfg), 3), dtype=np.int32)
+    cross = np.full(len(cfg), -1, dtype=np.int32)  # exact crossing of the stored record, -1: degenerate
     for i in np.nonzero(ok)[0]:
         c = cfg[i]
         q = exact.query_xyz(c[0:2].reshape(1, 2))[0]
         R, A, B = exact.vertex_xyz(c[2:8].reshape(3, 2))
         want[i] = (exact.orient(A, B, q, sos=False), exact.orient(R, q, A, sos=False), exact.orient(R, q, B, sos=False))
-    g, w = got[ok], want[ok]
+        # the record is stored in the order that makes orient(A, B, R) = +1
+        s2, s3, s4 = want[i]
+        if exact.orient(A, B, R, sos=False) < 0:
+            s2, s3, s4 = -s2, s4, s3
+        if s2 == 1 or s3 == 1 or s4 == -1:
+            cross[i] = 0
+        elif s2 == -1 and s3 == -1 and s4 == 1:
+            cross[i] = 1
+    g, w = got[ok, :3], want[ok]
     decided = g != 0
     assert np.array_equal(g[decided], w[decided]), "the local-frame FP32 tier returned a wrong sign"
     # points 1e-5 of the cell size or more from the arc are decided in FP32
     assert decided.mean() > 0.6, decided.mean()
+    # the tier's combined test: decided answers are the exact crossing, and a
+    # degenerate case (an exact zero and no sign that rules the crossing out)
+    # is never decided
+    gx, wx = got[ok, 3], cross[ok]
+    dx = gx >= 0
+    assert np.array_equal(gx[dx], wx[dx]), "the local-frame FP32 crossing test returned a wrong answer"
+    assert dx.mean() > 0.7, dx.mean()

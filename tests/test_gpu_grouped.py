@@ -1,10 +1,12 @@
-"""The pass-1 queue put in leaf-bucket order before the tiers run
-(k_bucket_sort: counts per bucket of 64 leaves, scan, scatter) against the
-tiers over the queue in pass-1 order (knob GAHHG_KNOB_GROUPED_PASS2 = 0): the
-same labels and the same per-tier escalation counts, for both precisions, on
-near-edge points of the 1.1M-edge C1 polygon (dense buckets: sorted) and on
-uniform points and the shipped NA0 polygon (sparse: the sort is skipped).
-Labels are also checked against the exact oracle where it is cheap.
+"""The pass-1 queue put in leaf-window order before the tiers run
+(k_part_count / k_part_scatter: a counting sort of the queue by window of
+consecutive leaves, each window about 24 MB of index records) against the
+tiers over the queue in pass-1 order (knob GAHHG_KNOB_GROUPED_PASS2 = 0, the
+default): the same labels and the same per-tier escalation counts, for both
+precisions, on near-edge points of the 1.1M-edge C1 polygon (a long queue:
+ordered) and on uniform points and the shipped NA0 polygon (short queues or
+one window: pass-1 order kept).  Labels are also checked against the exact
+oracle where it is cheap.
 Reference boundary loop: source/GPISPAHHG.cu:1481-1501.
 """
 import numpy as np
