@@ -12,6 +12,10 @@ statistics of the report and a SHA-256 digest of the grid arrays; plus the
 exact oracle's labels.
 
     python tests/golden/make_explist_fixtures.py [/path/to/reference]
+    python tests/golden/make_explist_fixtures.py --tennessee [/path/to/reference]
+
+The second form writes explist_tennessee.npz, every Tennessee invocation
+(main_tennessee below).
 
 Needs the reference checkout and the CPU builds (python oracle/build_ref.py,
 python oracle/build_oracle.py) and libgahhg.so (host code only).
@@ -129,5 +133,48 @@ def main(refroot=None):
           "points where the reference and the exact oracle differ")
 
 
+def main_tennessee(refroot=None):
+    """tests/golden/explist_tennessee.npz: every Tennessee invocation of
+    test/explist.bat (2,498 polygons of the same boundary at 5 to 25,003
+    vertices, 601 MB of text).  The polygon texts are stored as one
+    LZMA-compressed blob (the polygons share most of their lines, so it
+    compresses to a few MB) with each polygon's byte range; the outputs as in
+    explist.npz."""
+    import lzma
+    refroot = refroot or os.environ.get("GAHHG_REFERENCE", "/root/reference")
+    from tests.golden.fixtures import Inputs
+    store = Inputs()
+    invs = sorted(i for i in invocations(refroot) if i[0].startswith("Tennessee/"))
+    assert all(q == "Tennessee_query.csv" for _p, q in invs)
+    texts = []
+    for p, _q in invs:
+        with open(os.path.join(refroot, "test/polygon", p), "rb") as f:
+            texts.append(f.read().decode().replace("\r\n", "\n"))
+    blob = "".join(texts).encode()
+    offs = np.concatenate([[0], np.cumsum([len(t.encode()) for t in texts])]).astype(np.int64)
+    q = store.z["query_Tennessee_query"]
+    with mp.get_context("spawn").Pool(os.cpu_count()) as pool:
+        res = pool.map(_run_one, [(t, q) for t in texts], chunksize=1)
+    out = {
+        "names": np.array([p for p, _q in invs]),
+        "queries": np.array(["Tennessee_query"] * len(invs)),
+        "text_xz": np.frombuffer(lzma.compress(blob, preset=9), dtype=np.uint8),
+        "text_off": offs,
+        "stats": np.stack([r[0] for r in res]),
+        "grid_digest": np.array([r[1] for r in res]),
+        "ref_in": np.concatenate([np.packbits(r[2] == 2) for r in res]),
+        "ref_zero": np.concatenate([np.nonzero(r[2] == 0)[0] for r in res] + [np.zeros(0, np.int64)]),
+        "ref_zero_count": np.array([int((r[2] == 0).sum()) for r in res]),
+        "exact_in": np.concatenate([np.packbits(r[3] == 2) for r in res]),
+        "npoints": np.array([len(r[2]) for r in res]),
+    }
+    np.savez_compressed(os.path.join(HERE, "explist_tennessee.npz"), **out)
+    print("wrote", len(invs), "Tennessee invocations;", sum(int((r[2] != r[3]).sum()) for r in res),
+          "points where the reference and the exact oracle differ")
+
+
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    if sys.argv[1:2] == ["--tennessee"]:
+        main_tennessee(*sys.argv[2:])
+    else:
+        main(*sys.argv[1:])
