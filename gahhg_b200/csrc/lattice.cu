@@ -166,24 +166,38 @@ __host__ __device__ inline void nudge_center(const Geo& g, int lvl, NodeCap& c, 
     }
 }
 
-// Conservative: may arc AB (unit vectors) come within angle r of R?
-__host__ __device__ inline bool edge_hits_cap(const D3& A, const D3& B, const double* R, double r)
+// The cap's thresholds: squared chord of its radius r and the bound on the
+// sine of the distance from its center to a great circle that meets it.
+__host__ __device__ inline double cap_chord2(double r)
 {
     const double chord = 2.0 * sin(0.5 * r) * (1.0 + 1e-9) + 1e-12;
-    const double c2 = chord * chord;
+    return chord * chord;
+}
+__host__ __device__ inline double cap_sin_bound(double r) { return sin(r) * (1.0 + 1e-9) + 1e-12; }
+
+// edge_hits_cap with the cap's thresholds and the edge's normal N = A x B,
+// nn = |N|, computed once by the caller.
+__host__ __device__ inline bool edge_hits_cap_pre(const D3& A, const D3& B, const D3& N, double nn, const double* R,
+                                                  double c2, double sb)
+{
     const double ax = A.x - R[0], ay = A.y - R[1], az = A.z - R[2];
     if (ax * ax + ay * ay + az * az <= c2) return true;
     const double bx = B.x - R[0], by = B.y - R[1], bz = B.z - R[2];
     if (bx * bx + by * by + bz * bz <= c2) return true;
-    const D3 N = cross(A, B);
-    const double nn = sqrt(dot(N, N));
     if (!(nn > 1e-300)) return false;
     const double s = (N.x * R[0] + N.y * R[1] + N.z * R[2]) / nn;
-    if (fabs(s) > sin(r) * (1.0 + 1e-9) + 1e-12) return false;
+    if (fabs(s) > sb) return false;
     const D3 Rv = d3(R[0], R[1], R[2]);
     const double t1 = dot(cross(N, A), Rv), t2 = dot(cross(B, N), Rv);
     const double tol = 1e-12 * nn;
     return t1 >= -tol && t2 >= -tol;
+}
+
+// Conservative: may arc AB (unit vectors) come within angle r of R?
+__host__ __device__ inline bool edge_hits_cap(const D3& A, const D3& B, const double* R, double r)
+{
+    const D3 N = cross(A, B);
+    return edge_hits_cap_pre(A, B, N, sqrt(dot(N, N)), R, cap_chord2(r), cap_sin_bound(r));
 }
 
 __host__ __device__ inline double lat_of(const D3& p) { return asin(fmin(1.0, fmax(-1.0, p.y))) / RAD; }
@@ -373,42 +387,70 @@ __global__ void k_l0_expand(BuildView v, const EdgeBox* __restrict__ box, const 
     }
 }
 
-// Cap (R, r) of every child node of a level, once: the pair passes below
-// test each child against every edge of its parent, twice.
-__global__ void k_child_caps(Geo g, int lvl, int nn, const long long* ix, const long long* iy, double4* caps)
+// Cap of every child node of a level, once: center R and the squared chord
+// in caps, the sine bound and the radius in capsb (cap_chord2 /
+// cap_sin_bound of its radius).
+__global__ void k_child_caps(Geo g, int lvl, int nn, const long long* ix, const long long* iy, double4* caps,
+                             double2* capsb)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nn) return;
     const NodeCap nc = node_cap(g, lvl, ix[c], iy[c]);
-    caps[c] = make_double4(nc.R[0], nc.R[1], nc.R[2], nc.r);
+    caps[c] = make_double4(nc.R[0], nc.R[1], nc.R[2], cap_chord2(nc.r));
+    capsb[c] = make_double2(cap_sin_bound(nc.r), nc.r);
 }
 
-// Children pairs: one thread per (refined parent, edge) pair.
-template <int PASS>
-__global__ void k_child_pairs(BuildView v, int npairs, const int* pair_node, const int* plist,
-                              const int* child_base, const double4* __restrict__ caps, int cstart, int* cnt,
-                              const int* off, int* cursor, int* list)
+// Children pairs, count pass: one thread per (refined parent, edge) pair
+// tests the parent's FAN x FAN children (consecutive nodes) and records its
+// hits as a mask, so the fill pass writes the list entries without testing
+// again.  (Sixteen lanes per pair, one child each, ran 2.2x slower on the C1
+// polygon: a pair is only sixteen tests, and the dependent loads that start
+// it were then paid by a half-warp instead of one thread.)
+__global__ void __launch_bounds__(TPB) k_child_pairs_count(BuildView v, int npairs, const int* __restrict__ pair_node,
+                                                           const int* __restrict__ plist,
+                                                           const int* __restrict__ child_base,
+                                                           const double4* __restrict__ caps,
+                                                           const double2* __restrict__ capsb, int cstart, int* cnt,
+                                                           uint16_t* hit)
 {
+    static_assert(FAN * FAN == 16, "a 16-bit hit mask per pair");
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= npairs) return;
-    const int p = pair_node[k];
-    const int cb = child_base[p];
+    const int cb = child_base[pair_node[k]];
     if (cb < 0) return;
     const int e = plist[k];
     const D3 A = v.pv[v.pe[2 * e]], B = v.pv[v.pe[2 * e + 1]];
-    for (int cy = 0; cy < FAN; cy++)
-        for (int cx = 0; cx < FAN; cx++) {
-            const int node = cb + cy * FAN + cx - cstart;
-            const double4 c = caps[node];
-            const double R[3] = {c.x, c.y, c.z};
-            if (!edge_hits_cap(A, B, R, c.w)) continue;
-            if (PASS == 0) {
-                atomicAdd(&cnt[node], 1);
-            } else {
-                const int pos = off[node] + atomicAdd(&cursor[node], 1);
-                list[pos] = e;
-            }
-        }
+    const D3 N = cross(A, B);
+    const double nn = sqrt(dot(N, N));
+    unsigned int m = 0;
+    for (int l = 0; l < FAN * FAN; l++) {
+        const int node = cb + l - cstart;
+        const double4 c = caps[node];
+        const double R[3] = {c.x, c.y, c.z};
+        if (!edge_hits_cap_pre(A, B, N, nn, R, c.w, capsb[node].x)) continue;
+        m |= 1u << l;
+        atomicAdd(&cnt[node], 1);
+    }
+    hit[k] = (uint16_t)m;
+}
+
+// Children pairs, fill pass: one thread per pair, one entry per hit.
+__global__ void k_child_pairs_fill(int npairs, const int* __restrict__ pair_node, const int* __restrict__ plist,
+                                   const int* __restrict__ child_base, int cstart, const uint16_t* __restrict__ hit,
+                                   const int* off, int* cursor, int* list)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= npairs) return;
+    const int cb = child_base[pair_node[k]];
+    if (cb < 0) return;
+    unsigned int m = hit[k];
+    const int e = plist[k];
+    while (m) {
+        const int l = __ffs(m) - 1;
+        m &= m - 1u;
+        const int node = cb + l - cstart;
+        list[off[node] + atomicAdd(&cursor[node], 1)] = e;
+    }
 }
 
 __global__ void k_fill_pair_node(const int* cnt, const int* off, int nn, int* pair_node)
@@ -622,23 +664,97 @@ __global__ void k_l0_labels(int W, int H, const uint8_t* vpar, const uint8_t* hp
 }
 
 // child label = parent label XOR parity(arc parent center -> child center)
-__global__ void k_child_labels(BuildView v, int lvl, int nchild, const int* child_parent, const long long* cix,
-                               const long long* ciy, const int* ccnt, const int* coff, const int* clist,
-                               const long long* pix, const long long* piy, const int* pcnt, const int* poff,
-                               const int* plist, const uint8_t* plabel, uint8_t* clabel, int* bad)
+// true when R coincides with an end of an edge of the list (nudge_center
+// would move it)
+__device__ __forceinline__ bool center_on_vertex(const double* R, const D3* pv, const int* pe, const int* list,
+                                                 int cnt)
+{
+    for (int k = 0; k < cnt; k++) {
+        const int e = list[k];
+        const D3 a = pv[pe[2 * e]], b = pv[pe[2 * e + 1]];
+        if ((a.x == R[0] && a.y == R[1] && a.z == R[2]) || (b.x == R[0] && b.y == R[1] && b.z == R[2])) return true;
+    }
+    return false;
+}
+
+// Child labels: parent label XOR the crossing parity of arc(parent center P,
+// child center Q) against the parent's list (exact predicates), as
+// arc_parity_lists computes it.  A parent's FAN x FAN children are
+// consecutive and nchild is a multiple of 16, so each 16-lane group of a
+// warp holds one parent's children: its first lane places the parent's
+// center and shares it, and the lanes share the children-independent half of
+// every crossing test, orient(A, B, P), computed by lane k mod 16 for edge
+// k.  Child centers come from the pair pass's caps (node_cap, recomputed
+// only when a center must be nudged off a vertex).
+__global__ void __launch_bounds__(TPB) k_child_labels(BuildView v, int lvl, int nchild, const int* child_parent,
+                                                      const long long* cix, const long long* ciy, const int* ccnt,
+                                                      const int* coff, const int* clist,
+                                                      const double4* __restrict__ ccaps,
+                                                      const double2* __restrict__ ccapsb, const long long* pix,
+                                                      const long long* piy, const int* pcnt, const int* poff,
+                                                      const int* plist, const uint8_t* plabel, uint8_t* clabel,
+                                                      int* bad)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nchild) return;
     const int p = child_parent[c];
-    NodeCap pc = node_cap(v.g, lvl, pix[p], piy[p]);
-    nudge_center(v.g, lvl, pc, v.pv, v.pe, plist + poff[p], pcnt[p]);
-    NodeCap cc = node_cap(v.g, lvl + 1, cix[c], ciy[c]);
-    nudge_center(v.g, lvl + 1, cc, v.pv, v.pe, clist + coff[c], ccnt[c]);
+    const int gl = threadIdx.x & 15;
+    const unsigned int grp = 0xFFFFu << (threadIdx.x & 16);
+    NodeCap pc;
+    if (gl == 0) {
+        pc = node_cap(v.g, lvl, pix[p], piy[p]);
+        nudge_center(v.g, lvl, pc, v.pv, v.pe, plist + poff[p], pcnt[p]);
+    }
+    double P[3];
+    P[0] = __shfl_sync(grp, pc.R[0], 0, 16);
+    P[1] = __shfl_sync(grp, pc.R[1], 0, 16);
+    P[2] = __shfl_sync(grp, pc.R[2], 0, 16);
+    const double pr = __shfl_sync(grp, pc.r, 0, 16);
+    NodeCap cc;
+    {
+        const double4 cr = ccaps[c];
+        cc.R[0] = cr.x;
+        cc.R[1] = cr.y;
+        cc.R[2] = cr.z;
+        cc.r = ccapsb[c].y;
+    }
+    if (center_on_vertex(cc.R, v.pv, v.pe, clist + coff[c], ccnt[c])) {
+        cc = node_cap(v.g, lvl + 1, cix[c], ciy[c]);
+        nudge_center(v.g, lvl + 1, cc, v.pv, v.pe, clist + coff[c], ccnt[c]);
+    }
     // nesting of caps: the child's cap must lie inside the parent's
-    const double dx = pc.R[0] - cc.R[0], dy = pc.R[1] - cc.R[1], dz = pc.R[2] - cc.R[2];
+    const double dx = P[0] - cc.R[0], dy = P[1] - cc.R[1], dz = P[2] - cc.R[2];
     const double dist = 2.0 * asin(fmin(1.0, 0.5 * sqrt(dx * dx + dy * dy + dz * dz)));
-    if (dist + cc.r > pc.r) atomicAdd(bad + 1, 1);
-    const int par = arc_parity_lists(v.pv, v.pe, pc.R, cc.R, plist + poff[p], pcnt[p], nullptr, 0, bad);
+    if (dist + cc.r > pr) atomicAdd(bad + 1, 1);
+    const double* Q = cc.R;
+    const int* L = plist + poff[p];
+    const int n = pcnt[p];
+    int par = 0;
+    for (int k0 = 0; k0 < n; k0 += 16) {
+        int acb_mine = 0;  // -orient(A, B, P) of edge k0 + gl
+        if (k0 + gl < n) {
+            const int e = L[k0 + gl];
+            const D3 a = v.pv[v.pe[2 * e]], b = v.pv[v.pe[2 * e + 1]];
+            const double A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z};
+            if (!exact::same(A, B) && !exact::same(A, P) && !exact::same(B, P)) acb_mine = -exact::orient(A, B, P);
+        }
+        const int m = min(16, n - k0);
+        for (int j = 0; j < m; j++) {
+            const int acb = __shfl_sync(grp, acb_mine, j, 16);
+            const int e = L[k0 + j];
+            const D3 a = v.pv[v.pe[2 * e]], b = v.pv[v.pe[2 * e + 1]];
+            const double A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z};
+            if (exact::same(A, B)) continue;
+            if (exact::same(A, P) || exact::same(B, P) || exact::same(A, Q) || exact::same(B, Q)) {
+                atomicAdd(bad, 1);
+                continue;
+            }
+            // exact::crossing(P, Q, A, B) with its first orientation shared
+            if (exact::orient(A, B, Q) != acb) continue;
+            if (-exact::orient(P, Q, B) != acb) continue;
+            if (exact::orient(P, Q, A) == acb) par ^= 1;
+        }
+    }
     clabel[c] = (uint8_t)(par ? 3 - plabel[p] : plabel[p]);
 }
 
@@ -2094,17 +2210,48 @@ int nearest_hub(const double* q)
 // domain that reaches within a degree of a pole takes in the whole polar cap
 // (all longitudes), so that points outside it are never close to an edge.
 // Latitude range and touched 0.1-degree longitude bins of edges [e0, e1).
-struct DomainScan {
-    double latmin = 90.0, latmax = -90.0;
-    bool full = false;
-    std::vector<uint8_t> bins = std::vector<uint8_t>(3600, 0);
+// The domain scan on the device: per edge its latitude range and the
+// 0.1-degree longitude bins it touches (long edges by their great-circle box,
+// short ones by their ends' latitude and longitude, padded by 1e-4 degrees),
+// reduced per block in shared memory and then with one atomic per block and
+// word.  Min, max and OR do not depend on the order of the edges.
+constexpr int DOMAIN_BIN_WORDS = (3600 + 31) / 32;
+struct DomainOut {
+    unsigned long long latmin, latmax;  // order-preserving keys of the doubles
+    unsigned int full;
+    unsigned int bins[DOMAIN_BIN_WORDS];
 };
 
-static void scan_domain(const Polygon* P, int e0, int e1, DomainScan& D)
+__device__ __forceinline__ unsigned long long order_key(double x)
 {
-    for (int e = e0; e < e1; e++) {
-        const int ia = P->pe[2 * e], ib = P->pe[2 * e + 1];
-        const D3 a = P->pv[ia], b = P->pv[ib];
+    const unsigned long long u = (unsigned long long)__double_as_longlong(x);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+__host__ inline double from_order_key(unsigned long long k)
+{
+    const unsigned long long u = (k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k;
+    double x;
+    memcpy(&x, &u, sizeof x);
+    return x;
+}
+
+__global__ void __launch_bounds__(TPB) k_domain_scan(const D3* __restrict__ pv, const int* __restrict__ pe, int n,
+                                                     DomainOut* out)
+{
+    __shared__ unsigned int s_bins[DOMAIN_BIN_WORDS];
+    __shared__ unsigned long long s_min, s_max;
+    __shared__ unsigned int s_full;
+    for (int k = threadIdx.x; k < DOMAIN_BIN_WORDS; k += TPB) s_bins[k] = 0;
+    if (threadIdx.x == 0) {
+        s_min = ~0ull;
+        s_max = 0ull;
+        s_full = 0;
+    }
+    __syncthreads();
+    double lmin = 90.0, lmax = -90.0;
+    bool full = false;
+    for (int e = blockIdx.x * TPB + threadIdx.x; e < n; e += gridDim.x * TPB) {
+        const D3 a = pv[pe[2 * e]], b = pv[pe[2 * e + 1]];
         if (a.x == b.x && a.y == b.y && a.z == b.z) continue;
         double la0, la1, lo0, lo1;
         bool fl = false;
@@ -2112,15 +2259,16 @@ static void scan_domain(const Polygon* P, int e0, int e1, DomainScan& D)
         if (dx * dx + dy * dy + dz * dz > 1e-4) {
             arc_box(a, b, la0, la1, lo0, lo1, fl);  // long edge: its great circle may bulge
         } else {
-            // short edge: the input degrees of its ends (the bulge is below 1e-4 deg, far
-            // inside the one-cell padding)
-            double oa = P->lonlat[2 * ia], ob = P->lonlat[2 * ib];
-            const double ta = P->lonlat[2 * ia + 1], tb = P->lonlat[2 * ib + 1];
-            la0 = std::min(ta, tb) - 1e-4;
-            la1 = std::max(ta, tb) + 1e-4;
-            oa -= 360.0 * floor((oa + 180.0) / 360.0);
-            ob -= 360.0 * floor((ob + 180.0) / 360.0);
-            if (oa > ob) std::swap(oa, ob);
+            // short edge: its ends (the bulge is below 1e-4 deg, far inside the one-cell padding)
+            const double ta = lat_of(a), tb = lat_of(b);
+            double oa = lon_of(a), ob = lon_of(b);
+            la0 = fmin(ta, tb) - 1e-4;
+            la1 = fmax(ta, tb) + 1e-4;
+            if (oa > ob) {
+                const double t = oa;
+                oa = ob;
+                ob = t;
+            }
             if (ob - oa <= 180.0) {
                 lo0 = oa;
                 lo1 = ob;
@@ -2130,45 +2278,60 @@ static void scan_domain(const Polygon* P, int e0, int e1, DomainScan& D)
             }
             if (fabs(ta) > 89.9 || fabs(tb) > 89.9) fl = true;
         }
-        D.latmin = std::min(D.latmin, la0);
-        D.latmax = std::max(D.latmax, la1);
+        lmin = fmin(lmin, la0);
+        lmax = fmax(lmax, la1);
         if (fl) {
-            D.full = true;
+            full = true;
             continue;
         }
-        const long long b0 = (long long)floor((lo0 + 180.0) * 10.0) - 1, b1 = (long long)floor((lo1 + 180.0) * 10.0) + 1;
-        for (long long k = b0; k <= b1; k++) D.bins[((k % 3600) + 3600) % 3600] = 1;
+        const int b0 = (int)floor((lo0 + 180.0) * 10.0) - 1, b1 = (int)floor((lo1 + 180.0) * 10.0) + 1;
+        for (int k = b0; k <= b1 && k <= b0 + 3600; k++) {
+            const int bit = ((k % 3600) + 3600) % 3600;
+            atomicOr(&s_bins[bit >> 5], 1u << (bit & 31));
+        }
+    }
+    for (int d = 16; d > 0; d >>= 1) {
+        lmin = fmin(lmin, __shfl_down_sync(0xffffffffu, lmin, d));
+        lmax = fmax(lmax, __shfl_down_sync(0xffffffffu, lmax, d));
+    }
+    full = __any_sync(0xffffffffu, full);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&s_min, order_key(lmin));
+        atomicMax(&s_max, order_key(lmax));
+        if (full) s_full = 1;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < DOMAIN_BIN_WORDS; k += TPB)
+        if (s_bins[k]) atomicOr(&out->bins[k], s_bins[k]);
+    if (threadIdx.x == 0) {
+        atomicMin(&out->latmin, s_min);
+        atomicMax(&out->latmax, s_max);
+        if (s_full) atomicOr(&out->full, 1u);
     }
 }
 
-gahhg_status compute_domain(const Polygon* P, long long target, Geo* G)
+gahhg_status compute_domain(const Polygon* P, long long target, Geo* G, cudaStream_t s, int device)
 {
-    // large polygons are scanned by several host threads (each over a range
-    // of edges, merged after); the result does not depend on the split
-    constexpr int EDGES_PER_THREAD = 1 << 17;
-    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
-    const int nt = std::max(1, std::min(std::min(hw, 16), P->pv_num / EDGES_PER_THREAD));
-    std::vector<DomainScan> part(nt);
-    if (nt == 1) {
-        scan_domain(P, 0, P->pv_num, part[0]);
-    } else {
-        std::vector<std::thread> th;
-        for (int t = 0; t < nt; t++) {
-            const int e0 = (int)((long long)P->pv_num * t / nt), e1 = (int)((long long)P->pv_num * (t + 1) / nt);
-            th.emplace_back(scan_domain, P, e0, e1, std::ref(part[t]));
-        }
-        for (auto& t : th) t.join();
+    DomainOut h;
+    {
+        DomainOut* d = nullptr;
+        GAHHG_TRY(pool_alloc((void**)&d, sizeof(DomainOut), device, s));
+        memset(&h, 0, sizeof h);
+        h.latmin = ~0ull;
+        GAHHG_CUDA_TRY(cudaMemcpyAsync(d, &h, sizeof h, cudaMemcpyHostToDevice, s));
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        const int grid = (int)std::max(1LL, std::min<long long>(sms * 4LL, (P->pv_num + TPB - 1) / TPB));
+        k_domain_scan<<<grid, TPB, 0, s>>>(P->d_pv, P->d_pe, P->pv_num, d);
+        GAHHG_CUDA_TRY(cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, s));
+        cudaFreeAsync(d, s);
+        GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
     }
-    double latmin = 90.0, latmax = -90.0;
-    bool full = false;
-    std::vector<uint8_t>& bins = part[0].bins;  // 0.1-degree longitude bins touched by some arc
-    for (int t = 0; t < nt; t++) {
-        latmin = std::min(latmin, part[t].latmin);
-        latmax = std::max(latmax, part[t].latmax);
-        full = full || part[t].full;
-        if (t > 0)
-            for (int k = 0; k < 3600; k++) bins[k] |= part[t].bins[k];
-    }
+    double latmin = h.latmax == 0ull ? 90.0 : from_order_key(h.latmin);
+    double latmax = h.latmax == 0ull ? -90.0 : from_order_key(h.latmax);
+    bool full = h.full != 0;
+    std::vector<uint8_t> bins(3600);  // 0.1-degree longitude bins touched by some arc
+    for (int k = 0; k < 3600; k++) bins[k] = (h.bins[k >> 5] >> (k & 31)) & 1u;
     if (latmin > latmax) {
         set_error("exact index: polygon has no edges of positive length");
         return GAHHG_ERR_ARG;
@@ -2298,7 +2461,7 @@ gahhg_status lattice_build(Grid* g)
 
     long long target = g->opts.lattice_top > 0 ? (long long)g->opts.lattice_top
                                                 : std::min<long long>(std::max<long long>(8LL * n, 1024), 8LL << 20);
-    GAHHG_TRY(compute_domain(P, target, &L->geo));
+    GAHHG_TRY(compute_domain(P, target, &L->geo, s, g->device));
     phase("domain");
     const int W = L->geo.W, H = L->geo.H;
     L->K = g->opts.lattice_leaf > 0 ? g->opts.lattice_leaf : 8;
@@ -2478,11 +2641,16 @@ gahhg_status lattice_build(Grid* g)
         GAHHG_CUDA_TRY(cudaMemsetAsync(cl.cnt.ptr, 0, sizeof(int) * cl.nn, s));
         GAHHG_CUDA_TRY(cudaMemsetAsync(cl.cursor.ptr, 0, sizeof(int) * cl.nn, s));
         DevArray<double4> caps;
+        DevArray<double2> capsb;
+        DevArray<uint16_t> hit;
         GAHHG_TRY(caps.reserve(cl.nn, s, false));
-        k_child_caps<<<blocks_for(cl.nn), TPB, 0, s>>>(L->geo, lvl + 1, cl.nn, cl.ix.ptr, cl.iy.ptr, caps.ptr);
-        k_child_pairs<0><<<blocks_for(pp.npairs), TPB, 0, s>>>(bv, pp.npairs, pp.pair_node.ptr, pp.list.ptr,
-                                                               pp.child_base.ptr, caps.ptr, cl.gstart, cl.cnt.ptr,
-                                                               nullptr, nullptr, nullptr);
+        GAHHG_TRY(capsb.reserve(cl.nn, s, false));
+        GAHHG_TRY(hit.reserve(std::max(pp.npairs, 1), s, false));
+        k_child_caps<<<blocks_for(cl.nn), TPB, 0, s>>>(L->geo, lvl + 1, cl.nn, cl.ix.ptr, cl.iy.ptr, caps.ptr,
+                                                       capsb.ptr);
+        k_child_pairs_count<<<blocks_for(pp.npairs), TPB, 0, s>>>(
+            bv, pp.npairs, pp.pair_node.ptr, pp.list.ptr, pp.child_base.ptr, caps.ptr, capsb.ptr, cl.gstart,
+            cl.cnt.ptr, hit.ptr);
         GAHHG_TRY(scan_state_reserve(&g->scan_state, cl.nn));
         GAHHG_TRY(scan_exclusive(cl.cnt.ptr, cl.off.ptr, cl.nn, g->d_counts + 10, g->scan_state, g->d_err, s));
         int ctotal = 0;
@@ -2490,10 +2658,10 @@ gahhg_status lattice_build(Grid* g)
         GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
         cl.npairs = ctotal;
         GAHHG_TRY(cl.list.reserve(std::max(ctotal, 1), s, false));
-        k_child_pairs<1><<<blocks_for(pp.npairs), TPB, 0, s>>>(bv, pp.npairs, pp.pair_node.ptr, pp.list.ptr,
-                                                               pp.child_base.ptr, caps.ptr, cl.gstart, cl.cnt.ptr,
-                                                               cl.off.ptr, cl.cursor.ptr, cl.list.ptr);
-        caps.release();
+        k_child_pairs_fill<<<blocks_for(pp.npairs), TPB, 0, s>>>(pp.npairs, pp.pair_node.ptr, pp.list.ptr,
+                                                                 pp.child_base.ptr, cl.gstart, hit.ptr, cl.off.ptr,
+                                                                 cl.cursor.ptr, cl.list.ptr);
+        hit.release();
         GAHHG_TRY(sort_lists(g, cl.cnt.ptr, cl.off.ptr, cl.nn, cl.list.ptr, sms, s));
         // child labels
         DevArray<int> child_parent;
@@ -2501,9 +2669,11 @@ gahhg_status lattice_build(Grid* g)
         k_child_parent<<<blocks_for(pp.nn), TPB, 0, s>>>(pp.child_base.ptr, pp.nn, cl.gstart, child_parent.ptr);
         GAHHG_TRY(cl.label.reserve(cl.nn, s, false));
         k_child_labels<<<blocks_for(cl.nn), TPB, 0, s>>>(bv, lvl, cl.nn, child_parent.ptr, cl.ix.ptr, cl.iy.ptr,
-                                                         cl.cnt.ptr, cl.off.ptr, cl.list.ptr, pp.ix.ptr, pp.iy.ptr,
-                                                         pp.cnt.ptr, pp.off.ptr, pp.list.ptr, pp.label.ptr,
-                                                         cl.label.ptr, d_bad);
+                                                         cl.cnt.ptr, cl.off.ptr, cl.list.ptr, caps.ptr, capsb.ptr,
+                                                         pp.ix.ptr, pp.iy.ptr, pp.cnt.ptr, pp.off.ptr, pp.list.ptr,
+                                                         pp.label.ptr, cl.label.ptr, d_bad);
+        caps.release();
+        capsb.release();
         GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
         child_parent.release();
         gnext += cl.nn;
