@@ -417,6 +417,10 @@ static gahhg_status run_query(Grid* g, const double* d_lonlat, size_t n, uint8_t
             set_error("exact precision needs a grid built with GAHHG_SEMANTICS_EXACT");
             return GAHHG_ERR_STATE;
         }
+        if ((uintptr_t)d_lonlat & 15u) {
+            set_error("exact queries read lon/lat in 16-byte units: the device buffer must be 16-byte aligned");
+            return GAHHG_ERR_ARG;
+        }
         return lattice_query(g, d_lonlat, n, d_labels, precision, s, d_counters);
     }
     set_error("unknown precision %d", precision);

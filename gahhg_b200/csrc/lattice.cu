@@ -2950,6 +2950,10 @@ gahhg_status lattice_query_noalloc(Grid* g, const double* d_lonlat, size_t n, ui
                   NOALLOC_MAX_POINTS);
         return GAHHG_ERR_CAPACITY;
     }
+    if ((uintptr_t)d_lonlat & 15u) {
+        set_error("exact queries read lon/lat in 16-byte units: the device buffer must be 16-byte aligned");
+        return GAHHG_ERR_ARG;
+    }
     uint32_t* queue = nullptr;
     GAHHG_TRY(noalloc_queue_address(g->device, &queue));
     if (n == 0) return GAHHG_OK;

@@ -142,7 +142,9 @@ void gahhg_grid_free(gahhg_grid* g);
 /* ---- query -------------------------------------------------------------- */
 
 /* GPISP::test / kernel_PISP (source/GPISPAHHG.cu:2062-2085, 1422-1504).
- * Device pointers: lonlat (2 doubles per point), labels (1 byte per point).
+ * Device pointers: lonlat (2 doubles per point; 16-byte aligned for the
+ * exact precisions, which read it in 16-byte units, else GAHHG_ERR_ARG),
+ * labels (1 byte per point).
  * Asynchronous on `stream`; statistics are updated when `sync` is non-zero. */
 gahhg_status gahhg_query_device(gahhg_grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels,
                                 int precision, void* stream, int sync);

@@ -6,6 +6,8 @@ perturbation), points equal to vertices, poles, the antimeridian, and inputs
 outside the nominal lon/lat ranges.  The FP32-filtered and FP64-filtered
 kernels must agree with each other and with the oracle.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -92,6 +94,28 @@ def test_exact_zero_cases(tmp_path):
     assert np.array_equal(g.query(pts, G.QUERY_FP64_FILTER), want)
     # vertices whose FakeLL latitude is exact are polygon vertices -> inside
     assert (got[1001 + 301:1001 + 301 + len(vert)] == 2).all()
+
+
+def test_misaligned_lonlat_is_refused(tmp_path):
+    """Exact queries read lon/lat in 16-byte units: a device buffer that is
+    not 16-byte aligned is refused with GAHHG_ERR_ARG (both entry points),
+    never read."""
+    import torch
+    from gahhg_b200 import _lib
+    rings = synth.c0_polygon()
+    path = str(tmp_path / "c0.txt")
+    synth.write_polygon(path, rings)
+    g = G.Grid(G.Polygon.from_file(path), semantics=G.SEMANTICS_EXACT).classify()
+    buf = torch.zeros(2 * 1000 + 1, dtype=torch.float64, device="cuda:0")
+    lab = torch.zeros(1000, dtype=torch.uint8, device="cuda:0")
+    with pytest.raises(_lib.GahhgError) as e:
+        g.query_device(buf.data_ptr() + 8, 1000, lab.data_ptr(), G.QUERY_FP32_FILTER)
+    assert e.value.status == _lib.ERR_ARG
+    st = _lib.lib().gahhg_query_device_noalloc(g._h, ctypes.c_void_p(buf.data_ptr() + 8), 1000,
+                                               ctypes.c_void_p(lab.data_ptr()), G.QUERY_FP32_FILTER,
+                                               ctypes.c_void_p(0))
+    assert st == _lib.ERR_ARG
+    g.query_device(buf.data_ptr(), 1000, lab.data_ptr(), G.QUERY_FP32_FILTER, sync=True)
 
 
 def test_non_finite_inputs_are_undefined(tmp_path):
