@@ -25,12 +25,19 @@ const char* last_error() { return g_err; }
 
 static std::mutex g_pool_mu;
 static cudaMemPool_t g_pools[64] = {};
+// set once per device under g_pool_mu; read without the lock afterwards
+// (every allocation of every build worker asks for its device's pool)
+static std::atomic<cudaMemPool_t> g_pool_ready[64] = {};
 
 static gahhg_status device_pool(int device, cudaMemPool_t* out)
 {
     if (device < 0 || device >= 64) {
         set_error("device ordinal %d out of range", device);
         return GAHHG_ERR_ARG;
+    }
+    if (cudaMemPool_t p = g_pool_ready[device].load(std::memory_order_acquire)) {
+        *out = p;
+        return GAHHG_OK;
     }
     std::lock_guard<std::mutex> lock(g_pool_mu);
     if (!g_pools[device]) {
@@ -41,6 +48,7 @@ static gahhg_status device_pool(int device, cudaMemPool_t* out)
         GAHHG_CUDA_TRY(cudaMemPoolCreate(&g_pools[device], &props));
         uint64_t keep = 4ull << 30;  // keep up to 4 GB cached between calls
         GAHHG_CUDA_TRY(cudaMemPoolSetAttribute(g_pools[device], cudaMemPoolAttrReleaseThreshold, &keep));
+        g_pool_ready[device].store(g_pools[device], std::memory_order_release);
     }
     *out = g_pools[device];
     return GAHHG_OK;

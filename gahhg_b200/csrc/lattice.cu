@@ -2554,6 +2554,8 @@ gahhg_status lattice_build(Grid* g)
     k_l0_coords<<<blocks_for(l0.nn), TPB, 0, s>>>(W, l0.nn, l0.ix.ptr, l0.iy.ptr);
 
     // level-0 labels
+    bool has_outside_label = false;
+    uint8_t* d_outside = nullptr;
     int* d_bad = g->d_counts + 48;  // [0] coincidences, [1] nesting, [2] long lists
     GAHHG_CUDA_TRY(cudaMemsetAsync(d_bad, 0, 4 * sizeof(int), s));
     {
@@ -2582,17 +2584,14 @@ gahhg_status lattice_build(Grid* g)
             has_outside = false;
         }
         uint8_t* d_out = reinterpret_cast<uint8_t*>(g->d_counts + 13);
-        if (has_outside) {
+        // read back with the build's last round trip
+        has_outside_label = has_outside;
+        d_outside = d_out;
+        if (has_outside)
             k_outside_label<<<1, 1, 0, s>>>(bv, ix, iy, ox, oy, l0.cnt.ptr, l0.off.ptr, l0.list.ptr, l0.label.ptr,
                                             d_out, d_bad);
-            uint8_t ol = 0;
-            GAHHG_CUDA_TRY(cudaMemcpyAsync(&ol, d_out, 1, cudaMemcpyDeviceToHost, s));
-            GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
-            L->outside_label = ol;
-        } else {
+        else
             L->outside_label = CELL_UNDEFINED;
-        }
-        GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
         vpar.release();
         hpar.release();
     }
@@ -2674,7 +2673,6 @@ gahhg_status lattice_build(Grid* g)
                                                          pp.label.ptr, cl.label.ptr, d_bad);
         caps.release();
         capsb.release();
-        GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
         child_parent.release();
         gnext += cl.nn;
     }
@@ -2688,6 +2686,9 @@ gahhg_status lattice_build(Grid* g)
     std::vector<long long> rec_base(L->nlev);
     long long leaf_total = 0, rec_total = 0;
     std::vector<DevArray<int>> is_leaf(L->nlev), leaf_off(L->nlev), nrec(L->nlev), rec_off(L->nlev);
+    // every level's leaf and record totals, read back together
+    DevArray<int> d_tot;
+    GAHHG_TRY(d_tot.reserve(2 * L->nlev, s, false));
     for (int lvl = 0; lvl < L->nlev; lvl++) {
         LevelBuf& b = lv[lvl];
         const int* cb = (lvl + 1 < L->nlev) ? b.child_base.ptr : nullptr;
@@ -2697,20 +2698,27 @@ gahhg_status lattice_build(Grid* g)
         GAHHG_TRY(rec_off[lvl].reserve(b.nn, s, false));
         k_leaf_flags<<<blocks_for(b.nn), TPB, 0, s>>>(b.nn, b.cnt.ptr, cb, is_leaf[lvl].ptr, nrec[lvl].ptr);
         GAHHG_TRY(scan_state_reserve(&g->scan_state, b.nn));
-        GAHHG_TRY(scan_exclusive(is_leaf[lvl].ptr, leaf_off[lvl].ptr, b.nn, g->d_counts + 14, g->scan_state, g->d_err, s));
-        GAHHG_TRY(scan_exclusive(nrec[lvl].ptr, rec_off[lvl].ptr, b.nn, g->d_counts + 15, g->scan_state, g->d_err, s));
-        int tot[2];
-        GAHHG_CUDA_TRY(cudaMemcpyAsync(tot, g->d_counts + 14, sizeof(tot), cudaMemcpyDeviceToHost, s));
-        GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
-        leaf_base[lvl] = (int)leaf_total;
-        nleaf[lvl] = tot[0];
-        rec_base[lvl] = rec_total;
-        leaf_total += tot[0];
-        rec_total += tot[1];
-        // leaf indices are global: shift by leaf_base when encoding
+        GAHHG_TRY(scan_exclusive(is_leaf[lvl].ptr, leaf_off[lvl].ptr, b.nn, d_tot.ptr + 2 * lvl, g->scan_state,
+                                 g->d_err, s));
+        GAHHG_TRY(scan_exclusive(nrec[lvl].ptr, rec_off[lvl].ptr, b.nn, d_tot.ptr + 2 * lvl + 1, g->scan_state,
+                                 g->d_err, s));
+        // leaf indices are per level here: shifted by the level's leaf base below
         k_encode<<<blocks_for(b.nn), TPB, 0, s>>>(b.nn, b.gstart, b.cnt.ptr, cb, b.label.ptr, leaf_off[lvl].ptr,
                                                   L->nodes.ptr);
     }
+    {
+        std::vector<int> tot(2 * L->nlev);
+        GAHHG_CUDA_TRY(cudaMemcpyAsync(tot.data(), d_tot.ptr, sizeof(int) * tot.size(), cudaMemcpyDeviceToHost, s));
+        GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+        for (int lvl = 0; lvl < L->nlev; lvl++) {
+            leaf_base[lvl] = (int)leaf_total;
+            nleaf[lvl] = tot[2 * lvl];
+            rec_base[lvl] = rec_total;
+            leaf_total += tot[2 * lvl];
+            rec_total += tot[2 * lvl + 1];
+        }
+    }
+    d_tot.release();
     if (rec_total >= 0xFFFFFFFFll) {
         set_error("exact index: too many edge records");
         return GAHHG_ERR_CAPACITY;
@@ -2734,7 +2742,6 @@ gahhg_status lattice_build(Grid* g)
                                                         d_bad);
     }
     GAHHG_CUDA_TRY(cudaGetLastError());
-    GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
     // leaf words were encoded with per-level leaf offsets; make them global
     for (int lvl = 1; lvl < L->nlev; lvl++) {
         if (leaf_base[lvl] == 0) continue;
@@ -2753,8 +2760,11 @@ gahhg_status lattice_build(Grid* g)
         k_summary<<<blocks_for(CW * CH), TPB, 0, s>>>(L->nodes.ptr, W, H, cs, L->summary.ptr, CW * CH);
     }
     int bad[4];
+    uint8_t ol = 0;
     GAHHG_CUDA_TRY(cudaMemcpyAsync(bad, d_bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
+    if (has_outside_label) GAHHG_CUDA_TRY(cudaMemcpyAsync(&ol, d_outside, 1, cudaMemcpyDeviceToHost, s));
     GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+    if (has_outside_label) L->outside_label = ol;
     phase("encode");
     for (auto& b : lv) b.release();
     for (int lvl = 0; lvl < L->nlev; lvl++) {
