@@ -24,6 +24,7 @@ struct gahhg_batch {
     int chunk_points = 4096;
     std::vector<Polygon*> polys;
     std::vector<Grid*> grids;
+    std::vector<GroupIndex*> groups;  // polygons built together, in order
     std::vector<int> swords;  // summary words per polygon (chunk sizing)
     DevArray<uint8_t> views;
     WorkerPool pool;
@@ -51,6 +52,7 @@ struct gahhg_batch {
         g_counters.release();
         views.release();
         for (Grid* g : grids) delete g;
+        for (GroupIndex* G : groups) group_free(G);
         pool.destroy();
         if (owner_stream) {
             cudaStreamSynchronize(owner_stream);
@@ -88,6 +90,28 @@ gahhg_status build_exact_grid(Polygon* P, int device, cudaStream_t s, void** sca
     g->d_err = nullptr;
     g->d_counts = nullptr;
     g->classified = true;
+    return st;
+}
+
+// Builds the exact indexes of polys[0 .. count) together on stream s (a
+// worker's context).
+gahhg_status build_group(Polygon* const* polys, int count, int device, cudaStream_t s, void** scan,
+                         const int* top, const int* leaf, GroupIndex** out)
+{
+    Grid g;
+    g.device = device;
+    g.stream = s;
+    g.borrowed = true;
+    g.scan_state = *scan;
+    GAHHG_TRY(pool_alloc((void**)&g.d_err, sizeof(DeviceErrors), device, s));
+    GAHHG_TRY(pool_alloc((void**)&g.d_counts, 64 * sizeof(int), device, s));
+    GAHHG_CUDA_TRY(cudaMemsetAsync(g.d_err, 0, sizeof(DeviceErrors), s));
+    const gahhg_status st = lattice_build_group(&g, polys, count, top, leaf, out);
+    *scan = g.scan_state;  // the build may have grown it
+    cudaFreeAsync(g.d_err, s);
+    cudaFreeAsync(g.d_counts, s);
+    g.d_err = nullptr;
+    g.d_counts = nullptr;
     return st;
 }
 
@@ -157,6 +181,11 @@ gahhg_status WorkerPool::build_all(const std::vector<Polygon*>& polys, const gah
 
 }  // namespace gahhg
 
+// Edges per group build: every step of a group runs once for all of its
+// polygons, and its scratch grows with its edges (about 1 KB per edge at the
+// peak of a C1-like build).
+constexpr long long GROUP_EDGES = 1LL << 20;
+
 extern "C" {
 
 gahhg_status gahhg_batch_build(const gahhg_polygon* const* polys, int count, const gahhg_build_opts* opts,
@@ -185,34 +214,92 @@ gahhg_status gahhg_batch_build(const gahhg_polygon* const* polys, int count, con
         }
         B->polys[i] = const_cast<Polygon*>(&polys[i]->p);
     }
-    int nw = workers > 0 ? workers : (int)std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
+    // group builds keep the GPU busy with a few workers; more only add scratch memory
+    int nw = workers > 0 ? workers : (int)std::min(4u, std::max(1u, std::thread::hardware_concurrency()));
     nw = std::min(nw, count);
     if (B->pool.create(B->device, nw) != GAHHG_OK) {
         delete B;
         return GAHHG_ERR_CUDA;
     }
     const double t0 = now_seconds();
-    int failed = -1;
-    const gahhg_status bst = B->pool.build_all(B->polys, base, top_cells, leaf_edges, B->grids, &failed);
-    if (bst != GAHHG_OK) {
-        const std::string msg = last_error();
-        delete B;
-        set_error("gahhg_batch_build: %s", msg.c_str());
-        return bst;
+    // The workers' groups allocate and free their scratch concurrently: a
+    // pool that trims its cache at every synchronisation would return it to
+    // the driver and allocate it again, group after group.  Keep up to a
+    // quarter of the device's memory cached (the pool then holds it until the
+    // process exits or a later call lowers it).
+    {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) GAHHG_TRY(pool_keep(B->device, total_b / 4));
+    }
+    // groups of consecutive polygons of at most GROUP_EDGES edges (a larger
+    // polygon is a group of its own), built by the pool's workers
+    std::vector<int> gstart(1, 0);
+    {
+        long long e = 0;
+        for (int i = 0; i < count; i++) {
+            const long long n = B->polys[i]->pv_num;
+            if (i > gstart.back() && e + n > GROUP_EDGES) {
+                gstart.push_back(i);
+                e = 0;
+            }
+            e += n;
+        }
+        gstart.push_back(count);
+    }
+    const int ngroups = (int)gstart.size() - 1;
+    B->groups.assign(ngroups, nullptr);
+    {
+        std::atomic<int> next(0), bad(-1);
+        std::mutex mu;
+        std::string first_error;
+        gahhg_status first_status = GAHHG_OK;
+        auto worker = [&](int w) {
+            cudaSetDevice(B->device);
+            for (;;) {
+                const int k = next.fetch_add(1);
+                if (k >= ngroups || bad.load() >= 0) break;
+                const int i0 = gstart[k], i1 = gstart[k + 1];
+                const gahhg_status st =
+                    build_group(B->polys.data() + i0, i1 - i0, B->device, B->pool.streams[w], &B->pool.scans[w],
+                                top_cells ? top_cells + i0 : nullptr, leaf_edges ? leaf_edges + i0 : nullptr,
+                                &B->groups[k]);
+                if (st != GAHHG_OK) {
+                    std::lock_guard<std::mutex> lock(mu);
+                    if (bad.load() < 0) {
+                        bad.store(k);
+                        first_status = st;
+                        first_error = last_error();
+                    }
+                }
+            }
+            cudaStreamSynchronize(B->pool.streams[w]);
+        };
+        std::vector<std::thread> th;
+        const int nt = std::min(nw, ngroups);
+        for (int w = 0; w < nt; w++) th.emplace_back(worker, w);
+        for (auto& t : th) t.join();
+        if (bad.load() >= 0) {
+            delete B;
+            set_error("gahhg_batch_build: polygons %d..: %s", gstart[bad.load()], first_error.c_str());
+            return first_status;
+        }
     }
     // per-polygon query views, in one device table
     const size_t vb = lattice_view_bytes();
     std::vector<uint8_t> host(vb * count);
     long long bytes = 0, edges = 0;
-    for (int i = 0; i < count; i++) {
-        lattice_view_write(B->grids[i], host.data() + vb * i);
-        B->swords.push_back((int)lattice_summary_words(B->grids[i]));
-        bytes += (long long)lattice_bytes(B->grids[i]->lattice);
-        edges += B->polys[i]->pv_num;
-        if (lattice_summary_words(B->grids[i]) > 4096) {
-            delete B;
-            set_error("gahhg_batch_build: polygon %d's summary exceeds the batch kernel's shared memory", i);
-            return GAHHG_ERR_CAPACITY;
+    for (int k = 0; k < ngroups; k++) {
+        bytes += group_bytes(B->groups[k]);
+        for (int i = gstart[k]; i < gstart[k + 1]; i++) {
+            group_view_write(B->groups[k], i - gstart[k], host.data() + vb * i);
+            const long long sw = group_summary_words(B->groups[k], i - gstart[k]);
+            B->swords.push_back((int)sw);
+            edges += B->polys[i]->pv_num;
+            if (sw > 4096) {
+                delete B;
+                set_error("gahhg_batch_build: polygon %d's summary exceeds the batch kernel's shared memory", i);
+                return GAHHG_ERR_CAPACITY;
+            }
         }
     }
     cudaStream_t s0 = B->pool.streams[0];

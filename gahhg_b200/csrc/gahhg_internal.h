@@ -211,6 +211,15 @@ gahhg_status check_device_errors(Grid* g, const char* phase);
 
 // exact engine
 gahhg_status lattice_build(Grid* g);
+// Exact indexes of several polygons built together (shared launches); g
+// lends the device, stream, scratch counts, error word and scan state.
+struct GroupIndex;
+gahhg_status lattice_build_group(Grid* g, Polygon* const* polys, int count, const int* top_cells,
+                                 const int* leaf_edges, GroupIndex** out);
+void group_free(GroupIndex* G);
+void group_view_write(const GroupIndex* G, int i, void* dst);
+long long group_summary_words(const GroupIndex* G, int i);
+long long group_bytes(const GroupIndex* G);
 gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels, int precision,
                            cudaStream_t s, uint64_t* d_counters);
 gahhg_status lattice_query_noalloc(Grid* g, const double* d_lonlat, size_t n, uint8_t* d_labels, int precision,

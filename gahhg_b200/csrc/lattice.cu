@@ -112,6 +112,31 @@ struct Geo {
     bool full_lon, to_north, to_south;
 };
 
+// A polygon of a group build: its level-0 grid, first top node, leaf size
+// and first edge in the group's arrays.
+struct PolyGeo {
+    Geo g;
+    long long top;
+    int K;
+    int e0;
+};
+
+// The level-0 grid of a node's polygon: the build's one polygon, or a group
+// build's polygon table through the level's node -> polygon array; top() is
+// the polygon's first top node (child indices in node words are relative to
+// it).
+struct OneGeo {
+    Geo g;
+    __device__ __forceinline__ const Geo& of(long long) const { return g; }
+    __device__ __forceinline__ long long top(long long) const { return 0; }
+};
+struct TableGeo {
+    const PolyGeo* pg;
+    const int* npoly;
+    __device__ __forceinline__ const Geo& of(long long v) const { return pg[npoly[v]].g; }
+    __device__ __forceinline__ long long top(long long v) const { return pg[npoly[v]].top; }
+};
+
 // Node geometry from (level, ix, iy): center (degrees, exact), cap radius.
 struct NodeCap {
     double R[3];
@@ -269,11 +294,66 @@ struct EdgeBox {
 // very long edge has a box of up to millions of cells, and one thread per
 // edge would hold its block for tens of milliseconds.
 constexpr int L0_CHUNK = 64;
+// Work items whose hit masks the count pass keeps for the fill pass (8 bytes
+// each; beyond this the fill pass tests again).
+constexpr unsigned long long L0_MASK_ITEMS = 1ull << 26;
 
 __device__ inline int l0_chunks(int n) { return (n + L0_CHUNK - 1) / L0_CHUNK; }
 
 // Per edge: its candidate box and number of work items; total64 accumulates
 // the 64-bit item total (the 32-bit scan of the counts must not wrap).
+// Candidate box of edge AB in the level-0 grid g; returns its work items.
+__device__ long long edge_box(const Geo& g, const D3& A, const D3& B, EdgeBox& bx)
+{
+    const int W = g.W, H = g.H;
+    double la0, la1, lo0, lo1;
+    bool full;
+    arc_box(A, B, la0, la1, lo0, lo1, full);
+    const double rmax = (CAP_FACTOR * (0.5 * g.dlat0 + 0.5 * g.dlon0 * g.cap_cos) * RAD) * (1.0 + 1e-6) + LOC_MARGIN;
+    const double rdeg = rmax / RAD + 1e-9;
+    la0 -= rdeg;
+    la1 += rdeg;
+    int iy0 = (int)floor((la0 - g.lat0) / g.dlat0), iy1 = (int)floor((la1 - g.lat0) / g.dlat0);
+    iy0 = max(iy0, 0);
+    iy1 = min(iy1, H - 1);
+    const double maxlat = fmax(fabs(la0), fabs(la1));
+    long long r0a = 0, r0b = W - 1, r1a = 1, r1b = 0;
+    bool all_cols = full || maxlat >= 89.0;
+    if (!all_cols) {
+        const double c = cos(maxlat * RAD);
+        const double wdeg = rdeg / c;
+        const double len = (lo1 - lo0) + 2 * wdeg;
+        if (len >= 360.0) {
+            all_cols = true;
+        } else {
+            double a = lo0 - wdeg - g.lon0;
+            a -= 360.0 * floor(a / 360.0);  // [0, 360)
+            r0a = (long long)floor(a / g.dlon0);
+            r0b = (long long)floor((a + len) / g.dlon0);
+            if (a + len >= 360.0) {
+                r1a = 0;
+                r1b = (long long)floor((a + len - 360.0) / g.dlon0);
+            }
+        }
+    }
+    if (all_cols) {
+        r0a = 0;
+        r0b = W - 1;
+        r1a = 1;
+        r1b = 0;
+    }
+    r0a = max(r0a, 0LL);
+    r0b = min(r0b, (long long)W - 1);
+    r1b = min(r1b, (long long)W - 1);
+    bx.iy0 = iy0;
+    bx.nrows = max(0, iy1 - iy0 + 1);
+    bx.c0 = (int)r0a;
+    bx.n0 = (int)max(0LL, r0b - r0a + 1);
+    bx.c1 = (int)r1a;
+    bx.n1 = (int)max(0LL, r1b - r1a + 1);
+    return (long long)bx.nrows * (l0_chunks(bx.n0) + l0_chunks(bx.n1));
+}
+
 __global__ void k_l0_box(BuildView v, EdgeBox* box, int* items, unsigned long long* total64)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -281,56 +361,7 @@ __global__ void k_l0_box(BuildView v, EdgeBox* box, int* items, unsigned long lo
     if (t < v.n) {
         EdgeBox bx{0, 0, 0, 0, 0, 0};
         const D3 A = v.pv[v.pe[2 * t]], B = v.pv[v.pe[2 * t + 1]];
-        if (!(A.x == B.x && A.y == B.y && A.z == B.z)) {
-            const int W = v.g.W, H = v.g.H;
-            double la0, la1, lo0, lo1;
-            bool full;
-            arc_box(A, B, la0, la1, lo0, lo1, full);
-            const double rmax =
-                (CAP_FACTOR * (0.5 * v.g.dlat0 + 0.5 * v.g.dlon0 * v.g.cap_cos) * RAD) * (1.0 + 1e-6) + LOC_MARGIN;
-            const double rdeg = rmax / RAD + 1e-9;
-            la0 -= rdeg;
-            la1 += rdeg;
-            int iy0 = (int)floor((la0 - v.g.lat0) / v.g.dlat0), iy1 = (int)floor((la1 - v.g.lat0) / v.g.dlat0);
-            iy0 = max(iy0, 0);
-            iy1 = min(iy1, H - 1);
-            const double maxlat = fmax(fabs(la0), fabs(la1));
-            long long r0a = 0, r0b = W - 1, r1a = 1, r1b = 0;
-            bool all_cols = full || maxlat >= 89.0;
-            if (!all_cols) {
-                const double c = cos(maxlat * RAD);
-                const double wdeg = rdeg / c;
-                const double len = (lo1 - lo0) + 2 * wdeg;
-                if (len >= 360.0) {
-                    all_cols = true;
-                } else {
-                    double a = lo0 - wdeg - v.g.lon0;
-                    a -= 360.0 * floor(a / 360.0);  // [0, 360)
-                    r0a = (long long)floor(a / v.g.dlon0);
-                    r0b = (long long)floor((a + len) / v.g.dlon0);
-                    if (a + len >= 360.0) {
-                        r1a = 0;
-                        r1b = (long long)floor((a + len - 360.0) / v.g.dlon0);
-                    }
-                }
-            }
-            if (all_cols) {
-                r0a = 0;
-                r0b = W - 1;
-                r1a = 1;
-                r1b = 0;
-            }
-            r0a = max(r0a, 0LL);
-            r0b = min(r0b, (long long)W - 1);
-            r1b = min(r1b, (long long)W - 1);
-            bx.iy0 = iy0;
-            bx.nrows = max(0, iy1 - iy0 + 1);
-            bx.c0 = (int)r0a;
-            bx.n0 = (int)max(0LL, r0b - r0a + 1);
-            bx.c1 = (int)r1a;
-            bx.n1 = (int)max(0LL, r1b - r1a + 1);
-            nit = (long long)bx.nrows * (l0_chunks(bx.n0) + l0_chunks(bx.n1));
-        }
+        if (!(A.x == B.x && A.y == B.y && A.z == B.z)) nit = edge_box(v.g, A, B, bx);
         box[t] = bx;
         items[t] = (int)min(nit, (long long)INT_MAX);
     }
@@ -342,27 +373,48 @@ __global__ void k_l0_box(BuildView v, EdgeBox* box, int* items, unsigned long lo
 
 // Level-0 pairs over the work items (persistent grid; the item total is read
 // on the device).  PASS 0 counts per cell, PASS 1 fills the lists.
-template <int PASS>
-__global__ void k_l0_expand(BuildView v, const EdgeBox* __restrict__ box, const int* __restrict__ item_off,
+// The level-0 grid of an edge's polygon (the build's one, or a group's
+// table through the edge -> polygon array).
+struct EdgeGeoTable {
+    const PolyGeo* pg;
+    const int* epoly;
+    __device__ __forceinline__ const Geo& of(long long e) const { return pg[epoly[e]].g; }
+    __device__ __forceinline__ long long top(long long e) const { return pg[epoly[e]].top; }
+};
+
+// Level-0 pairs over the work items (persistent grid; the item total is read
+// on the device).  PASS 0 tests an item's cells (at most L0_CHUNK) and counts
+// per cell, recording the item's hits in mask[it] when mask is given; PASS 1
+// fills the lists from those masks (or tests again without them).
+template <int PASS, class GEO>
+__global__ void k_l0_expand(const D3* __restrict__ pv, const int* __restrict__ pe, long long ne, GEO geo,
+                            const EdgeBox* __restrict__ box, const int* __restrict__ item_off,
                             const int* total_items, const unsigned long long* total64, int* cnt, const int* off,
-                            int* cursor, int* list)
+                            int* cursor, int* list, unsigned long long* mask)
 {
+    static_assert(L0_CHUNK <= 64, "a 64-bit hit mask per item");
     if (*total64 > (unsigned long long)INT_MAX) return;  // the host reports it; the 32-bit offsets wrapped
     const int total = *total_items;
-    const int W = v.g.W, H = v.g.H;
     for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < total; it += gridDim.x * blockDim.x) {
-        int lo = 0, hi = v.n;  // the last edge whose first item is <= it
+        unsigned long long m = 0;
+        if (PASS == 1 && mask) {
+            m = mask[it];
+            if (!m) continue;
+        }
+        long long lo = 0, hi = ne;  // the last edge whose first item is <= it
         while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
+            const long long mid = (lo + hi) >> 1;
             if (item_off[mid] <= it) lo = mid;
             else hi = mid;
         }
-        const int t = lo;
+        const long long t = lo;
         const EdgeBox b = box[t];
+        const Geo& G = geo.of(t);
+        const int W = G.W, H = G.H;
         const int k0 = l0_chunks(b.n0), kk = k0 + l0_chunks(b.n1);
         const int local = it - item_off[t];
-        const int iy = b.iy0 + local / kk;
-        const int ch = local % kk;
+        const int iy = kk ? b.iy0 + local / kk : -1;
+        const int ch = kk ? local % kk : 0;
         int xa, xb;
         if (ch < k0) {
             xa = b.c0 + ch * L0_CHUNK;
@@ -371,17 +423,25 @@ __global__ void k_l0_expand(BuildView v, const EdgeBox* __restrict__ box, const 
             xa = b.c1 + (ch - k0) * L0_CHUNK;
             xb = min(b.c1 + b.n1, xa + L0_CHUNK);
         }
-        if (iy < 0 || iy >= H || xa < 0 || xb > W) continue;
-        const D3 A = v.pv[v.pe[2 * t]], B = v.pv[v.pe[2 * t + 1]];
-        for (int ix = xa; ix < xb; ix++) {
-            const NodeCap c = node_cap(v.g, 0, ix, iy);
-            if (!edge_hits_cap(A, B, c.R, c.r)) continue;
-            const int node = iy * W + ix;
-            if (PASS == 0) {
-                atomicAdd(&cnt[node], 1);
-            } else {
-                const int pos = off[node] + atomicAdd(&cursor[node], 1);
-                list[pos] = t;
+        if (iy < 0 || iy >= H || xa < 0 || xb > W) {
+            if (PASS == 0 && mask) mask[it] = 0;
+            continue;
+        }
+        const long long row = geo.top(t) + (long long)iy * W;
+        if (PASS == 0 || !mask) {
+            const D3 A = pv[pe[2 * t]], B = pv[pe[2 * t + 1]];
+            for (int ix = xa; ix < xb; ix++) {
+                const NodeCap c = node_cap(G, 0, ix, iy);
+                if (edge_hits_cap(A, B, c.R, c.r)) m |= 1ull << (ix - xa);
+            }
+        }
+        if (PASS == 0) {
+            if (mask) mask[it] = m;
+            for (unsigned long long r = m; r; r &= r - 1) atomicAdd(&cnt[row + xa + __ffsll((long long)r) - 1], 1);
+        } else {
+            for (unsigned long long r = m; r; r &= r - 1) {
+                const long long node = row + xa + __ffsll((long long)r) - 1;
+                list[off[node] + atomicAdd(&cursor[node], 1)] = (int)t;
             }
         }
     }
@@ -686,7 +746,8 @@ __device__ __forceinline__ bool center_on_vertex(const double* R, const D3* pv, 
 // every crossing test, orient(A, B, P), computed by lane k mod 16 for edge
 // k.  Child centers come from the pair pass's caps (node_cap, recomputed
 // only when a center must be nudged off a vertex).
-__global__ void __launch_bounds__(TPB) k_child_labels(BuildView v, int lvl, int nchild, const int* child_parent,
+template <class GEO>
+__global__ void __launch_bounds__(TPB) k_child_labels(BuildView v, GEO geo, int lvl, int nchild, const int* child_parent,
                                                       const long long* cix, const long long* ciy, const int* ccnt,
                                                       const int* coff, const int* clist,
                                                       const double4* __restrict__ ccaps,
@@ -701,9 +762,10 @@ __global__ void __launch_bounds__(TPB) k_child_labels(BuildView v, int lvl, int 
     const int gl = threadIdx.x & 15;
     const unsigned int grp = 0xFFFFu << (threadIdx.x & 16);
     NodeCap pc;
+    const Geo& G = geo.of(p);
     if (gl == 0) {
-        pc = node_cap(v.g, lvl, pix[p], piy[p]);
-        nudge_center(v.g, lvl, pc, v.pv, v.pe, plist + poff[p], pcnt[p]);
+        pc = node_cap(G, lvl, pix[p], piy[p]);
+        nudge_center(G, lvl, pc, v.pv, v.pe, plist + poff[p], pcnt[p]);
     }
     double P[3];
     P[0] = __shfl_sync(grp, pc.R[0], 0, 16);
@@ -719,8 +781,8 @@ __global__ void __launch_bounds__(TPB) k_child_labels(BuildView v, int lvl, int 
         cc.r = ccapsb[c].y;
     }
     if (center_on_vertex(cc.R, v.pv, v.pe, clist + coff[c], ccnt[c])) {
-        cc = node_cap(v.g, lvl + 1, cix[c], ciy[c]);
-        nudge_center(v.g, lvl + 1, cc, v.pv, v.pe, clist + coff[c], ccnt[c]);
+        cc = node_cap(G, lvl + 1, cix[c], ciy[c]);
+        nudge_center(G, lvl + 1, cc, v.pv, v.pe, clist + coff[c], ccnt[c]);
     }
     // nesting of caps: the child's cap must lie inside the parent's
     const double dx = P[0] - cc.R[0], dy = P[1] - cc.R[1], dz = P[2] - cc.R[2];
@@ -788,14 +850,15 @@ __global__ void k_arc_parity_all(const D3* pv, const int* pe, int n, const doubl
 }
 
 // Final node words, leaf records.
-__global__ void k_encode(int nn, int gstart, const int* cnt, const int* child_base, const uint8_t* label,
+template <class GEO>
+__global__ void k_encode(GEO geo, int nn, int gstart, const int* cnt, const int* child_base, const uint8_t* label,
                          const int* leaf_off, uint32_t* nodes)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nn) return;
     uint32_t w;
     if (child_base && child_base[p] >= 0)
-        w = KIND_INNER | (uint32_t)child_base[p];
+        w = KIND_INNER | (uint32_t)(child_base[p] - geo.top(p));
     else if (cnt[p] == 0)
         w = KIND_PURE | label[p];
     else
@@ -812,7 +875,8 @@ __global__ void k_leaf_flags(int nn, const int* cnt, const int* child_base, int*
     nrec[p] = leaf ? cnt[p] : 0;
 }
 
-__global__ void k_leaf_records(BuildView v, int lvl, int nn, const int* is_leaf, const int* leaf_off,
+template <class GEO>
+__global__ void k_leaf_records(BuildView v, GEO geo, int lvl, int nn, const int* is_leaf, const int* leaf_off,
                                const int* rec_off, int leaf_base, long long rec_base, const long long* ix,
                                const long long* iy, const int* cnt, const int* off, const int* list,
                                const uint8_t* label, LeafRec* leaves, float4* recs, uint32_t* eids, double* leafR,
@@ -820,8 +884,9 @@ __global__ void k_leaf_records(BuildView v, int lvl, int nn, const int* is_leaf,
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nn || !is_leaf[p]) return;
-    NodeCap c = node_cap(v.g, lvl, ix[p], iy[p]);
-    nudge_center(v.g, lvl, c, v.pv, v.pe, list + off[p], cnt[p]);
+    const Geo& G = geo.of(p);
+    NodeCap c = node_cap(G, lvl, ix[p], iy[p]);
+    nudge_center(G, lvl, c, v.pv, v.pe, list + off[p], cnt[p]);
     LeafRec L;
     L.lon = c.lonc;
     L.lat = c.latc;
@@ -2096,9 +2161,11 @@ struct LevelBuf {
     DevArray<int> cnt, off, cursor, list, pair_node, child_base, flag, foff;
     DevArray<long long> ix, iy;
     DevArray<uint8_t> label;
+    DevArray<int> poly;  // group builds: each node's polygon
     int npairs = 0;
     void release()
     {
+        poly.release();
         cnt.release();
         off.release();
         cursor.release();
@@ -2310,6 +2377,463 @@ __global__ void __launch_bounds__(TPB) k_domain_scan(const D3* __restrict__ pv, 
     }
 }
 
+// ----------------------------------------------------------- group builds --
+//
+// A batch's polygons are built in groups: every step of the exact-index build
+// runs once for all polygons of a group (shared launches over concatenated
+// edges and nodes, a polygon table for the per-polygon geometry), so a
+// group's launches and host round trips scale with its levels, not with its
+// polygons.  The steps are those of lattice_build, node for node and edge for
+// edge: a polygon's index is the one its own build gives, renumbered into the
+// group's arrays (node words hold child indices relative to the polygon's
+// first top node, so its query view sees its own numbering; leaves, records
+// and edge ids are group-wide).
+
+
+// base[0..n] ascending: the p with base[p] <= x < base[p + 1] (the last such
+// p when ranges are empty)
+__device__ __forceinline__ int find_range(const long long* __restrict__ base, int n, long long x)
+{
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(base + mid) <= x) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// group edge -> polygon; the polygon's vertex indices shifted to the group's
+__global__ void kb_edges(const long long* ebase, const long long* vbase, int np, long long ne, int* epoly, int* pe)
+{
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    const int p = find_range(ebase, np, e);
+    epoly[e] = p;
+    const int vb = (int)vbase[p];
+    pe[2 * e] += vb;
+    pe[2 * e + 1] += vb;
+}
+
+// k_domain_scan for every polygon of a group: per-edge results into the
+// edge's polygon's DomainOut with global atomics (bins read first, so most
+// edges set no bit that is already set)
+__global__ void __launch_bounds__(TPB) kb_domain_scan(const D3* __restrict__ pv, const int* __restrict__ pe,
+                                                      long long ne, const int* __restrict__ epoly, DomainOut* out)
+{
+    for (long long e0 = (long long)blockIdx.x * TPB; e0 < ne; e0 += (long long)gridDim.x * TPB) {
+        const long long e = e0 + threadIdx.x;
+        int p = -1;
+        double la0 = 90.0, la1 = -90.0;
+        bool fl = false, any = false;
+        int b0 = 0, b1 = -1;
+        if (e < ne) {
+            p = epoly[e];
+            const D3 a = pv[pe[2 * e]], b = pv[pe[2 * e + 1]];
+            if (!(a.x == b.x && a.y == b.y && a.z == b.z)) {
+                any = true;
+                double lo0, lo1;
+                const double dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+                if (dx * dx + dy * dy + dz * dz > 1e-4) {
+                    arc_box(a, b, la0, la1, lo0, lo1, fl);
+                } else {
+                    const double ta = lat_of(a), tb = lat_of(b);
+                    double oa = lon_of(a), ob = lon_of(b);
+                    la0 = fmin(ta, tb) - 1e-4;
+                    la1 = fmax(ta, tb) + 1e-4;
+                    if (oa > ob) {
+                        const double t = oa;
+                        oa = ob;
+                        ob = t;
+                    }
+                    if (ob - oa <= 180.0) {
+                        lo0 = oa;
+                        lo1 = ob;
+                    } else {
+                        lo0 = ob;
+                        lo1 = oa + 360.0;
+                    }
+                    if (fabs(ta) > 89.9 || fabs(tb) > 89.9) fl = true;
+                }
+                if (!fl) {
+                    b0 = (int)floor((lo0 + 180.0) * 10.0) - 1;
+                    b1 = (int)floor((lo1 + 180.0) * 10.0) + 1;
+                }
+            }
+        }
+        // a warp whose edges all belong to one polygon reduces before its atomics
+        const unsigned int same = __match_any_sync(0xffffffffu, p);
+        if (same == 0xffffffffu && p >= 0) {
+            double mn = la0, mx = la1;
+            for (int d = 16; d > 0; d >>= 1) {
+                mn = fmin(mn, __shfl_down_sync(0xffffffffu, mn, d));
+                mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, d));
+            }
+            const bool f = __any_sync(0xffffffffu, any && fl);
+            const bool a = __any_sync(0xffffffffu, any);
+            if ((threadIdx.x & 31) == 0 && a) {
+                atomicMin(&out[p].latmin, order_key(mn));
+                atomicMax(&out[p].latmax, order_key(mx));
+                if (f) atomicOr(&out[p].full, 1u);
+            }
+        } else if (p >= 0 && any) {
+            atomicMin(&out[p].latmin, order_key(la0));
+            atomicMax(&out[p].latmax, order_key(la1));
+            if (fl) atomicOr(&out[p].full, 1u);
+        }
+        if (p >= 0 && any && !fl) {
+            for (int k = b0; k <= b1 && k <= b0 + 3600; k++) {
+                const int bit = ((k % 3600) + 3600) % 3600;
+                unsigned int* w = &out[p].bins[bit >> 5];
+                if (!(*(volatile unsigned int*)w & (1u << (bit & 31)))) atomicOr(w, 1u << (bit & 31));
+            }
+        }
+    }
+}
+
+// Parity, count and last index of the group edges [e0, e1) crossing arc
+// P -> Q, summed over the block (as k_arc_parity_all); coincident is set
+// when an edge end coincides with P or Q.  Every thread of the block calls.
+__device__ void block_arc_parity(const D3* pv, const int* pe, long long e0, long long e1, const double* P,
+                                 const double* Q, int& parity, int& ncross, int& last, bool& coincident)
+{
+    __shared__ int s_par, s_cnt, s_last, s_co;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_par = 0;
+        s_cnt = 0;
+        s_last = -1;
+        s_co = 0;
+    }
+    __syncthreads();
+    int par = 0, cnt = 0, lst = -1, co = 0;
+    for (long long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        const D3 a = pv[pe[2 * e]], b = pv[pe[2 * e + 1]];
+        const double A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z};
+        if (exact::same(A, B)) continue;
+        if (exact::same(A, P) || exact::same(B, P) || exact::same(A, Q) || exact::same(B, Q)) {
+            co = 1;
+            continue;
+        }
+        if (exact::crossing(P, Q, A, B)) {
+            par ^= 1;
+            cnt++;
+            lst = max(lst, (int)(e - e0));
+        }
+    }
+    if (par) atomicXor(&s_par, 1);
+    if (cnt) atomicAdd(&s_cnt, cnt);
+    if (lst >= 0) atomicMax(&s_last, lst);
+    if (co) s_co = 1;
+    __syncthreads();
+    parity = s_par;
+    ncross = s_cnt;
+    last = s_last;
+    coincident = s_co != 0;
+    __syncthreads();
+}
+
+__constant__ double c_hubs[6][3] = {
+    {1.0, 0.000731, 0.000419},  {-1.0, 0.000627, -0.000883}, {0.000577, 1.0, 0.000941},
+    {-0.000351, -1.0, 0.000713}, {0.000809, -0.000467, 1.0}, {-0.000689, 0.000523, -1.0},
+};
+
+__device__ int nearest_hub_d(const double* q)
+{
+    int best = 0;
+    double bd = -1e300;
+    for (int k = 0; k < 6; k++) {
+        const double d = c_hubs[k][0] * q[0] + c_hubs[k][1] * q[1] + c_hubs[k][2] * q[2];
+        if (d > bd) {
+            bd = d;
+            best = k;
+        }
+    }
+    return best;
+}
+
+// One block per polygon: the reference point just left of an outer-ring
+// edge (reference_point) and the exact label of the first level-0 center
+// through the hubs (lattice_build's origin step).  origin[p] = the label, or
+// 0 when no outer edge gives a reference point, -1 when a hub or the center
+// coincides with a vertex.
+constexpr int ORIGIN_TPB = 512;
+__global__ void __launch_bounds__(ORIGIN_TPB) kb_origin(const D3* __restrict__ pv, const int* __restrict__ pe,
+                                                 const PolyGeo* __restrict__ pg, const long long* __restrict__ ebase,
+                                                 const int* __restrict__ nouter, int* origin)
+{
+    const int p = blockIdx.x;
+    const long long e0 = ebase[p], e1 = ebase[p + 1];
+    __shared__ double s_xi[3], s_xo[3];
+    __shared__ int s_ok;
+    bool found = false;
+    double xin[3] = {0.0, 0.0, 0.0};
+    for (int e = 0; e < nouter[p] && !found; e++) {
+        __syncthreads();  // every thread has read the previous candidate's s_ok
+        if (threadIdx.x == 0) {
+            s_ok = 0;
+            const D3 a = pv[pe[2 * (e0 + e)]], b = pv[pe[2 * (e0 + e) + 1]];
+            const double A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z};
+            double m[3] = {A[0] + B[0], A[1] + B[1], A[2] + B[2]};
+            const double nm = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+            const double N[3] = {A[1] * B[2] - A[2] * B[1], A[2] * B[0] - A[0] * B[2], A[0] * B[1] - A[1] * B[0]};
+            const double nn = sqrt(N[0] * N[0] + N[1] * N[1] + N[2] * N[2]);
+            if (!exact::same(A, B) && nm > 1e-3 && nn > 0) {
+                const double d[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
+                const double t = 1e-3 * sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+                double xi[3], xo[3];
+                for (int k = 0; k < 3; k++) {
+                    xi[k] = m[k] / nm + t * (N[k] / nn);
+                    xo[k] = m[k] / nm - t * (N[k] / nn);
+                }
+                if (exact::orient(A, B, xi) > 0 && exact::orient(A, B, xo) < 0) {
+                    for (int k = 0; k < 3; k++) {
+                        s_xi[k] = xi[k];
+                        s_xo[k] = xo[k];
+                    }
+                    s_ok = 1;
+                }
+            }
+        }
+        __syncthreads();
+        if (!s_ok) continue;  // the same in every thread
+        double xo[3] = {s_xo[0], s_xo[1], s_xo[2]}, xi[3] = {s_xi[0], s_xi[1], s_xi[2]};
+        int par, nc, le;
+        bool co;
+        block_arc_parity(pv, pe, e0, e1, xo, xi, par, nc, le, co);
+        if (!co && par == 1 && nc == 1 && le == e) {
+            found = true;
+            for (int k = 0; k < 3; k++) xin[k] = xi[k];
+        }
+    }
+    if (!found) {
+        if (threadIdx.x == 0) origin[p] = 0;
+        return;
+    }
+    const NodeCap c00 = node_cap(pg[p].g, 0, 0, 0);
+    double path[5][3];
+    int np = 0;
+    for (int k = 0; k < 3; k++) path[np][k] = xin[k];
+    np++;
+    const double ud = (xin[0] * c00.R[0] + xin[1] * c00.R[1] + xin[2] * c00.R[2]) /
+                      sqrt((xin[0] * xin[0] + xin[1] * xin[1] + xin[2] * xin[2]) *
+                           (c00.R[0] * c00.R[0] + c00.R[1] * c00.R[1] + c00.R[2] * c00.R[2]));
+    if (ud < 0.1) {
+        const int ha = nearest_hub_d(xin), hb = nearest_hub_d(c00.R);
+        for (int k = 0; k < 3; k++) path[np][k] = c_hubs[ha][k];
+        np++;
+        if ((ha ^ 1) == hb) {
+            for (int k = 0; k < 3; k++) path[np][k] = c_hubs[(ha + 2) % 6][k];
+            np++;
+        }
+        if (hb != ha) {
+            for (int k = 0; k < 3; k++) path[np][k] = c_hubs[hb][k];
+            np++;
+        }
+    }
+    for (int k = 0; k < 3; k++) path[np][k] = c00.R[k];
+    np++;
+    int label = CELL_IN;
+    for (int k = 0; k + 1 < np; k++) {
+        int par, nc, le;
+        bool co;
+        block_arc_parity(pv, pe, e0, e1, path[k], path[k + 1], par, nc, le, co);
+        if (co) {
+            if (threadIdx.x == 0) origin[p] = -1;
+            return;
+        }
+        if (par) label = 3 - label;
+    }
+    if (threadIdx.x == 0) origin[p] = label;
+}
+
+// k_l0_box for the group's edges (each in its polygon's grid)
+__global__ void kb_l0_box(const D3* __restrict__ pv, const int* __restrict__ pe, long long ne,
+                          const int* __restrict__ epoly, const PolyGeo* __restrict__ pg, EdgeBox* box, int* items,
+                          unsigned long long* total64)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long nit = 0;
+    if (t < ne) {
+        EdgeBox bx{0, 0, 0, 0, 0, 0};
+        const D3 A = pv[pe[2 * t]], B = pv[pe[2 * t + 1]];
+        if (!(A.x == B.x && A.y == B.y && A.z == B.z)) {
+            const Geo& G = pg[epoly[t]].g;
+            nit = edge_box(G, A, B, bx);
+        }
+        box[t] = bx;
+        items[t] = (int)min(nit, (long long)INT_MAX);
+    }
+    unsigned long long w = (unsigned long long)nit;
+    for (int d = 16; d > 0; d >>= 1) w += __shfl_down_sync(0xffffffffu, w, d);
+    if ((threadIdx.x & 31) == 0 && w) atomicAdd(total64, w);
+}
+
+// Level-0 node coordinates and polygons.
+__global__ void kb_l0_coords(const long long* __restrict__ tops, int np, const PolyGeo* __restrict__ pg, int nn,
+                             long long* ix, long long* iy, int* npoly)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nn) return;
+    const int p = find_range(tops, np, v);
+    const long long local = v - pg[p].top;
+    const int W = pg[p].g.W;
+    ix[v] = local % W;
+    iy[v] = local / W;
+    npoly[v] = p;
+}
+
+// k_l0_neighbour_parity for the group: per polygon its W (H - 1) vertical
+// pairs, then its W - 1 horizontal pairs of row 0, from pb[p] in `par`.
+__global__ void kb_l0_neighbour_parity(const D3* __restrict__ pv, const int* __restrict__ pe,
+                                       const PolyGeo* __restrict__ pg, const long long* __restrict__ pb, int np,
+                                       const int* cnt, const int* off, const int* list, uint8_t* par, int* bad)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= pb[np]) return;
+    const int p = find_range(pb, np, t);
+    const PolyGeo& P = pg[p];
+    const int W = P.g.W, H = P.g.H;
+    const long long u = t - pb[p];
+    const long long nv = (long long)W * (H - 1);
+    int i, j, i2, j2;
+    if (u < nv) {
+        i = (int)(u % W);
+        j = (int)(u / W);
+        i2 = i;
+        j2 = j + 1;
+    } else {
+        i = (int)(u - nv);
+        j = 0;
+        i2 = i + 1;
+        j2 = 0;
+    }
+    const long long a0 = P.top + (long long)j * W + i, b0 = P.top + (long long)j2 * W + i2;
+    uint8_t r = 0;
+    if (cnt[a0] || cnt[b0]) {
+        NodeCap a = node_cap(P.g, 0, i, j), b = node_cap(P.g, 0, i2, j2);
+        nudge_center(P.g, 0, a, pv, pe, list + off[a0], cnt[a0]);
+        nudge_center(P.g, 0, b, pv, pe, list + off[b0], cnt[b0]);
+        r = (uint8_t)arc_parity_lists(pv, pe, a.R, b.R, list + off[a0], cnt[a0], list + off[b0], cnt[b0], bad);
+    }
+    par[t] = r;
+}
+
+// k_l0_labels for the group: one thread per column of every polygon (cb[p]:
+// the polygon's first column).
+__global__ void kb_l0_labels(const PolyGeo* __restrict__ pg, const long long* __restrict__ cb,
+                             const long long* __restrict__ pb, int np, const uint8_t* __restrict__ par,
+                             const int* __restrict__ origin, uint8_t* label)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= cb[np]) return;
+    const int p = find_range(cb, np, t);
+    const PolyGeo& P = pg[p];
+    const int W = P.g.W, H = P.g.H;
+    const int i = (int)(t - cb[p]);
+    const uint8_t* vpar = par + pb[p];
+    const uint8_t* hpar = vpar + (long long)W * (H - 1);
+    int l = origin[p];  // 1 or 2
+    for (int k = 0; k < i; k++)
+        if (hpar[k]) l = 3 - l;
+    label[P.top + i] = (uint8_t)l;
+    for (int j = 1; j < H; j++) {
+        if (vpar[(long long)(j - 1) * W + i]) l = 3 - l;
+        label[P.top + (long long)j * W + i] = (uint8_t)l;
+    }
+}
+
+// k_outside_label for every polygon with a region outside its domain
+// (oxy[p] = (ix, iy, ox, oy) from the host, ox == INT_MIN: none).
+__global__ void kb_outside_label(const D3* __restrict__ pv, const int* __restrict__ pe,
+                                 const PolyGeo* __restrict__ pg, int np, const int4* __restrict__ oxy,
+                                 const int* cnt, const int* off, const int* list, const uint8_t* label, uint8_t* out,
+                                 int* bad)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    const int4 o = oxy[p];
+    if (o.z == INT_MIN) {
+        out[p] = CELL_UNDEFINED;
+        return;
+    }
+    const PolyGeo& P = pg[p];
+    const long long v = P.top + (long long)o.y * P.g.W + o.x;
+    NodeCap a = node_cap(P.g, 0, o.x, o.y);
+    nudge_center(P.g, 0, a, pv, pe, list + off[v], cnt[v]);
+    const NodeCap b = node_cap(P.g, 0, o.z, o.w);
+    const int par = arc_parity_lists(pv, pe, a.R, b.R, list + off[v], cnt[v], nullptr, 0, bad);
+    out[p] = (uint8_t)(par ? 3 - label[v] : label[v]);
+}
+
+__global__ void kb_refine_flags(const int* cnt, const int* npoly, const PolyGeo* __restrict__ pg, int nn, int* flag)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < nn) flag[v] = cnt[v] > pg[npoly[v]].K ? 1 : 0;
+}
+
+// k_make_children for the group: children take their parent's polygon
+__global__ void kb_make_children(const int* flag, const int* foff, int nn, int cstart, const long long* pix,
+                                 const long long* piy, const int* npoly, int* child_base, long long* cix,
+                                 long long* ciy, int* cpoly)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nn) return;
+    if (!flag[v]) {
+        child_base[v] = -1;
+        return;
+    }
+    child_base[v] = cstart + foff[v] * FAN * FAN;
+    const long long px = pix[v], py = piy[v];
+    for (int cy = 0; cy < FAN; cy++)
+        for (int cx = 0; cx < FAN; cx++) {
+            const int c = foff[v] * FAN * FAN + cy * FAN + cx;
+            cix[c] = px * FAN + cx;
+            ciy[c] = py * FAN + cy;
+            cpoly[c] = npoly[v];
+        }
+}
+
+__global__ void kb_child_caps(const PolyGeo* __restrict__ pg, int lvl, int nn, const long long* ix,
+                              const long long* iy, const int* cpoly, double4* caps, double2* capsb)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nn) return;
+    const NodeCap nc = node_cap(pg[cpoly[c]].g, lvl, ix[c], iy[c]);
+    caps[c] = make_double4(nc.R[0], nc.R[1], nc.R[2], cap_chord2(nc.r));
+    capsb[c] = make_double2(cap_sin_bound(nc.r), nc.r);
+}
+
+// k_summary for every polygon: coarse cell c of polygon p (sc[p]: its first
+// cell in the group) into its summary words from soff[p]
+__global__ void kb_summary(const uint32_t* nodes, const PolyGeo* __restrict__ pg, const long long* __restrict__ sc,
+                           const int* __restrict__ cshift, const long long* __restrict__ soff, int np,
+                           uint32_t* summary)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= sc[np]) return;
+    const int p = find_range(sc, np, t);
+    const int c = (int)(t - sc[p]);
+    const int W = pg[p].g.W, H = pg[p].g.H, cs = cshift[p];
+    const int f = 1 << cs;
+    const int CW = (W + f - 1) >> cs;
+    const int cx = c % CW, cy = c / CW;
+    const uint32_t* top = nodes + pg[p].top;
+    uint32_t code = 0xFFu;
+    for (int y = cy * f; y < min((cy + 1) * f, H) && code != 2u; y++)
+        for (int x = cx * f; x < min((cx + 1) * f, W); x++) {
+            const uint32_t w = top[(size_t)y * W + x];
+            const uint32_t v = ((w & KIND_MASK) == KIND_PURE) ? (w & 3u) - 1u : 2u;  // 0 out, 1 in, 2 mixed
+            if (code == 0xFFu) code = v;
+            else if (code != v) code = 2u;
+            if (code == 2u) break;
+        }
+    atomicOr(&summary[soff[p] + (c >> 4)], code << ((c & 15) * 2));
+}
+
+
+gahhg_status geo_from_scan(const DomainOut& h, const Polygon* P, long long target, Geo* G);
+
 gahhg_status compute_domain(const Polygon* P, long long target, Geo* G, cudaStream_t s, int device)
 {
     DomainOut h;
@@ -2327,6 +2851,12 @@ gahhg_status compute_domain(const Polygon* P, long long target, Geo* G, cudaStre
         cudaFreeAsync(d, s);
         GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
     }
+    return geo_from_scan(h, P, target, G);
+}
+
+// The level-0 grid from the domain scan's result (host).
+gahhg_status geo_from_scan(const DomainOut& h, const Polygon* P, long long target, Geo* G)
+{
     double latmin = h.latmax == 0ull ? 90.0 : from_order_key(h.latmin);
     double latmax = h.latmax == 0ull ? -90.0 : from_order_key(h.latmax);
     bool full = h.full != 0;
@@ -2526,12 +3056,7 @@ gahhg_status lattice_build(Grid* g)
     k_l0_box<<<blocks_for(n), TPB, 0, s>>>(bv, boxes.ptr, items.ptr, d_items64);
     GAHHG_TRY(scan_state_reserve(&g->scan_state, std::max(n, l0.nn)));
     GAHHG_TRY(scan_exclusive(items.ptr, item_off.ptr, n, d_items, g->scan_state, g->d_err, s));
-    k_l0_expand<0><<<sms * 8, TPB, 0, s>>>(bv, boxes.ptr, item_off.ptr, d_items, d_items64, l0.cnt.ptr, nullptr,
-                                            nullptr, nullptr);
-    GAHHG_TRY(scan_exclusive(l0.cnt.ptr, l0.off.ptr, l0.nn, g->d_counts + 8, g->scan_state, g->d_err, s));
-    int total = 0;
     unsigned long long items64 = 0;
-    GAHHG_CUDA_TRY(cudaMemcpyAsync(&total, g->d_counts + 8, sizeof(int), cudaMemcpyDeviceToHost, s));
     GAHHG_CUDA_TRY(cudaMemcpyAsync(&items64, d_items64, sizeof(items64), cudaMemcpyDeviceToHost, s));
     GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
     if (items64 > (unsigned long long)INT_MAX) {
@@ -2539,11 +3064,22 @@ gahhg_status lattice_build(Grid* g)
                   items64);
         return GAHHG_ERR_CAPACITY;
     }
+    // the count pass's hits per item, so the fill pass does not test again
+    DevArray<unsigned long long> hits;
+    if (items64 <= L0_MASK_ITEMS) GAHHG_TRY(hits.reserve(std::max<unsigned long long>(items64, 1), s, false));
+    const OneGeo one{L->geo};
+    k_l0_expand<0><<<sms * 8, TPB, 0, s>>>(bv.pv, bv.pe, (long long)n, one, boxes.ptr, item_off.ptr, d_items,
+                                            d_items64, l0.cnt.ptr, nullptr, nullptr, nullptr, hits.ptr);
+    GAHHG_TRY(scan_exclusive(l0.cnt.ptr, l0.off.ptr, l0.nn, g->d_counts + 8, g->scan_state, g->d_err, s));
+    int total = 0;
+    GAHHG_CUDA_TRY(cudaMemcpyAsync(&total, g->d_counts + 8, sizeof(int), cudaMemcpyDeviceToHost, s));
+    GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
     phase("l0 count");
     l0.npairs = total;
     GAHHG_TRY(l0.list.reserve(std::max(total, 1), s, false));
-    k_l0_expand<1><<<sms * 8, TPB, 0, s>>>(bv, boxes.ptr, item_off.ptr, d_items, d_items64, l0.cnt.ptr, l0.off.ptr,
-                                            l0.cursor.ptr, l0.list.ptr);
+    k_l0_expand<1><<<sms * 8, TPB, 0, s>>>(bv.pv, bv.pe, (long long)n, one, boxes.ptr, item_off.ptr, d_items,
+                                            d_items64, l0.cnt.ptr, l0.off.ptr, l0.cursor.ptr, l0.list.ptr, hits.ptr);
+    hits.release();
     boxes.release();
     items.release();
     item_off.release();
@@ -2667,7 +3203,7 @@ gahhg_status lattice_build(Grid* g)
         GAHHG_TRY(child_parent.reserve(cl.nn, s, false));
         k_child_parent<<<blocks_for(pp.nn), TPB, 0, s>>>(pp.child_base.ptr, pp.nn, cl.gstart, child_parent.ptr);
         GAHHG_TRY(cl.label.reserve(cl.nn, s, false));
-        k_child_labels<<<blocks_for(cl.nn), TPB, 0, s>>>(bv, lvl, cl.nn, child_parent.ptr, cl.ix.ptr, cl.iy.ptr,
+        k_child_labels<<<blocks_for(cl.nn), TPB, 0, s>>>(bv, OneGeo{L->geo}, lvl, cl.nn, child_parent.ptr, cl.ix.ptr, cl.iy.ptr,
                                                          cl.cnt.ptr, cl.off.ptr, cl.list.ptr, caps.ptr, capsb.ptr,
                                                          pp.ix.ptr, pp.iy.ptr, pp.cnt.ptr, pp.off.ptr, pp.list.ptr,
                                                          pp.label.ptr, cl.label.ptr, d_bad);
@@ -2703,7 +3239,7 @@ gahhg_status lattice_build(Grid* g)
         GAHHG_TRY(scan_exclusive(nrec[lvl].ptr, rec_off[lvl].ptr, b.nn, d_tot.ptr + 2 * lvl + 1, g->scan_state,
                                  g->d_err, s));
         // leaf indices are per level here: shifted by the level's leaf base below
-        k_encode<<<blocks_for(b.nn), TPB, 0, s>>>(b.nn, b.gstart, b.cnt.ptr, cb, b.label.ptr, leaf_off[lvl].ptr,
+        k_encode<<<blocks_for(b.nn), TPB, 0, s>>>(OneGeo{L->geo}, b.nn, b.gstart, b.cnt.ptr, cb, b.label.ptr, leaf_off[lvl].ptr,
                                                   L->nodes.ptr);
     }
     {
@@ -2735,7 +3271,7 @@ gahhg_status lattice_build(Grid* g)
     k_edge_ends<<<blocks_for(n), TPB, 0, s>>>(bv.pv, bv.pe, n, L->ends.ptr);
     for (int lvl = 0; lvl < L->nlev; lvl++) {
         LevelBuf& b = lv[lvl];
-        k_leaf_records<<<blocks_for(b.nn), TPB, 0, s>>>(bv, lvl, b.nn, is_leaf[lvl].ptr, leaf_off[lvl].ptr,
+        k_leaf_records<<<blocks_for(b.nn), TPB, 0, s>>>(bv, OneGeo{L->geo}, lvl, b.nn, is_leaf[lvl].ptr, leaf_off[lvl].ptr,
                                                         rec_off[lvl].ptr, leaf_base[lvl], rec_base[lvl], b.ix.ptr,
                                                         b.iy.ptr, b.cnt.ptr, b.off.ptr, b.list.ptr, b.label.ptr,
                                                         L->leaves.ptr, L->recs.ptr, L->eids.ptr, L->leafR.ptr,
@@ -2787,22 +3323,40 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
                                 unsigned int* qcount, long long chunk, int device, const Tiers* tiers,
                                 const PartScratch* part = nullptr);
 
+// The locate arithmetic of a view from its level-0 grid.
+static void set_view_geo(QueryView& Q, const Geo& g)
+{
+    Q.W = g.W;
+    Q.H = g.H;
+    Q.Wd = (double)g.W;
+    Q.Hd = (double)g.H;
+    Q.su_lon = 1.0 / g.dlon0;
+    Q.su_lat = 1.0 / g.dlat0;
+    Q.u0 = -g.lon0 * Q.su_lon;
+    Q.v0 = -(g.lat0 + 90.0) * Q.su_lat;
+    Q.U360 = 360.0 * Q.su_lon;
+    Q.full_lon = g.full_lon;
+    Q.to_north = g.to_north;
+    Q.to_south = g.to_south;
+}
+
+// Coarse summary shape of a level-0 grid: cells of 2^cshift x 2^cshift top
+// cells, at most 65,536 of them (16 KB of 2-bit codes).
+static void summary_shape(int W, int H, int* cshift, int* CW, int* CH)
+{
+    int cs = 0;
+    auto blocks = [&](int c) { return (long long)((W + (1 << c) - 1) >> c) * ((H + (1 << c) - 1) >> c); };
+    while (blocks(cs) > 65536) cs++;
+    *cshift = cs;
+    *CW = (W + (1 << cs) - 1) >> cs;
+    *CH = (H + (1 << cs) - 1) >> cs;
+}
+
 QueryView make_view(const Grid* g)
 {
     const Lattice* L = g->lattice;
     QueryView Q;
-    Q.W = L->geo.W;
-    Q.H = L->geo.H;
-    Q.Wd = (double)L->geo.W;
-    Q.Hd = (double)L->geo.H;
-    Q.su_lon = 1.0 / L->geo.dlon0;
-    Q.su_lat = 1.0 / L->geo.dlat0;
-    Q.u0 = -L->geo.lon0 * Q.su_lon;
-    Q.v0 = -(L->geo.lat0 + 90.0) * Q.su_lat;
-    Q.U360 = 360.0 * Q.su_lon;
-    Q.full_lon = L->geo.full_lon;
-    Q.to_north = L->geo.to_north;
-    Q.to_south = L->geo.to_south;
+    set_view_geo(Q, L->geo);
     Q.outside = KIND_PURE | (uint32_t)L->outside_label;
     Q.nodes = L->nodes.ptr;
     Q.leaves = L->leaves.ptr;
@@ -2823,6 +3377,517 @@ QueryView make_view(const Grid* g)
     if (L->nleaves < 2 * PART_MAX) Q.nparts = 1;
     Q.part_scale = Q.nparts > 1 ? (float)((double)Q.nparts / (double)L->nleaves) : 0.0f;
     return Q;
+}
+
+// ------------------------------------------------------ group build host --
+
+struct GroupIndex {
+    int count = 0;
+    DevArray<D3> pv;        // the group's vertices, polygon after polygon
+    DevArray<int> pe;       // its edges (group vertex indices)
+    DevArray<uint32_t> nodes;
+    DevArray<LeafRec> leaves;
+    DevArray<float4> recs;
+    DevArray<uint32_t> eids;
+    DevArray<double2> ends;
+    DevArray<double> leafR;
+    DevArray<uint32_t> summary;
+    std::vector<QueryView> views;  // per polygon
+    std::vector<int> swords;
+    long long nnodes = 0, nleaves = 0, nrecs = 0, nedges = 0;
+    void release()
+    {
+        pv.release();
+        pe.release();
+        nodes.release();
+        leaves.release();
+        recs.release();
+        eids.release();
+        ends.release();
+        leafR.release();
+        summary.release();
+    }
+};
+
+void group_free(GroupIndex* G)
+{
+    if (!G) return;
+    G->release();
+    delete G;
+}
+
+void group_view_write(const GroupIndex* G, int i, void* dst) { memcpy(dst, &G->views[i], sizeof(QueryView)); }
+long long group_summary_words(const GroupIndex* G, int i) { return G->swords[i]; }
+long long group_bytes(const GroupIndex* G)
+{
+    return G->nnodes * (long long)sizeof(uint32_t) + G->nleaves * (long long)(sizeof(LeafRec) + 3 * sizeof(double)) +
+           G->nrecs * (long long)(sizeof(float4) + sizeof(uint32_t)) + G->nedges * 3 * (long long)sizeof(double2);
+}
+
+namespace {
+
+// host array -> device array on s (the device array is reserved here)
+template <class T>
+gahhg_status upload(DevArray<T>& d, const std::vector<T>& h, cudaStream_t s)
+{
+    GAHHG_TRY(d.reserve(std::max<size_t>(h.size(), 1), s, false));
+    if (!h.empty()) GAHHG_CUDA_TRY(cudaMemcpyAsync(d.ptr, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
+    return GAHHG_OK;
+}
+
+}  // namespace
+
+// Exact indexes of polys[0 .. count) built together on stream s (g carries
+// the device, the scratch counts and error word and the scan state).  The
+// steps and their order follow lattice_build; see the group kernels above.
+gahhg_status lattice_build_group(Grid* g, Polygon* const* polys, int count, const int* top_cells,
+                                 const int* leaf_edges, GroupIndex** out)
+{
+    cudaStream_t s = g->stream;
+    const int np = count;
+    // GAHHG_DEBUG: wall time of each phase (synchronising) on stderr
+    const bool dbg = getenv("GAHHG_DEBUG") != nullptr;
+    double tph = now_seconds();
+    auto phase = [&](const char* name) {
+        if (!dbg) return;
+        cudaStreamSynchronize(s);
+        const double t = now_seconds();
+        fprintf(stderr, "group phase %-12s %9.3f ms (%d polygons)\n", name, (t - tph) * 1e3, np);
+        tph = t;
+    };
+    GroupIndex* GI = new GroupIndex();
+    *out = GI;
+    GI->count = np;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
+
+    // ---- edges and vertices of the group
+    std::vector<long long> ebase(np + 1, 0), vbase(np + 1, 0);
+    std::vector<int> nouter(np);
+    for (int p = 0; p < np; p++) {
+        const Polygon* P = polys[p];
+        ebase[p + 1] = ebase[p] + P->pv_num;
+        vbase[p + 1] = vbase[p] + (long long)P->pv.size();
+        nouter[p] = P->ring_start.size() > 1 ? P->ring_start[1] : P->pv_num;
+    }
+    const long long ne = ebase[np], nvx = vbase[np];
+    if (ne >= INT_MAX / 2 || nvx >= INT_MAX) {
+        set_error("exact index group: %lld edges exceed the group limit", ne);
+        return GAHHG_ERR_CAPACITY;
+    }
+    GI->nedges = ne;
+    GAHHG_TRY(GI->pv.reserve(std::max(nvx, 1LL), s, false));
+    GAHHG_TRY(GI->pe.reserve(std::max(2 * ne, 1LL), s, false));
+    for (int p = 0; p < np; p++) {
+        const Polygon* P = polys[p];
+        if (P->pv_num == 0) continue;
+        GAHHG_CUDA_TRY(cudaMemcpyAsync(GI->pv.ptr + vbase[p], P->pv.data(), sizeof(D3) * P->pv.size(),
+                                       cudaMemcpyHostToDevice, s));
+        GAHHG_CUDA_TRY(cudaMemcpyAsync(GI->pe.ptr + 2 * ebase[p], P->pe.data(), sizeof(int) * 2 * P->pv_num,
+                                       cudaMemcpyHostToDevice, s));
+    }
+    DevArray<long long> d_ebase, d_vbase;
+    DevArray<int> epoly, d_nouter;
+    GAHHG_TRY(upload(d_ebase, ebase, s));
+    GAHHG_TRY(upload(d_vbase, vbase, s));
+    GAHHG_TRY(upload(d_nouter, nouter, s));
+    GAHHG_TRY(epoly.reserve(std::max(ne, 1LL), s, false));
+    kb_edges<<<(int)((ne + TPB - 1) / TPB), TPB, 0, s>>>(d_ebase.ptr, d_vbase.ptr, np, ne, epoly.ptr, GI->pe.ptr);
+    const D3* pv = GI->pv.ptr;
+    const int* pe = GI->pe.ptr;
+    BuildView bv{Geo{}, pv, pe, (int)ne};
+
+    phase("upload");
+    // ---- domains (one scan for every polygon, one round trip)
+    std::vector<PolyGeo> pg(np);
+    std::vector<long long> tops(np + 1, 0);
+    {
+        std::vector<DomainOut> h(np);
+        for (auto& d : h) {
+            memset(&d, 0, sizeof d);
+            d.latmin = ~0ull;
+        }
+        DevArray<DomainOut> d;
+        GAHHG_TRY(upload(d, h, s));
+        const int grid = (int)std::max(1LL, std::min<long long>(sms * 8LL, (ne + TPB - 1) / TPB));
+        kb_domain_scan<<<grid, TPB, 0, s>>>(pv, pe, ne, epoly.ptr, d.ptr);
+        GAHHG_CUDA_TRY(cudaMemcpyAsync(h.data(), d.ptr, sizeof(DomainOut) * np, cudaMemcpyDeviceToHost, s));
+        GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+        d.release();
+        // the level-0 grids on host threads (a polygon's takes tens of microseconds)
+        std::vector<gahhg_status> st(np, GAHHG_OK);
+        std::vector<std::string> msg(np);
+        auto geo_range = [&](int p0, int p1) {
+            for (int p = p0; p < p1; p++) {
+                const Polygon* P = polys[p];
+                const long long n = P->pv_num;
+                const long long target = top_cells && top_cells[p] > 0
+                                             ? (long long)top_cells[p]
+                                             : std::min<long long>(std::max<long long>(8LL * n, 1024), 8LL << 20);
+                st[p] = geo_from_scan(h[p], P, target, &pg[p].g);
+                if (st[p] != GAHHG_OK) msg[p] = last_error();
+            }
+        };
+        const int nt = std::max(1, std::min({np / 16, 16, (int)std::max(1u, std::thread::hardware_concurrency())}));
+        if (nt == 1) {
+            geo_range(0, np);
+        } else {
+            std::vector<std::thread> th;
+            for (int t = 0; t < nt; t++) th.emplace_back(geo_range, (int)((long long)np * t / nt), (int)((long long)np * (t + 1) / nt));
+            for (auto& t : th) t.join();
+        }
+        for (int p = 0; p < np; p++) {
+            if (st[p] != GAHHG_OK) {
+                set_error("polygon %d: %s", p, msg[p].c_str());
+                return st[p];
+            }
+            pg[p].K = leaf_edges && leaf_edges[p] > 0 ? leaf_edges[p] : 8;
+            pg[p].e0 = (int)ebase[p];
+            pg[p].top = tops[p];
+            tops[p + 1] = tops[p] + (long long)pg[p].g.W * pg[p].g.H;
+        }
+    }
+    const long long n0 = tops[np];
+    if (n0 >= NODE_BUDGET) {
+        set_error("exact index group: %lld level-0 cells exceed the node budget", n0);
+        return GAHHG_ERR_CAPACITY;
+    }
+    DevArray<PolyGeo> d_pg;
+    DevArray<long long> d_tops;
+    GAHHG_TRY(upload(d_pg, pg, s));
+    GAHHG_TRY(upload(d_tops, tops, s));
+
+    phase("domain");
+    // ---- exact label of every polygon's first level-0 center
+    DevArray<int> origin;
+    GAHHG_TRY(origin.reserve(np, s, false));
+    kb_origin<<<np, ORIGIN_TPB, 0, s>>>(pv, pe, d_pg.ptr, d_ebase.ptr, d_nouter.ptr, origin.ptr);
+
+    phase("origin");
+    // ---- level 0: candidate boxes in work items, pair tests, lists
+    std::vector<LevelBuf> lv(1);
+    LevelBuf& l0 = lv[0];
+    l0.nn = (int)n0;
+    l0.gstart = 0;
+    GAHHG_TRY(l0.cnt.reserve(l0.nn, s, false));
+    GAHHG_TRY(l0.off.reserve(l0.nn, s, false));
+    GAHHG_TRY(l0.cursor.reserve(l0.nn, s, false));
+    GAHHG_CUDA_TRY(cudaMemsetAsync(l0.cnt.ptr, 0, sizeof(int) * l0.nn, s));
+    GAHHG_CUDA_TRY(cudaMemsetAsync(l0.cursor.ptr, 0, sizeof(int) * l0.nn, s));
+    {
+        DevArray<EdgeBox> boxes;
+        DevArray<int> items, item_off;
+        GAHHG_TRY(boxes.reserve(std::max(ne, 1LL), s, false));
+        GAHHG_TRY(items.reserve(std::max(ne, 1LL), s, false));
+        GAHHG_TRY(item_off.reserve(std::max(ne, 1LL), s, false));
+        unsigned long long* d_items64 = reinterpret_cast<unsigned long long*>(g->d_counts + 16);
+        int* d_items = g->d_counts + 18;
+        GAHHG_CUDA_TRY(cudaMemsetAsync(d_items64, 0, sizeof(unsigned long long), s));
+        kb_l0_box<<<(int)((ne + TPB - 1) / TPB), TPB, 0, s>>>(pv, pe, ne, epoly.ptr, d_pg.ptr, boxes.ptr, items.ptr,
+                                                              d_items64);
+        GAHHG_TRY(scan_state_reserve(&g->scan_state, (int)std::max<long long>(ne, l0.nn)));
+        GAHHG_TRY(scan_exclusive(items.ptr, item_off.ptr, (int)ne, d_items, g->scan_state, g->d_err, s));
+        unsigned long long items64 = 0;
+        GAHHG_CUDA_TRY(cudaMemcpyAsync(&items64, d_items64, sizeof(items64), cudaMemcpyDeviceToHost, s));
+        GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+        if (items64 > (unsigned long long)INT_MAX) {
+            set_error("exact index group: %llu level-0 candidate work items exceed 2^31", items64);
+            return GAHHG_ERR_CAPACITY;
+        }
+        DevArray<unsigned long long> hits;
+        if (items64 <= L0_MASK_ITEMS) GAHHG_TRY(hits.reserve(std::max<unsigned long long>(items64, 1), s, false));
+        const EdgeGeoTable eg{d_pg.ptr, epoly.ptr};
+        k_l0_expand<0><<<sms * 8, TPB, 0, s>>>(pv, pe, ne, eg, boxes.ptr, item_off.ptr, d_items, d_items64,
+                                                l0.cnt.ptr, nullptr, nullptr, nullptr, hits.ptr);
+        GAHHG_TRY(scan_exclusive(l0.cnt.ptr, l0.off.ptr, l0.nn, g->d_counts + 8, g->scan_state, g->d_err, s));
+        int total = 0;
+        GAHHG_CUDA_TRY(cudaMemcpyAsync(&total, g->d_counts + 8, sizeof(int), cudaMemcpyDeviceToHost, s));
+        GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+        l0.npairs = total;
+        GAHHG_TRY(l0.list.reserve(std::max(total, 1), s, false));
+        k_l0_expand<1><<<sms * 8, TPB, 0, s>>>(pv, pe, ne, eg, boxes.ptr, item_off.ptr, d_items, d_items64,
+                                                l0.cnt.ptr, l0.off.ptr, l0.cursor.ptr, l0.list.ptr, hits.ptr);
+        hits.release();
+    }
+    phase("l0 pairs");
+    GAHHG_TRY(sort_lists(g, l0.cnt.ptr, l0.off.ptr, l0.nn, l0.list.ptr, sms, s));
+    GAHHG_TRY(l0.ix.reserve(l0.nn, s, false));
+    GAHHG_TRY(l0.iy.reserve(l0.nn, s, false));
+    GAHHG_TRY(l0.poly.reserve(l0.nn, s, false));
+    kb_l0_coords<<<blocks_for(l0.nn), TPB, 0, s>>>(d_tops.ptr, np, d_pg.ptr, l0.nn, l0.ix.ptr, l0.iy.ptr,
+                                                   l0.poly.ptr);
+
+    phase("l0 sort");
+    // ---- level-0 labels and each polygon's label outside its domain
+    int* d_bad = g->d_counts + 48;  // [0] coincidences, [1] nesting, [2] long lists
+    GAHHG_CUDA_TRY(cudaMemsetAsync(d_bad, 0, 4 * sizeof(int), s));
+    DevArray<uint8_t> outl;
+    GAHHG_TRY(outl.reserve(np, s, false));
+    {
+        std::vector<long long> pb(np + 1, 0), cb(np + 1, 0);
+        std::vector<int4> oxy(np);
+        for (int p = 0; p < np; p++) {
+            const Geo& G0 = pg[p].g;
+            const int W = G0.W, H = G0.H;
+            pb[p + 1] = pb[p] + (long long)W * (H - 1) + (W - 1);
+            cb[p + 1] = cb[p] + W;
+            // the region outside the domain, from the nearest border cell
+            int ix = 0, iy = 0, ox = 0, oy = 0;
+            if (!G0.full_lon) {
+                ox = -1;
+            } else if (!G0.to_south) {
+                oy = -1;
+            } else if (!G0.to_north) {
+                iy = H - 1;
+                oy = H;
+            } else {
+                ox = INT_MIN;  // no outside region
+            }
+            oxy[p] = make_int4(ix, iy, ox, oy);
+        }
+        DevArray<long long> d_pb, d_cb;
+        DevArray<int4> d_oxy;
+        DevArray<uint8_t> par;
+        GAHHG_TRY(upload(d_pb, pb, s));
+        GAHHG_TRY(upload(d_cb, cb, s));
+        GAHHG_TRY(upload(d_oxy, oxy, s));
+        GAHHG_TRY(par.reserve(std::max(pb[np], 1LL), s, false));
+        GAHHG_TRY(l0.label.reserve(l0.nn, s, false));
+        if (pb[np] > 0)
+            kb_l0_neighbour_parity<<<(int)((pb[np] + TPB - 1) / TPB), TPB, 0, s>>>(
+                pv, pe, d_pg.ptr, d_pb.ptr, np, l0.cnt.ptr, l0.off.ptr, l0.list.ptr, par.ptr, d_bad);
+        kb_l0_labels<<<(int)((cb[np] + TPB - 1) / TPB), TPB, 0, s>>>(d_pg.ptr, d_cb.ptr, d_pb.ptr, np, par.ptr,
+                                                                      origin.ptr, l0.label.ptr);
+        kb_outside_label<<<(np + TPB - 1) / TPB, TPB, 0, s>>>(pv, pe, d_pg.ptr, np, d_oxy.ptr, l0.cnt.ptr,
+                                                               l0.off.ptr, l0.list.ptr, l0.label.ptr, outl.ptr, d_bad);
+        par.release();
+        d_pb.release();
+        d_cb.release();
+        d_oxy.release();
+    }
+
+    phase("l0 labels");
+    // ---- refinement, every polygon's level at once
+    const int maxlev = 9;
+    long long gnext = l0.nn;
+    for (int lvl = 0; lvl < maxlev; lvl++) {
+        LevelBuf& pl = lv[lvl];
+        GAHHG_TRY(pl.flag.reserve(pl.nn, s, false));
+        GAHHG_TRY(pl.foff.reserve(pl.nn, s, false));
+        kb_refine_flags<<<blocks_for(pl.nn), TPB, 0, s>>>(pl.cnt.ptr, pl.poly.ptr, d_pg.ptr, pl.nn, pl.flag.ptr);
+        GAHHG_TRY(scan_state_reserve(&g->scan_state, pl.nn));
+        GAHHG_TRY(scan_exclusive(pl.flag.ptr, pl.foff.ptr, pl.nn, g->d_counts + 9, g->scan_state, g->d_err, s));
+        int nref = 0;
+        GAHHG_CUDA_TRY(cudaMemcpyAsync(&nref, g->d_counts + 9, sizeof(int), cudaMemcpyDeviceToHost, s));
+        GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+        if (nref == 0) break;
+        // the budgets hold for the whole group (a polygon built alone keeps its
+        // own); past them the remaining cells stay leaves with more edges
+        if (gnext + (long long)nref * FAN * FAN > NODE_BUDGET || 4LL * pl.npairs > PAIR_BUDGET) break;
+        lv.emplace_back();
+        LevelBuf& cl = lv.back();
+        LevelBuf& pp = lv[lvl];  // re-fetch after emplace_back
+        cl.nn = nref * FAN * FAN;
+        cl.gstart = (int)gnext;
+        GAHHG_TRY(pp.child_base.reserve(pp.nn, s, false));
+        GAHHG_TRY(cl.ix.reserve(cl.nn, s, false));
+        GAHHG_TRY(cl.iy.reserve(cl.nn, s, false));
+        GAHHG_TRY(cl.poly.reserve(cl.nn, s, false));
+        kb_make_children<<<blocks_for(pp.nn), TPB, 0, s>>>(pp.flag.ptr, pp.foff.ptr, pp.nn, cl.gstart, pp.ix.ptr,
+                                                           pp.iy.ptr, pp.poly.ptr, pp.child_base.ptr, cl.ix.ptr,
+                                                           cl.iy.ptr, cl.poly.ptr);
+        GAHHG_TRY(pp.pair_node.reserve(std::max(pp.npairs, 1), s, false));
+        k_fill_pair_node<<<blocks_for(pp.nn), TPB, 0, s>>>(pp.cnt.ptr, pp.off.ptr, pp.nn, pp.pair_node.ptr);
+        GAHHG_TRY(cl.cnt.reserve(cl.nn, s, false));
+        GAHHG_TRY(cl.off.reserve(cl.nn, s, false));
+        GAHHG_TRY(cl.cursor.reserve(cl.nn, s, false));
+        GAHHG_CUDA_TRY(cudaMemsetAsync(cl.cnt.ptr, 0, sizeof(int) * cl.nn, s));
+        GAHHG_CUDA_TRY(cudaMemsetAsync(cl.cursor.ptr, 0, sizeof(int) * cl.nn, s));
+        DevArray<double4> caps;
+        DevArray<double2> capsb;
+        DevArray<uint16_t> hit;
+        GAHHG_TRY(caps.reserve(cl.nn, s, false));
+        GAHHG_TRY(capsb.reserve(cl.nn, s, false));
+        GAHHG_TRY(hit.reserve(std::max(pp.npairs, 1), s, false));
+        kb_child_caps<<<blocks_for(cl.nn), TPB, 0, s>>>(d_pg.ptr, lvl + 1, cl.nn, cl.ix.ptr, cl.iy.ptr, cl.poly.ptr,
+                                                        caps.ptr, capsb.ptr);
+        k_child_pairs_count<<<blocks_for(pp.npairs), TPB, 0, s>>>(bv, pp.npairs, pp.pair_node.ptr, pp.list.ptr,
+                                                                  pp.child_base.ptr, caps.ptr, capsb.ptr, cl.gstart,
+                                                                  cl.cnt.ptr, hit.ptr);
+        GAHHG_TRY(scan_state_reserve(&g->scan_state, cl.nn));
+        GAHHG_TRY(scan_exclusive(cl.cnt.ptr, cl.off.ptr, cl.nn, g->d_counts + 10, g->scan_state, g->d_err, s));
+        int ctotal = 0;
+        GAHHG_CUDA_TRY(cudaMemcpyAsync(&ctotal, g->d_counts + 10, sizeof(int), cudaMemcpyDeviceToHost, s));
+        GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+        cl.npairs = ctotal;
+        GAHHG_TRY(cl.list.reserve(std::max(ctotal, 1), s, false));
+        k_child_pairs_fill<<<blocks_for(pp.npairs), TPB, 0, s>>>(pp.npairs, pp.pair_node.ptr, pp.list.ptr,
+                                                                 pp.child_base.ptr, cl.gstart, hit.ptr, cl.off.ptr,
+                                                                 cl.cursor.ptr, cl.list.ptr);
+        hit.release();
+        GAHHG_TRY(sort_lists(g, cl.cnt.ptr, cl.off.ptr, cl.nn, cl.list.ptr, sms, s));
+        DevArray<int> child_parent;
+        GAHHG_TRY(child_parent.reserve(cl.nn, s, false));
+        k_child_parent<<<blocks_for(pp.nn), TPB, 0, s>>>(pp.child_base.ptr, pp.nn, cl.gstart, child_parent.ptr);
+        GAHHG_TRY(cl.label.reserve(cl.nn, s, false));
+        k_child_labels<<<blocks_for(cl.nn), TPB, 0, s>>>(bv, TableGeo{d_pg.ptr, pp.poly.ptr}, lvl, cl.nn,
+                                                         child_parent.ptr, cl.ix.ptr, cl.iy.ptr, cl.cnt.ptr,
+                                                         cl.off.ptr, cl.list.ptr, caps.ptr, capsb.ptr, pp.ix.ptr,
+                                                         pp.iy.ptr, pp.cnt.ptr, pp.off.ptr, pp.list.ptr,
+                                                         pp.label.ptr, cl.label.ptr, d_bad);
+        caps.release();
+        capsb.release();
+        child_parent.release();
+        gnext += cl.nn;
+    }
+    const int nlev = (int)lv.size();
+    GI->nnodes = gnext;
+
+    phase("refine");
+    // ---- encode: node words, leaf records, summaries
+    GAHHG_TRY(GI->nodes.reserve(std::max(GI->nnodes, 1LL), s, false));
+    std::vector<int> leaf_base(nlev);
+    std::vector<long long> rec_base(nlev);
+    long long leaf_total = 0, rec_total = 0;
+    std::vector<DevArray<int>> is_leaf(nlev), leaf_off(nlev), nrec(nlev), rec_off(nlev);
+    DevArray<int> d_tot;
+    GAHHG_TRY(d_tot.reserve(2 * nlev, s, false));
+    for (int lvl = 0; lvl < nlev; lvl++) {
+        LevelBuf& b = lv[lvl];
+        const int* cbase = (lvl + 1 < nlev) ? b.child_base.ptr : nullptr;
+        GAHHG_TRY(is_leaf[lvl].reserve(b.nn, s, false));
+        GAHHG_TRY(leaf_off[lvl].reserve(b.nn, s, false));
+        GAHHG_TRY(nrec[lvl].reserve(b.nn, s, false));
+        GAHHG_TRY(rec_off[lvl].reserve(b.nn, s, false));
+        k_leaf_flags<<<blocks_for(b.nn), TPB, 0, s>>>(b.nn, b.cnt.ptr, cbase, is_leaf[lvl].ptr, nrec[lvl].ptr);
+        GAHHG_TRY(scan_state_reserve(&g->scan_state, b.nn));
+        GAHHG_TRY(scan_exclusive(is_leaf[lvl].ptr, leaf_off[lvl].ptr, b.nn, d_tot.ptr + 2 * lvl, g->scan_state,
+                                 g->d_err, s));
+        GAHHG_TRY(scan_exclusive(nrec[lvl].ptr, rec_off[lvl].ptr, b.nn, d_tot.ptr + 2 * lvl + 1, g->scan_state,
+                                 g->d_err, s));
+        k_encode<<<blocks_for(b.nn), TPB, 0, s>>>(TableGeo{d_pg.ptr, b.poly.ptr}, b.nn, b.gstart, b.cnt.ptr, cbase,
+                                                  b.label.ptr, leaf_off[lvl].ptr, GI->nodes.ptr);
+    }
+    {
+        std::vector<int> tot(2 * nlev);
+        GAHHG_CUDA_TRY(cudaMemcpyAsync(tot.data(), d_tot.ptr, sizeof(int) * tot.size(), cudaMemcpyDeviceToHost, s));
+        GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+        for (int lvl = 0; lvl < nlev; lvl++) {
+            leaf_base[lvl] = (int)leaf_total;
+            rec_base[lvl] = rec_total;
+            leaf_total += tot[2 * lvl];
+            rec_total += tot[2 * lvl + 1];
+        }
+    }
+    d_tot.release();
+    if (rec_total >= 0xFFFFFFFFll || leaf_total >= (long long)INDEX_MASK) {
+        set_error("exact index group: too many leaves or edge records");
+        return GAHHG_ERR_CAPACITY;
+    }
+    GAHHG_TRY(GI->leaves.reserve(leaf_total + 1, s, false));
+    GAHHG_TRY(GI->recs.reserve(std::max(rec_total, 1LL), s, false));
+    GAHHG_TRY(GI->eids.reserve(std::max(rec_total, 1LL), s, false));
+    GAHHG_TRY(GI->leafR.reserve(3 * (size_t)std::max(leaf_total, 1LL), s, false));
+    GAHHG_TRY(GI->ends.reserve(3 * (size_t)std::max(ne, 1LL), s, false));
+    GI->nleaves = leaf_total;
+    GI->nrecs = rec_total;
+    k_edge_ends<<<(int)((ne + TPB - 1) / TPB), TPB, 0, s>>>(pv, pe, (int)ne, GI->ends.ptr);
+    for (int lvl = 0; lvl < nlev; lvl++) {
+        LevelBuf& b = lv[lvl];
+        k_leaf_records<<<blocks_for(b.nn), TPB, 0, s>>>(bv, TableGeo{d_pg.ptr, b.poly.ptr}, lvl, b.nn,
+                                                        is_leaf[lvl].ptr, leaf_off[lvl].ptr, rec_off[lvl].ptr,
+                                                        leaf_base[lvl], rec_base[lvl], b.ix.ptr, b.iy.ptr, b.cnt.ptr,
+                                                        b.off.ptr, b.list.ptr, b.label.ptr, GI->leaves.ptr,
+                                                        GI->recs.ptr, GI->eids.ptr, GI->leafR.ptr, d_bad);
+    }
+    GAHHG_CUDA_TRY(cudaGetLastError());
+    for (int lvl = 1; lvl < nlev; lvl++) {
+        if (leaf_base[lvl] == 0) continue;
+        k_shift_leaf_words<<<blocks_for(lv[lvl].nn), TPB, 0, s>>>(GI->nodes.ptr, lv[lvl].gstart, lv[lvl].nn,
+                                                                  leaf_base[lvl]);
+    }
+    // coarse summaries, each polygon's from a 16-byte aligned word
+    std::vector<long long> sc(np + 1, 0), soff(np + 1, 0);
+    std::vector<int> cshift(np);
+    GI->swords.resize(np);
+    for (int p = 0; p < np; p++) {
+        int cs, CW, CH;
+        summary_shape(pg[p].g.W, pg[p].g.H, &cs, &CW, &CH);
+        cshift[p] = cs;
+        GI->swords[p] = (CW * CH + 15) / 16;
+        sc[p + 1] = sc[p] + (long long)CW * CH;
+        soff[p + 1] = soff[p] + ((GI->swords[p] + 3) & ~3);
+    }
+    {
+        DevArray<long long> d_sc, d_soff;
+        DevArray<int> d_cshift;
+        GAHHG_TRY(upload(d_sc, sc, s));
+        GAHHG_TRY(upload(d_soff, soff, s));
+        GAHHG_TRY(upload(d_cshift, cshift, s));
+        // 1,024 spare words: a bulk copy of a summary reads up to its 16-byte multiple
+        GAHHG_TRY(GI->summary.reserve(soff[np] + 1024, s, false));
+        GAHHG_CUDA_TRY(cudaMemsetAsync(GI->summary.ptr, 0, sizeof(uint32_t) * (soff[np] + 1024), s));
+        kb_summary<<<(int)((sc[np] + TPB - 1) / TPB), TPB, 0, s>>>(GI->nodes.ptr, d_pg.ptr, d_sc.ptr, d_cshift.ptr,
+                                                                   d_soff.ptr, np, GI->summary.ptr);
+        d_sc.release();
+        d_soff.release();
+        d_cshift.release();
+    }
+    phase("encode");
+    // ---- the build's last round trip: failures, origins, outside labels
+    int bad[4];
+    std::vector<int> h_origin(np);
+    std::vector<uint8_t> h_out(np);
+    GAHHG_CUDA_TRY(cudaMemcpyAsync(bad, d_bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
+    GAHHG_CUDA_TRY(cudaMemcpyAsync(h_origin.data(), origin.ptr, sizeof(int) * np, cudaMemcpyDeviceToHost, s));
+    GAHHG_CUDA_TRY(cudaMemcpyAsync(h_out.data(), outl.ptr, np, cudaMemcpyDeviceToHost, s));
+    GAHHG_CUDA_TRY(cudaStreamSynchronize(s));
+    for (auto& b : lv) b.release();
+    for (int lvl = 0; lvl < nlev; lvl++) {
+        is_leaf[lvl].release();
+        leaf_off[lvl].release();
+        nrec[lvl].release();
+        rec_off[lvl].release();
+    }
+    for (int p = 0; p < np; p++) {
+        if (h_origin[p] == 0) {
+            set_error("exact index: polygon %d: no outer-ring edge gives a reference point", p);
+            return GAHHG_ERR_STATE;
+        }
+        if (h_origin[p] < 0) {
+            set_error("exact index: polygon %d: a hub or the origin center coincides with a polygon vertex", p);
+            return GAHHG_ERR_STATE;
+        }
+    }
+    if (bad[0] || bad[1] || bad[2]) {
+        set_error("exact index group: %d center/vertex coincidences, %d cap nesting violations, %d oversize leaves",
+                  bad[0], bad[1], bad[2]);
+        return GAHHG_ERR_DEVICE;
+    }
+    GAHHG_TRY(check_device_errors(g, "exact index group build"));
+    // ---- every polygon's query view into the group's arrays
+    GI->views.resize(np);
+    for (int p = 0; p < np; p++) {
+        QueryView& Q = GI->views[p];
+        memset(&Q, 0, sizeof Q);
+        set_view_geo(Q, pg[p].g);
+        Q.outside = KIND_PURE | (uint32_t)h_out[p];
+        Q.nodes = GI->nodes.ptr + pg[p].top;
+        Q.leaves = GI->leaves.ptr;
+        Q.recs = GI->recs.ptr;
+        Q.eids = GI->eids.ptr;
+        Q.ends = GI->ends.ptr;
+        Q.leafR = GI->leafR.ptr;
+        Q.pv = pv;
+        Q.pe = pe;
+        Q.cshift = cshift[p];
+        Q.CW = (pg[p].g.W + (1 << cshift[p]) - 1) >> cshift[p];
+        Q.swords = GI->swords[p];
+        Q.summary = GI->summary.ptr + soff[p];
+        Q.nparts = 1;  // the leaf-window order of single-polygon queries is not used by batches
+        Q.part_scale = 0.0f;
+    }
+    return GAHHG_OK;
 }
 
 // Points per pass; the pass-2 queue holds one 4-byte index per point.
