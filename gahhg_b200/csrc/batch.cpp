@@ -2,10 +2,12 @@
 // CUDA-graph replay.
 //
 // No counterpart in the reference (one polygon per process,
-// source/GPISP.cu:15-70).  Builds run on a pool of host threads, each with
-// its own non-blocking stream and look-back scan state, so the GPU overlaps
-// the small, synchronisation-heavy builds of many polygons; device memory
-// comes from the stream-ordered pool, so no build synchronises the device.
+// source/GPISP.cu:15-70).  Builds run in groups of consecutive polygons
+// (lattice_build_group: every step once for all polygons of a group, so
+// launches and host round trips scale with levels, not polygons) on a pool of
+// host threads, each with its own non-blocking stream and look-back scan
+// state; device memory comes from the stream-ordered pool, so no build
+// synchronises the device.
 // A query takes all polygons' points at once (polygon after polygon) and
 // runs pass 1 as one persistent launch over chunks of points.
 #include <algorithm>

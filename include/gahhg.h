@@ -183,7 +183,7 @@ typedef struct gahhg_batch gahhg_batch;
 
 typedef struct {
     int polygons;
-    int workers;               /* host threads that built the lattices */
+    int workers;               /* host threads that built the groups of lattices */
     long long edges;
     long long lattice_bytes;   /* device bytes of all exact indexes */
     double build_s;            /* wall time of gahhg_batch_build */
@@ -196,8 +196,11 @@ typedef struct {
 } gahhg_batch_stats;
 
 /* Builds the exact index of every polygon (exact semantics only; the hexagon
- * hierarchy is not built).  Builds run concurrently on `workers` host threads
- * (0 = up to 16), each with its own stream.  top_cells / leaf_edges, when not
+ * hierarchy is not built).  Consecutive polygons of up to 2^20 edges in all
+ * are built together, each step once for the whole group; groups are built
+ * concurrently on `workers` host threads (0 = up to 4), each with its own
+ * stream.  The device memory pool keeps up to a quarter of the device's
+ * memory cached from then on.  top_cells / leaf_edges, when not
  * NULL, set each polygon's lattice_top / lattice_leaf (e.g. from the
  * autotuner); 0 entries mean automatic.  The polygons must outlive the batch. */
 gahhg_status gahhg_batch_build(const gahhg_polygon* const* polys, int count, const gahhg_build_opts* opts,
