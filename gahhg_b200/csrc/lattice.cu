@@ -1636,14 +1636,21 @@ struct BatchChunk {
 };
 
 constexpr int BATCH_SUMMARY_WORDS = 4096;  // 16 KB of shared memory
-constexpr int BATCH_UNROLL = 8;            // points per thread in flight in the batch locate (72 registers)
+// Points per thread in flight in the batch locate, and blocks per SM: five
+// points in lockstep at 48 registers, five blocks (160 KB of shared memory)
+// took a 1,024-polygon C3 batch from 75.6 (8 points, two blocks) to 106.5
+// Gpts/s; 4 points x 5 blocks 101.2, 6 x 4 101.8, 6 x 5 102.3, 4 x 6 91.2,
+// 8 x 3 93.5 (labels identical).  More warps hide more of the node descents'
+// latency than more points per thread.
+constexpr int BATCH_UNROLL = 5;
+constexpr int BATCH_BLOCKS = 5;
 
 // Pass 1 over a batch: a persistent grid takes chunks in order from an atomic
 // counter (polygons of very different sizes balance themselves), stages the
 // chunk's polygon summary in shared memory and runs the single-polygon tile
 // loop on it.
 template <bool STATS>
-__global__ void __launch_bounds__(TPB) k_batch_locate(const QueryView* __restrict__ views,
+__global__ void __launch_bounds__(TPB, BATCH_BLOCKS) k_batch_locate(const QueryView* __restrict__ views,
                                                      const BatchChunk* __restrict__ chunks, int nchunks,
                                                      unsigned int* next_chunk, const double2* __restrict__ ll,
                                                      uint8_t* __restrict__ out, uint32_t* __restrict__ queue,
@@ -4125,9 +4132,7 @@ gahhg_status batch_query_launch(const void* d_views, const void* d_chunks, int n
     const BatchChunk* chunks = (const BatchChunk*)d_chunks;
     unsigned long long* ctr = (unsigned long long*)d_stats;
     if (zero_counters) GAHHG_CUDA_TRY(cudaMemsetAsync(counters, 0, 5 * sizeof(unsigned int), s));
-    // two blocks per SM: with three (which the registers would allow) the
-    // concurrent chunks' node tables crowd L2 and the pass runs slower
-    const int grid = std::min(nchunks, sms * 2);
+    const int grid = std::min(nchunks, sms * BATCH_BLOCKS);  // persistent: every block resident
     Tiers T;
     tier_caps(queue_cap, &T.cap2, &T.cap3);
     T.l1 = queue + queue_cap;
