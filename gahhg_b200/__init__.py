@@ -57,7 +57,9 @@ class Polygon:
         return xyz, pe
 
     def __del__(self):
-        if getattr(self, "_h", None):
+        # at interpreter exit the module's globals may already be gone; the
+        # process is ending and frees the handle itself
+        if getattr(self, "_h", None) and _lib is not None:
             _lib.lib().gahhg_polygon_free(self._h)
             self._h = None
 
@@ -148,7 +150,9 @@ class Grid:
                                              str(path).encode(), 1 if to_stdout else 0))
 
     def __del__(self):
-        if getattr(self, "_h", None):
+        # at interpreter exit the module's globals may already be gone; the
+        # process is ending and frees the handle itself
+        if getattr(self, "_h", None) and _lib is not None:
             _lib.lib().gahhg_grid_free(self._h)
             self._h = None
 
@@ -193,7 +197,9 @@ class Batch:
         return s.as_dict()
 
     def __del__(self):
-        if getattr(self, "_h", None):
+        # at interpreter exit the module's globals may already be gone; the
+        # process is ending and frees the handle itself
+        if getattr(self, "_h", None) and _lib is not None:
             _lib.lib().gahhg_batch_free(self._h)
             self._h = None
 
