@@ -278,7 +278,7 @@ def run_c3(args, count=None, tune_budget=None, steps=None, polys=None):
     d_pts = synth.device_cap_points(lons, lats, radii, counts, 5, dev)
     n = int(offsets[-1])
     d_lab = torch.empty(n, dtype=torch.uint8, device=dev)
-    chunk = autotune.tune_chunk(B, d_pts, offsets, d_lab, reps=2)
+    chunk, shape = autotune.tune_launch(B, d_pts, offsets, d_lab, reps=2)
     stream = torch.cuda.current_stream()
     B.query_device(d_pts.data_ptr(), offsets, d_lab.data_ptr(), G.QUERY_FP32_FILTER, stream.cuda_stream, sync=True)
     esc = B.stats()
@@ -316,6 +316,7 @@ def run_c3(args, count=None, tune_budget=None, steps=None, polys=None):
         "build_ms": {"batch_build_wall": round(build_wall * 1e3, 1), "workers": bst["workers"],
                      "generate_s": round(gen_s, 1), "autotune_s": round(tune_s, 1)},
         "lattice_bytes": bst["lattice_bytes"], "tuning": tuning.as_dict(), "chunk_points": chunk,
+        "launch_shape": dict(zip(("points_per_thread", "blocks_per_sm"), G.Batch.shapes()[shape])),
         "escalation": {"boundary_points": esc["boundary_points"], "fp64_tests": esc["esc_fp64"],
                        "exact_tests": esc["esc_exact"], "boundary_fraction": round(esc["boundary_points"] / n, 6)},
     }, polys)

@@ -177,6 +177,23 @@ class Batch:
         if chunk_points:
             check(L.gahhg_batch_set_chunk(h, chunk_points))
 
+    @staticmethod
+    def shapes():
+        """The query's pass-1 launch shapes, by index: (points per thread,
+        blocks per SM)."""
+        L = _lib.lib()
+        out = []
+        a, b = ctypes.c_int(), ctypes.c_int()
+        while L.gahhg_batch_shape_info(len(out), ctypes.byref(a), ctypes.byref(b)) == 0:
+            out.append((a.value, b.value))
+        return out
+
+    def set_chunk(self, chunk_points):
+        check(_lib.lib().gahhg_batch_set_chunk(self._h, chunk_points))
+
+    def set_shape(self, shape):
+        check(_lib.lib().gahhg_batch_set_shape(self._h, shape))
+
     def query_device(self, d_lonlat, offsets, d_labels, precision=QUERY_AUTO, stream=0, sync=False, graph=False):
         """d_lonlat / d_labels: device pointers; offsets: host int64 array (count+1)."""
         off = np.ascontiguousarray(offsets, dtype=np.int64)

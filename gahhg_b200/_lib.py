@@ -140,6 +140,9 @@ _SIGS = {
                                          ctypes.POINTER(_P)]),
     "gahhg_batch_size": (ctypes.c_int, [_P]),
     "gahhg_batch_set_chunk": (ctypes.c_int, [_P, ctypes.c_int]),
+    "gahhg_batch_shape_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                              ctypes.POINTER(ctypes.c_int)]),
+    "gahhg_batch_set_shape": (ctypes.c_int, [_P, ctypes.c_int]),
     "gahhg_batch_query_device": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int, _P, ctypes.c_int]),
     "gahhg_batch_query_graph": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int, _P]),
     "gahhg_batch_stats_get": (ctypes.c_int, [_P, ctypes.POINTER(BatchStats)]),

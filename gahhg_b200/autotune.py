@@ -11,8 +11,9 @@ class:
   leaf_edges      edges per leaf before a cell is split (lattice_leaf);
                   fewer mean shorter crossing loops and deeper lattices;
 
-and then the point-chunk size of the persistent batch query (the load
-balancing grain).  Candidates are measured, not modelled: each candidate
+and then, per batch, the point-chunk size of the persistent batch query
+(the load balancing grain) and the launch shape of its first pass (points
+per thread in flight x resident blocks per SM; threads per block stay 256).  Candidates are measured, not modelled: each candidate
 builds the sampled polygons as a batch and times queries of their own points
 with CUDA events.  The result is a plain table that `Batch` takes as its
 per-polygon `top_cells` / `leaf_edges`.
@@ -97,15 +98,39 @@ def tune(polygons, points, per_class=3, reps=5, seed=0, budget_s=60.0, mem_ratio
 
 
 def tune_chunk(batch, d_pts, offsets, d_lab, reps=5):
+    """Sets and returns the fastest chunk size of `batch` on these points."""
     best = None
-    from . import _lib
     for ch in CHUNKS:
-        _lib.check(_lib.lib().gahhg_batch_set_chunk(batch._h, ch))
+        batch.set_chunk(ch)
         t = _time_batch(batch, d_pts, offsets, d_lab, reps)
         if best is None or t < best[0]:
             best = (t, ch)
-    _lib.check(_lib.lib().gahhg_batch_set_chunk(batch._h, best[1]))
+    batch.set_chunk(best[1])
     return best[1]
+
+
+def tune_shape(batch, d_pts, offsets, d_lab, reps=5, log=None):
+    """Sets and returns the index of the fastest pass-1 launch shape (points
+    per thread x blocks per SM, `Batch.shapes()`) of `batch` on these points:
+    the descent is latency-bound, and how many points a thread keeps in
+    flight against how many warps an SM holds depends on the mix of polygon
+    sizes and points."""
+    best = None
+    for i, (u, blocks) in enumerate(Batch.shapes()):
+        batch.set_shape(i)
+        t = _time_batch(batch, d_pts, offsets, d_lab, reps)
+        if log:
+            log("shape %d (%d points x %d blocks) query %.3f ms" % (i, u, blocks, t * 1e3))
+        if best is None or t < best[0]:
+            best = (t, i)
+    batch.set_shape(best[1])
+    return best[1]
+
+
+def tune_launch(batch, d_pts, offsets, d_lab, reps=5, log=None):
+    """Chunk size, then launch shape, of `batch`'s query; returns both."""
+    ch = tune_chunk(batch, d_pts, offsets, d_lab, reps)
+    return ch, tune_shape(batch, d_pts, offsets, d_lab, reps, log)
 
 
 class Tuning:

@@ -24,6 +24,7 @@ struct gahhg_batch {
     int device = 0;
     int count = 0;
     int chunk_points = 4096;
+    int shape = 0;  // pass-1 launch shape (batch_shape_info)
     std::vector<Polygon*> polys;
     std::vector<Grid*> grids;
     std::vector<GroupIndex*> groups;  // polygons built together, in order
@@ -319,13 +320,43 @@ gahhg_status gahhg_batch_build(const gahhg_polygon* const* polys, int count, con
 
 int gahhg_batch_size(const gahhg_batch* b) { return b ? b->count : 0; }
 
+// The captured query no longer matches the batch's settings: the next graph
+// query captures again (an executable graph still running is freed when it
+// completes).
+static void drop_graph(gahhg_batch* b)
+{
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+}
+
 gahhg_status gahhg_batch_set_chunk(gahhg_batch* b, int chunk_points)
 {
     if (!b || chunk_points < 256 || chunk_points > (1 << 20)) {
         set_error("chunk_points must be in [256, 1048576]");
         return GAHHG_ERR_ARG;
     }
+    if (b->chunk_points != chunk_points) drop_graph(b);
     b->chunk_points = chunk_points;
+    return GAHHG_OK;
+}
+
+gahhg_status gahhg_batch_shape_info(int shape, int* points_per_thread, int* blocks_per_sm)
+{
+    if (!batch_shape_info(shape, points_per_thread, blocks_per_sm)) {
+        set_error("launch shape %d: there are %d shapes", shape, batch_shape_count());
+        return GAHHG_ERR_ARG;
+    }
+    return GAHHG_OK;
+}
+
+gahhg_status gahhg_batch_set_shape(gahhg_batch* b, int shape)
+{
+    if (!b || !batch_shape_info(shape, nullptr, nullptr)) {
+        set_error("launch shape must be in [0, %d)", batch_shape_count());
+        return GAHHG_ERR_ARG;
+    }
+    if (b->shape != shape) drop_graph(b);
+    b->shape = shape;
     return GAHHG_OK;
 }
 
@@ -385,7 +416,7 @@ gahhg_status gahhg_batch_query_device(gahhg_batch* b, const double* d_lonlat, co
         cudaEventRecord(e0, s);
     }
     gahhg_status st = batch_query_launch(b->views.ptr, d_chunks, nchunks, d_lonlat, d_labels, precision, queue,
-                                         qcap, counters, d_stats, s, b->device);
+                                         qcap, counters, d_stats, s, b->device, true, b->shape);
     if (sync && st == GAHHG_OK) {
         cudaEventRecord(e1, s);
         uint64_t c[4] = {0, 0, 0, 0};
@@ -455,7 +486,8 @@ gahhg_status gahhg_batch_query_graph(gahhg_batch* b, const double* d_lonlat, con
             st = GAHHG_ERR_CUDA;
         } else {
             st = batch_query_launch(b->views.ptr, b->g_chunks.ptr, b->g_nchunks, d_lonlat, d_labels, precision,
-                                    b->g_queue.ptr, b->g_qcap, b->g_counters.ptr, nullptr, cs, b->device);
+                                    b->g_queue.ptr, b->g_qcap, b->g_counters.ptr, nullptr, cs, b->device, true,
+                                    b->shape);
             if (cudaStreamEndCapture(cs, &graph) != cudaSuccess) st = GAHHG_ERR_CUDA;
         }
         cudaStreamDestroy(cs);

@@ -243,11 +243,14 @@ size_t batch_chunk_count_bound(long long points, int nseg, int chunk_points);
 // Words of a batch queue whose pass-2 part holds queue_cap points (with their
 // leaf words; the escalation queues and theirs follow).
 size_t batch_queue_words(long long queue_cap);
-// counters[0..4] must be zero on entry unless zero_counters is set.
+// counters[0..4] must be zero on entry unless zero_counters is set.  shape
+// indexes the pass-1 launch shapes (batch_shape_info).
 gahhg_status batch_query_launch(const void* d_views, const void* d_chunks, int nchunks, const double* d_lonlat,
                                 uint8_t* d_labels, int precision, uint32_t* queue, long long queue_cap,
                                 unsigned int* counters, uint64_t* d_stats, cudaStream_t s, int device,
-                                bool zero_counters = true);
+                                bool zero_counters = true, int shape = 0);
+int batch_shape_count();
+bool batch_shape_info(int shape, int* points_per_thread, int* blocks_per_sm);
 size_t lattice_bytes(const Lattice* L);
 size_t lattice_device_bytes(const Lattice* L);  // capacity held on the device
 

@@ -1636,21 +1636,28 @@ struct BatchChunk {
 };
 
 constexpr int BATCH_SUMMARY_WORDS = 4096;  // 16 KB of shared memory
-// Points per thread in flight in the batch locate, and blocks per SM: five
-// points in lockstep at 48 registers, five blocks (160 KB of shared memory)
-// took a 1,024-polygon C3 batch from 75.6 (8 points, two blocks) to 106.5
-// Gpts/s; 4 points x 5 blocks 101.2, 6 x 4 101.8, 6 x 5 102.3, 4 x 6 91.2,
-// 8 x 3 93.5 (labels identical).  More warps hide more of the node descents'
-// latency than more points per thread.
-constexpr int BATCH_UNROLL = 5;
-constexpr int BATCH_BLOCKS = 5;
+// Launch shapes of the batch locate: points per thread in flight (in
+// lockstep) and blocks per SM (all resident; each holds 32 KB of shared
+// memory, and the register budget per thread follows from the blocks).  The
+// default, five points at five blocks (48 registers), took a 1,024-polygon
+// C3 batch from 75.6 (8 points, two blocks) to 106.5 Gpts/s; 4 x 5 101.2,
+// 6 x 4 101.8, 6 x 5 102.3, 4 x 6 91.2, 8 x 3 93.5 (labels identical): more
+// warps hide more of the node descents' latency than more points per
+// thread.  Batches of other point mixes may prefer another row (2 x 6, at
+// 40 registers with a few bytes spilled, leaves fewer lanes idle in chunks
+// of few points); the batch autotuner measures them.
+struct BatchShape {
+    int unroll, blocks;
+};
+constexpr BatchShape BATCH_SHAPES[] = {{5, 5}, {2, 6}, {6, 4}, {8, 3}};
+constexpr int BATCH_NSHAPES = (int)(sizeof(BATCH_SHAPES) / sizeof(BATCH_SHAPES[0]));
 
 // Pass 1 over a batch: a persistent grid takes chunks in order from an atomic
 // counter (polygons of very different sizes balance themselves), stages the
 // chunk's polygon summary in shared memory and runs the single-polygon tile
 // loop on it.
-template <bool STATS>
-__global__ void __launch_bounds__(TPB, BATCH_BLOCKS) k_batch_locate(const QueryView* __restrict__ views,
+template <bool STATS, int UNROLL, int BLOCKS>
+__global__ void __launch_bounds__(TPB, BLOCKS) k_batch_locate(const QueryView* __restrict__ views,
                                                      const BatchChunk* __restrict__ chunks, int nchunks,
                                                      unsigned int* next_chunk, const double2* __restrict__ ll,
                                                      uint8_t* __restrict__ out, uint32_t* __restrict__ queue,
@@ -1690,8 +1697,7 @@ __global__ void __launch_bounds__(TPB, BATCH_BLOCKS) k_batch_locate(const QueryV
             sum = s_own;
             __syncthreads();
         }
-        locate_range<STATS, true, BATCH_UNROLL>(Q, sum, ll, out, queue, leafq, qcount, c.start, c.count, 0, 1,
-                                                inside);
+        locate_range<STATS, true, UNROLL>(Q, sum, ll, out, queue, leafq, qcount, c.start, c.count, 0, 1, inside);
         __syncthreads();
     }
     if (late) {
@@ -1742,12 +1748,15 @@ struct OneView {
     __device__ __forceinline__ const QueryView& of(uint32_t) const { return Q; }
 };
 
-// ...or the chunk holding it (binary search of the chunk starts).
+// ...or the chunk holding it: the first active lane of the warp finds its
+// point's chunk by binary search of the chunk starts and shares it, and a
+// lane whose point lies outside that chunk searches for its own (the queues
+// hold a chunk's points together, so most lanes share the first lane's).
 struct ChunkViews {
     const QueryView* views;
     const BatchChunk* chunks;
     int nchunks;
-    __device__ __forceinline__ const QueryView& of(uint32_t i) const
+    __device__ __forceinline__ int search(uint32_t i) const
     {
         int lo = 0, hi = nchunks;  // chunks[lo].start <= i < chunks[hi].start
         while (hi - lo > 1) {
@@ -1755,7 +1764,18 @@ struct ChunkViews {
             if (__ldg(&chunks[mid].start) <= (long long)i) lo = mid;
             else hi = mid;
         }
-        return views[__ldg(&chunks[lo].view)];
+        return lo;
+    }
+    __device__ __forceinline__ const QueryView& of(uint32_t i) const
+    {
+        const unsigned int act = __activemask();
+        const int lead = __ffs(act) - 1;
+        int c = 0;
+        if ((int)(threadIdx.x & 31) == lead) c = search(i);
+        c = __shfl_sync(act, c, lead);
+        const long long st = __ldg(&chunks[c].start);
+        if (!((long long)i >= st && (long long)i < st + __ldg(&chunks[c].count))) c = search(i);
+        return views[__ldg(&chunks[c].view)];
     }
 };
 
@@ -4104,6 +4124,40 @@ void batch_make_chunks(const long long* offsets, int nseg, int chunk_points, con
     batch_write_chunks(offsets, nseg, chunk_points, swords, seg_view, out.data(), nchunks);
 }
 
+// Launches the batch locate instance of shape `shape` (statistics on when
+// `ctr` is set).
+template <int I>
+static void batch_locate_launch(int shape, int grid, cudaStream_t s, const QueryView* views, const BatchChunk* chunks,
+                                int nchunks, unsigned int* next_chunk, const double2* ll, uint8_t* out,
+                                uint32_t* queue, uint32_t* leafq, unsigned int* qcount, unsigned long long* ctr,
+                                int polls)
+{
+    if constexpr (I < BATCH_NSHAPES) {
+        if (shape != I) {
+            batch_locate_launch<I + 1>(shape, grid, s, views, chunks, nchunks, next_chunk, ll, out, queue, leafq,
+                                       qcount, ctr, polls);
+            return;
+        }
+        constexpr int U = BATCH_SHAPES[I].unroll, B = BATCH_SHAPES[I].blocks;
+        if (ctr)
+            k_batch_locate<true, U, B><<<grid, TPB, 0, s>>>(views, chunks, nchunks, next_chunk, ll, out, queue, leafq,
+                                                            qcount, ctr, polls);
+        else
+            k_batch_locate<false, U, B><<<grid, TPB, 0, s>>>(views, chunks, nchunks, next_chunk, ll, out, queue,
+                                                             leafq, qcount, ctr, polls);
+    }
+}
+
+int batch_shape_count() { return BATCH_NSHAPES; }
+
+bool batch_shape_info(int shape, int* points_per_thread, int* blocks_per_sm)
+{
+    if (shape < 0 || shape >= BATCH_NSHAPES) return false;
+    if (points_per_thread) *points_per_thread = BATCH_SHAPES[shape].unroll;
+    if (blocks_per_sm) *blocks_per_sm = BATCH_SHAPES[shape].blocks;
+    return true;
+}
+
 size_t batch_queue_words(long long queue_cap)
 {
     unsigned int cap2 = 0, cap3 = 0;
@@ -4118,7 +4172,7 @@ size_t batch_queue_words(long long queue_cap)
 gahhg_status batch_query_launch(const void* d_views, const void* d_chunks, int nchunks, const double* d_lonlat,
                                 uint8_t* d_labels, int precision, uint32_t* queue, long long queue_cap,
                                 unsigned int* counters, uint64_t* d_stats, cudaStream_t s, int device,
-                                bool zero_counters)
+                                bool zero_counters, int shape)
 {
     if (nchunks == 0) return GAHHG_OK;
     static std::atomic<int> sms_cache[64];
@@ -4132,7 +4186,6 @@ gahhg_status batch_query_launch(const void* d_views, const void* d_chunks, int n
     const BatchChunk* chunks = (const BatchChunk*)d_chunks;
     unsigned long long* ctr = (unsigned long long*)d_stats;
     if (zero_counters) GAHHG_CUDA_TRY(cudaMemsetAsync(counters, 0, 5 * sizeof(unsigned int), s));
-    const int grid = std::min(nchunks, sms * BATCH_BLOCKS);  // persistent: every block resident
     Tiers T;
     tier_caps(queue_cap, &T.cap2, &T.cap3);
     T.l1 = queue + queue_cap;
@@ -4143,12 +4196,10 @@ gahhg_status batch_query_launch(const void* d_views, const void* d_chunks, int n
     T.m2 = T.l3 + T.cap3;
     T.cnt = counters + 2;
     const int polls = (int)knob(GAHHG_KNOB_STAGING_POLL_LIMIT);
-    if (ctr)
-        k_batch_locate<true><<<grid, TPB, 0, s>>>(views, chunks, nchunks, counters + 1, (const double2*)d_lonlat,
-                                                  d_labels, queue, T.l1, counters, ctr, polls);
-    else
-        k_batch_locate<false><<<grid, TPB, 0, s>>>(views, chunks, nchunks, counters + 1, (const double2*)d_lonlat,
-                                                   d_labels, queue, T.l1, counters, ctr, polls);
+    if (shape < 0 || shape >= BATCH_NSHAPES) shape = 0;
+    const int grid = std::min(nchunks, sms * BATCH_SHAPES[shape].blocks);  // persistent: every block resident
+    batch_locate_launch<0>(shape, grid, s, views, chunks, nchunks, counters + 1, (const double2*)d_lonlat, d_labels,
+                           queue, T.l1, counters, ctr, polls);
     leaf_tiers_launch(ChunkViews{views, chunks, nchunks}, (const double2*)d_lonlat, d_labels, queue, counters, T,
                       precision, ctr, sms, s);
     GAHHG_CUDA_TRY(cudaGetLastError());

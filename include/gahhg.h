@@ -208,6 +208,14 @@ gahhg_status gahhg_batch_build(const gahhg_polygon* const* polys, int count, con
 int gahhg_batch_size(const gahhg_batch* b);
 /* Points per work chunk of the persistent query launch (default 4096). */
 gahhg_status gahhg_batch_set_chunk(gahhg_batch* b, int chunk_points);
+/* Launch shapes of the query's first pass (the descent to a leaf): shape
+ * `shape` runs `points_per_thread` points per thread in lockstep at
+ * `blocks_per_sm` resident blocks of 256 threads per SM.  Shapes are numbered
+ * from 0 (the default) until gahhg_batch_shape_info answers GAHHG_ERR_ARG.
+ * Labels do not depend on the shape; the fastest depends on the batch's mix
+ * of polygons and points (the autotuner measures them). */
+gahhg_status gahhg_batch_shape_info(int shape, int* points_per_thread, int* blocks_per_sm);
+gahhg_status gahhg_batch_set_shape(gahhg_batch* b, int shape);
 /* Labels for all polygons at once.  d_lonlat holds the points polygon after
  * polygon: polygon p owns points [offsets[p], offsets[p+1]) (host array of
  * count+1 entries, offsets[0] = 0, fewer than 2^32 points in all).  Exact

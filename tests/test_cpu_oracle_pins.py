@@ -133,6 +133,22 @@ def test_c_abi_exports_every_declared_symbol():
     assert L.gahhg_abi_version() == 1
 
 
+def test_batch_launch_shapes_listed_without_a_gpu():
+    """The batch query's pass-1 launch shapes are a host table: the default
+    first, each within the SM's resident-thread and shared-memory limits
+    (256 threads and 32 KB per block), and an index past the end is refused."""
+    import ctypes
+    import gahhg_b200 as G
+    from gahhg_b200 import _lib
+    shapes = G.Batch.shapes()
+    assert shapes[0] == (5, 5) and len(set(shapes)) == len(shapes) >= 4
+    for u, blocks in shapes:
+        assert 1 <= u <= 16 and blocks * 256 <= 2048 and blocks * 33 <= 227
+    a, b = ctypes.c_int(), ctypes.c_int()
+    assert _lib.lib().gahhg_batch_shape_info(len(shapes), ctypes.byref(a), ctypes.byref(b)) == _lib.ERR_ARG
+    assert _lib.lib().gahhg_batch_shape_info(-1, ctypes.byref(a), ctypes.byref(b)) == _lib.ERR_ARG
+
+
 def test_exact_oracle_agrees_with_reference_on_shipped_queries(oracle_ref, inputs, ref_outputs, tmp_path):
     """Away from the reference's tolerance band the two oracles must agree.
     Known exception: one Mars/001 query 5e-4 rad from the boundary that the

@@ -123,3 +123,61 @@ def test_summary_staged_by_bulk_copy(batch_case):
     B.query_device(d_pts.data_ptr(), off, lab.data_ptr(), G.QUERY_FP32_FILTER, sync=True)
     G.Grid(P[2], semantics=G.SEMANTICS_EXACT, device=0).classify().query(pts[2], G.QUERY_FP32_FILTER)
     assert G.staging_fallbacks(0) == before
+
+
+def test_group_boundaries_equal_single():
+    """Batches are built in groups of consecutive polygons of up to 2^20 edges
+    (a larger polygon is a group of its own): small polygons around the
+    1.1M-edge C1 polygon (groups [small], [C1], [small]) give the labels each
+    polygon's own build gives, on near-edge and uniform points; the batch
+    statistics count every polygon's edges."""
+    import torch
+    rng = np.random.default_rng(21)
+    small = synth.c3_polygons(6, seed=22, vmax=3000)
+    c1 = synth.c1_polygon()
+    rings = [r for r, _c, _r in small[:3]] + [c1] + [r for r, _c, _r in small[3:]]
+    P = [G.Polygon.from_rings(r) for r in rings]
+    pts = [np.concatenate([synth.near_edge_points(r, 3000, rng), synth.uniform_points(2000, rng)]) for r in rings]
+    B = G.Batch(P)
+    flat, off = _layout(pts)
+    d_pts = torch.from_numpy(flat).cuda()
+    lab = torch.zeros(len(flat), dtype=torch.uint8, device="cuda")
+    B.query_device(d_pts.data_ptr(), off, lab.data_ptr(), G.QUERY_FP32_FILTER, sync=True)
+    got = lab.cpu().numpy()
+    for i, poly in enumerate(P):
+        want = G.Grid(poly, semantics=G.SEMANTICS_EXACT).classify().query(pts[i], G.QUERY_FP32_FILTER)
+        seg = got[off[i]:off[i + 1]]
+        assert np.array_equal(seg, want), "polygon %d: %d labels differ" % (i, int((seg != want).sum()))
+    assert B.stats()["edges"] == sum(p.num_edges for p in P)
+
+
+def test_launch_shapes_give_the_same_labels(batch_case):
+    """Every pass-1 launch shape (points per thread x blocks per SM) gives the
+    default shape's labels and in-count, directly and through a graph that
+    the shape change recaptures; a chunk change recaptures it too."""
+    import torch
+    polys, pts, P = batch_case
+    shapes = G.Batch.shapes()
+    assert shapes[0] == (5, 5) and len(shapes) >= 2
+    B = G.Batch(P)
+    flat, off = _layout(pts)
+    d_pts = torch.from_numpy(flat).cuda()
+    want = torch.zeros(len(flat), dtype=torch.uint8, device="cuda")
+    B.query_device(d_pts.data_ptr(), off, want.data_ptr(), G.QUERY_FP32_FILTER, sync=True)
+    n_in = B.stats()["in_count"]
+    lab = torch.zeros(len(flat), dtype=torch.uint8, device="cuda")
+    B.query_device(d_pts.data_ptr(), off, lab.data_ptr(), G.QUERY_FP32_FILTER, graph=True)
+    for i in range(len(shapes)):
+        B.set_shape(i)
+        for chunk in (1024, 4096):
+            B.set_chunk(chunk)
+            lab.fill_(7)
+            B.query_device(d_pts.data_ptr(), off, lab.data_ptr(), G.QUERY_FP32_FILTER, sync=True)
+            assert torch.equal(lab, want), (shapes[i], chunk)
+            assert B.stats()["in_count"] == n_in
+            lab.fill_(7)
+            B.query_device(d_pts.data_ptr(), off, lab.data_ptr(), G.QUERY_FP32_FILTER, graph=True)
+            torch.cuda.synchronize()
+            assert torch.equal(lab, want), (shapes[i], chunk, "graph")
+    with pytest.raises(G.GahhgError):
+        B.set_shape(len(shapes))
