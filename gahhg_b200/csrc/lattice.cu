@@ -1643,13 +1643,13 @@ constexpr int BATCH_SUMMARY_WORDS = 4096;  // 16 KB of shared memory
 // C3 batch from 75.6 (8 points, two blocks) to 106.5 Gpts/s; 4 x 5 101.2,
 // 6 x 4 101.8, 6 x 5 102.3, 4 x 6 91.2, 8 x 3 93.5 (labels identical): more
 // warps hide more of the node descents' latency than more points per
-// thread.  Batches of other point mixes may prefer another row (2 x 6, at
-// 40 registers with a few bytes spilled, leaves fewer lanes idle in chunks
-// of few points); the batch autotuner measures them.
+// thread (2 x 6 spills at 40 registers and ran at 56.6).  Batches of other
+// point mixes may prefer another row (4 x 4 leaves fewer lanes idle in
+// chunks of few points); the batch autotuner measures them.
 struct BatchShape {
     int unroll, blocks;
 };
-constexpr BatchShape BATCH_SHAPES[] = {{5, 5}, {2, 6}, {6, 4}, {8, 3}};
+constexpr BatchShape BATCH_SHAPES[] = {{5, 5}, {4, 4}, {6, 4}, {8, 3}};
 constexpr int BATCH_NSHAPES = (int)(sizeof(BATCH_SHAPES) / sizeof(BATCH_SHAPES[0]));
 
 // Pass 1 over a batch: a persistent grid takes chunks in order from an atomic
@@ -1748,15 +1748,12 @@ struct OneView {
     __device__ __forceinline__ const QueryView& of(uint32_t) const { return Q; }
 };
 
-// ...or the chunk holding it: the first active lane of the warp finds its
-// point's chunk by binary search of the chunk starts and shares it, and a
-// lane whose point lies outside that chunk searches for its own (the queues
-// hold a chunk's points together, so most lanes share the first lane's).
+// ...or the chunk holding it (binary search of the chunk starts).
 struct ChunkViews {
     const QueryView* views;
     const BatchChunk* chunks;
     int nchunks;
-    __device__ __forceinline__ int search(uint32_t i) const
+    __device__ __forceinline__ const QueryView& of(uint32_t i) const
     {
         int lo = 0, hi = nchunks;  // chunks[lo].start <= i < chunks[hi].start
         while (hi - lo > 1) {
@@ -1764,18 +1761,7 @@ struct ChunkViews {
             if (__ldg(&chunks[mid].start) <= (long long)i) lo = mid;
             else hi = mid;
         }
-        return lo;
-    }
-    __device__ __forceinline__ const QueryView& of(uint32_t i) const
-    {
-        const unsigned int act = __activemask();
-        const int lead = __ffs(act) - 1;
-        int c = 0;
-        if ((int)(threadIdx.x & 31) == lead) c = search(i);
-        c = __shfl_sync(act, c, lead);
-        const long long st = __ldg(&chunks[c].start);
-        if (!((long long)i >= st && (long long)i < st + __ldg(&chunks[c].count))) c = search(i);
-        return views[__ldg(&chunks[c].view)];
+        return views[__ldg(&chunks[lo].view)];
     }
 };
 
