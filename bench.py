@@ -765,14 +765,17 @@ def leg_c2(args, g, gref, rings, stream):
             g.query_device(pp, n, lp, prec, sh)
         t = timed_loop(lambda: g.query_device(pp, n, lp, prec, sh), steps, stream)
         rates[name] = n * steps / t / 1e6
-    # pass 2 over the queue in leaf-bucket order (the default keeps pass-1
-    # order), FP32 filter, for comparison
-    old = G.set_knob(G.KNOB_GROUPED_PASS2, 1)
-    for _ in range(max(3, args.warmup)):
-        g.query_device(pp, n, lp, G.QUERY_FP32_FILTER, sh)
-    t = timed_loop(lambda: g.query_device(pp, n, lp, G.QUERY_FP32_FILTER, sh), steps, stream)
+    # pass 2 over the queue in leaf-window order and in leaf order (the
+    # default keeps pass-1 order), both precisions, for comparison
+    old = G.set_knob(G.KNOB_GROUPED_PASS2, 0)
+    for order, oname in ((1, "window_ordered"), (2, "leaf_sorted")):
+        G.set_knob(G.KNOB_GROUPED_PASS2, order)
+        for name, prec in (("fp32_filter", G.QUERY_FP32_FILTER), ("fp64_filter", G.QUERY_FP64_FILTER)):
+            for _ in range(max(3, args.warmup)):
+                g.query_device(pp, n, lp, prec, sh)
+            t = timed_loop(lambda: g.query_device(pp, n, lp, prec, sh), steps, stream)
+            rates["%s_%s_pass2" % (name, oname)] = n * steps / t / 1e6
     G.set_knob(G.KNOB_GROUPED_PASS2, old)
-    rates["leaf_ordered_pass2"] = n * steps / t / 1e6
     for _ in range(2):
         gref.query_device(pp, n, lp, G.QUERY_REFERENCE_FP64, sh)
     kref = 3
@@ -789,7 +792,7 @@ def leg_c2(args, g, gref, rings, stream):
         "fp32_filter_mpts": round(rates["fp32_filter"], 1),
         "fp64_filter_mpts": round(rates["fp64_filter"], 1),
         "fp32_over_fp64_filter": round(rates["fp32_filter"] / rates["fp64_filter"], 3),
-        "fp32_filter_leaf_ordered_pass2_mpts": round(rates["leaf_ordered_pass2"], 1),
+        "pass2_orders_mpts": {k[:-len("_pass2")]: round(v, 1) for k, v in rates.items() if k.endswith("_pass2")},
         "reference_fp64_descent_mpts": round(n / tref / 1e6, 1),
         "reference_fp64_max_depth": REF_DEPTH_C1,
         "roofline": {"bound": "hbm", "achieved": round(BYTES_PER_POINT * n / per32 / 1e9, 1), "peak": peak,

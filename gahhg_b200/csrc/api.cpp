@@ -208,8 +208,8 @@ namespace {
 constexpr int KNOB_COUNT = 8;
 constexpr long long KNOB_DEFAULT[KNOB_COUNT] = {0, 0, 1 << 16, 1 << 22, 1 << 20, 0, 0, 0};  // index = gahhg_knob
 std::atomic<long long> g_knobs[KNOB_COUNT] = {0, 0, 1 << 16, 1 << 22, 1 << 20, 0, 0, 0};
-// on/off knobs (0 or 1) rather than limits
-inline bool knob_is_switch(int k) { return k == GAHHG_KNOB_GROUPED_PASS2; }
+// knobs that choose among a few modes (0 .. knob_modes - 1) rather than limits
+inline int knob_modes(int k) { return k == GAHHG_KNOB_GROUPED_PASS2 ? 3 : 0; }
 }  // namespace
 
 long long knob(int k) { return (k > 0 && k < KNOB_COUNT) ? g_knobs[k].load(std::memory_order_relaxed) : 0; }
@@ -242,8 +242,12 @@ gahhg_status gahhg_set_knob(int k, long long value)
         set_error("unknown knob %d", k);
         return GAHHG_ERR_ARG;
     }
-    if (knob_is_switch(k) ? (value != 0 && value != 1) : (value < 0 || value > KNOB_DEFAULT[k])) {
-        set_error("knob %d takes %s, not %lld", k, knob_is_switch(k) ? "0 or 1" : "0 .. its default", value);
+    const int modes = knob_modes(k);
+    if (modes ? (value < 0 || value >= modes) : (value < 0 || value > KNOB_DEFAULT[k])) {
+        if (modes)
+            set_error("knob %d takes 0 .. %d, not %lld", k, modes - 1, value);
+        else
+            set_error("knob %d takes 0 .. its default, not %lld", k, value);
         return GAHHG_ERR_ARG;
     }
     gahhg::g_knobs[k].store(value, std::memory_order_relaxed);

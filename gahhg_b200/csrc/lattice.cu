@@ -2069,6 +2069,146 @@ __global__ void __launch_bounds__(P_TPB) k_part_scatter(const uint32_t* __restri
     if (blockIdx.x == 0 && threadIdx.x == 0) *S.done = 1u;
 }
 
+// --------------------------------------- pass-2 queue in leaf order --
+//
+// The finest order: a counting sort of the pass-1 queue by leaf, so that the
+// points of one leaf sit together and the warps of the first tier mostly
+// take points of one leaf (their loads of the leaf's record and edge records
+// are then one request per warp, served by L1 after the first).  Four
+// launches:
+//   k_ls_count      each entry takes its rank in its leaf (an atomic on the
+//                   leaf's count; the last bucket holds points pass 1 did not
+//                   locate);
+//   k_ls_tile_sums  the counts' sums per tile of LS_TILE leaves;
+//   k_ls_scan       each block scans one tile, starting from the sum of the
+//                   tiles before it (no waits between blocks);
+//   k_ls_scatter    each entry goes to its leaf's start plus its rank.
+// The counts, ranks and the sorted arrays of a C2 pass fit in L2, so the
+// random atomics and writes of the sort do not reach DRAM.
+constexpr int LS_TPB = 256;
+constexpr int LS_ITEMS = 16;
+constexpr int LS_TILE = LS_TPB * LS_ITEMS;
+
+struct LeafSortScratch {
+    unsigned int* cnt;    // [nb] entries per bucket; zero before the pass
+    unsigned int* start;  // [nb + 1] exclusive prefix of cnt
+    unsigned int* tsum;   // [tiles] sums of cnt per tile
+    unsigned int* rank;   // [queue] an entry's rank in its bucket
+    uint32_t* spts;       // point indices in leaf order
+    uint32_t* sleaf;      // their leaf words
+    unsigned int* done;   // set to 1 with the sorted arrays; zero before the pass
+    int nb;               // buckets: leaves + 1
+    int tiles;            // ceil(nb / LS_TILE)
+};
+
+__device__ __forceinline__ int leaf_bucket(uint32_t w, int nb)
+{
+    return (w & KIND_MASK) == KIND_LEAF ? (int)min(w & INDEX_MASK, (uint32_t)(nb - 1)) : nb - 1;
+}
+
+__global__ void __launch_bounds__(LS_TPB) k_ls_count(const uint32_t* __restrict__ l1,
+                                                     const unsigned int* __restrict__ qcount, LeafSortScratch S)
+{
+    wait_for_predecessor();
+    const unsigned int m = *qcount;
+    if (m >= PART_MIN_QUEUE)
+        for (unsigned int t = blockIdx.x * LS_TPB + threadIdx.x; t < m; t += gridDim.x * LS_TPB)
+            S.rank[t] = atomicAdd(S.cnt + leaf_bucket(l1[t], S.nb), 1u);
+    allow_dependents();
+}
+
+// Block-wide sum of one value per thread (every thread gets it).
+__device__ __forceinline__ unsigned int ls_block_sum(unsigned int v, unsigned int* s_w)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();  // s_w may still be read from the previous call
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = v;
+    __syncthreads();
+    unsigned int t = 0;
+#pragma unroll
+    for (int k = 0; k < LS_TPB / 32; k++) t += s_w[k];
+    return t;
+}
+
+__global__ void __launch_bounds__(LS_TPB) k_ls_tile_sums(const unsigned int* __restrict__ qcount, LeafSortScratch S)
+{
+    __shared__ unsigned int s_w[LS_TPB / 32];
+    wait_for_predecessor();
+    if (*qcount >= PART_MIN_QUEUE) {
+        for (int tile = blockIdx.x; tile < S.tiles; tile += gridDim.x) {
+            unsigned int v = 0;
+            const int b0 = tile * LS_TILE;
+            for (int k = threadIdx.x; k < LS_TILE; k += LS_TPB)
+                if (b0 + k < S.nb) v += S.cnt[b0 + k];
+            v = ls_block_sum(v, s_w);
+            if (threadIdx.x == 0) S.tsum[tile] = v;
+        }
+    }
+    allow_dependents();
+}
+
+__global__ void __launch_bounds__(LS_TPB) k_ls_scan(const unsigned int* __restrict__ qcount, LeafSortScratch S)
+{
+    __shared__ unsigned int s_w[LS_TPB / 32];
+    __shared__ unsigned int s_wx[LS_TPB / 32];
+    wait_for_predecessor();
+    if (*qcount >= PART_MIN_QUEUE) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int tile = blockIdx.x; tile < S.tiles; tile += gridDim.x) {
+            unsigned int before = 0;
+            for (int k = threadIdx.x; k < tile; k += LS_TPB) before += S.tsum[k];
+            before = ls_block_sum(before, s_w);
+            // this thread's LS_ITEMS consecutive buckets
+            const int b0 = tile * LS_TILE + threadIdx.x * LS_ITEMS;
+            unsigned int c[LS_ITEMS], run = 0;
+#pragma unroll
+            for (int k = 0; k < LS_ITEMS; k++) {
+                c[k] = b0 + k < S.nb ? S.cnt[b0 + k] : 0u;
+                run += c[k];
+            }
+            // exclusive scan of the threads' totals: in the warp, then over warps
+            unsigned int x = run;
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            __syncthreads();  // s_wx may still be read from the previous tile
+            if (lane == 31) s_wx[warp] = x;
+            __syncthreads();
+            unsigned int wbase = 0;
+            for (int k = 0; k < warp; k++) wbase += s_wx[k];
+            unsigned int at = before + wbase + x - run;
+#pragma unroll
+            for (int k = 0; k < LS_ITEMS; k++) {
+                if (b0 + k < S.nb) S.start[b0 + k] = at;
+                at += c[k];
+            }
+            if (b0 <= S.nb - 1 && S.nb - 1 < b0 + LS_ITEMS) S.start[S.nb] = at;  // the total
+        }
+    }
+    allow_dependents();
+}
+
+__global__ void __launch_bounds__(LS_TPB) k_ls_scatter(const uint32_t* __restrict__ queue,
+                                                       const uint32_t* __restrict__ l1,
+                                                       const unsigned int* __restrict__ qcount, LeafSortScratch S)
+{
+    wait_for_predecessor();
+    const unsigned int m = *qcount;
+    if (m >= PART_MIN_QUEUE) {
+        for (unsigned int t = blockIdx.x * LS_TPB + threadIdx.x; t < m; t += gridDim.x * LS_TPB) {
+            const uint32_t w = l1[t];
+            const unsigned int at = S.start[leaf_bucket(w, S.nb)] + S.rank[t];
+            if (at < m) {  // counts and entries agree; never write past the queue
+                S.spts[at] = queue[t];
+                S.sleaf[at] = w;
+            }
+        }
+    }
+    allow_dependents();
+    if (m >= PART_MIN_QUEUE && blockIdx.x == 0 && threadIdx.x == 0) *S.done = 1u;
+}
+
 // Launch with programmatic stream serialization (see wait_for_predecessor).
 template <typename... KArgs, typename... Args>
 void launch_dependent_tpb(void (*kernel)(KArgs...), int grid, int tpb, cudaStream_t s, Args... args)
@@ -3334,7 +3474,7 @@ gahhg_status lattice_build(Grid* g)
 gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long long n, uint8_t* d_labels,
                                 int precision, cudaStream_t s, uint64_t* d_counters, uint32_t* queue,
                                 unsigned int* qcount, long long chunk, int device, const Tiers* tiers,
-                                const PartScratch* part = nullptr);
+                                const PartScratch* part = nullptr, const LeafSortScratch* lsort = nullptr);
 
 // The locate arithmetic of a view from its level-0 grid.
 static void set_view_geo(QueryView& Q, const Geo& g)
@@ -3918,12 +4058,20 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
     // [its leaf words][tier-3 queue][its leaf words][tier-2 masks][queue in
     // window order: points, leaf words (chunk each)].
     // One memset per pass clears the control words from the queue fill on.
+    // [leaf order only: entries per leaf: nb][leaf starts: nb + 1][tile
+    // sums][ranks: chunk].
     unsigned int cap2 = 0, cap3 = 0;
     tier_caps(chunk, &cap2, &cap3);
-    const bool windows = knob(GAHHG_KNOB_GROUPED_PASS2) != 0 && Q.nparts > 1 && chunk >= PART_MIN_QUEUE;
+    const long long order = knob(GAHHG_KNOB_GROUPED_PASS2);
+    const bool windows = order == 1 && Q.nparts > 1 && chunk >= PART_MIN_QUEUE;
+    const bool leaves = order == 2 && chunk >= PART_MIN_QUEUE && g->lattice->nleaves > 0 &&
+                        g->lattice->nleaves < (1LL << 30);
+    const int nb = leaves ? (int)g->lattice->nleaves + 1 : 0;
+    const int tiles = (nb + LS_TILE - 1) / LS_TILE;
     const size_t l1_at = (size_t)chunk + 192;
     const size_t sorted_at = l1_at + (size_t)chunk + 3 * (size_t)cap2 + 2 * (size_t)cap3;
-    const size_t words = sorted_at + (windows ? 2 * (size_t)chunk : 0);
+    const size_t ls_at = sorted_at + 2 * (size_t)chunk;
+    const size_t words = windows ? ls_at : leaves ? ls_at + 2 * (size_t)nb + 1 + tiles + (size_t)chunk : sorted_at;
     uint32_t* queue = nullptr;
     GAHHG_TRY(pool_alloc((void**)&queue, sizeof(uint32_t) * words, g->device, s));
     unsigned int* qcount = (unsigned int*)(queue + chunk + 32);
@@ -3945,8 +4093,19 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
     W.sleaf = queue + sorted_at + chunk;
     W.np = Q.nparts;
     W.scale = Q.part_scale;
+    LeafSortScratch LS;
+    LS.done = qcount + 4;
+    LS.spts = queue + sorted_at;
+    LS.sleaf = queue + sorted_at + chunk;
+    LS.cnt = queue + ls_at;
+    LS.start = LS.cnt + nb;
+    LS.tsum = LS.start + nb + 1;
+    LS.rank = LS.tsum + tiles;
+    LS.nb = nb;
+    LS.tiles = tiles;
     const gahhg_status st = lattice_query_with(Q, d_lonlat, (long long)n, d_labels, precision, s, d_counters,
-                                               queue, qcount, chunk, g->device, &T, windows ? &W : nullptr);
+                                               queue, qcount, chunk, g->device, &T, windows ? &W : nullptr,
+                                               leaves ? &LS : nullptr);
     cudaFreeAsync(queue, s);
     return st;
 }
@@ -3956,7 +4115,7 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
 gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long long n, uint8_t* d_labels,
                                 int precision, cudaStream_t s, uint64_t* d_counters, uint32_t* queue,
                                 unsigned int* qcount, long long chunk, int device, const Tiers* tiers,
-                                const PartScratch* part)
+                                const PartScratch* part, const LeafSortScratch* lsort)
 {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -3966,8 +4125,9 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
         const double2* ll = (const double2*)d_lonlat + off;
         // the queue fill, the tier counters and, when ordering by window, the
         // flag, the counts and the cursors (the control words run up to them)
-        const size_t zero_words = part ? (size_t)(part->cursor + PART_MAX - qcount) : (tiers ? 4 : 1);
+        const size_t zero_words = part ? (size_t)(part->cursor + PART_MAX - qcount) : lsort ? 5 : (tiers ? 4 : 1);
         GAHHG_CUDA_TRY(cudaMemsetAsync(qcount, 0, sizeof(unsigned int) * zero_words, s));
+        if (lsort) GAHHG_CUDA_TRY(cudaMemsetAsync(lsort->cnt, 0, sizeof(unsigned int) * lsort->nb, s));
         const long long tiles = ((long long)m + TPB * LOC_UNROLL - 1) / (TPB * LOC_UNROLL);
         const int grid = (int)std::min<long long>(tiles, (long long)sms * 8);
         uint32_t* leafq = tiers ? tiers->l1 : nullptr;
@@ -3984,6 +4144,19 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
             T.spts = part->spts;
             T.sleaf = part->sleaf;
             T.sorted = part->done;
+            leaf_tiers_launch(OneView{Q}, ll, d_labels + off, queue, qcount, T, precision, ctr, sms, s);
+        } else if (tiers && lsort) {
+            // the pass-1 queue in leaf order, then the tiers over it
+            const uint32_t* l1 = tiers->l1;
+            const unsigned int* qc = qcount;
+            launch_dependent_tpb(k_ls_count, sms * 8, LS_TPB, s, l1, qc, *lsort);
+            launch_dependent_tpb(k_ls_tile_sums, std::min(lsort->tiles, sms * 8), LS_TPB, s, qc, *lsort);
+            launch_dependent_tpb(k_ls_scan, std::min(lsort->tiles, sms * 8), LS_TPB, s, qc, *lsort);
+            launch_dependent_tpb(k_ls_scatter, sms * 8, LS_TPB, s, (const uint32_t*)queue, l1, qc, *lsort);
+            Tiers T = *tiers;
+            T.spts = lsort->spts;
+            T.sleaf = lsort->sleaf;
+            T.sorted = lsort->done;
             leaf_tiers_launch(OneView{Q}, ll, d_labels + off, queue, qcount, T, precision, ctr, sms, s);
         } else if (tiers) {
             leaf_tiers_launch(OneView{Q}, ll, d_labels + off, queue, qcount, *tiers, precision, ctr, sms, s);

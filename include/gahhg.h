@@ -361,13 +361,12 @@ gahhg_status gahhg_grid0_export(double* v, void* b, void* c);
 gahhg_status gahhg_staging_fallbacks(int device, unsigned long long* count);
 
 /* Process-wide tuning and test knobs.  No counterpart in the reference.
- * GAHHG_KNOB_GROUPED_PASS2: 1 puts the points that pass 1 of a
- * single-polygon exact query could not label in order of windows of
- * consecutive leaves (about 24 MB of index each) before the crossing tests
- * run, when there are enough of them and the index spans several windows;
- * 0 (default) keeps them in input order.  Labels are the same either way; on
- * a B200 the ordering costs more than the locality it buys (measured on
- * near-edge points).
+ * GAHHG_KNOB_GROUPED_PASS2: the order in which the crossing tests take the
+ * points that pass 1 of a single-polygon exact query could not label, when
+ * there are at least 2^18 of them: 0 (default) input order; 1 windows of
+ * consecutive leaves (about 24 MB of index each; only when the index spans
+ * several windows); 2 leaf order (a counting sort by leaf).  Labels are the
+ * same in every order.
  * Values take effect for work enqueued after the call. */
 typedef enum {
     GAHHG_KNOB_GROUPED_PASS2 = 1,
