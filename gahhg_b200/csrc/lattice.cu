@@ -1202,7 +1202,10 @@ constexpr uint32_t MASK_ALL = 0xFFFFFFFFu;
 // the default leaf size): the first group goes out before the offset's
 // arithmetic, so its latency hides behind the sines and cosines.
 constexpr int T1_GROUP = 4;
-constexpr int T1_BLOCKS = 4;  // blocks per SM of tier 1 (registers)
+// Blocks per SM of tier 1: five (48 registers, 20 bytes spilled) ran C2 at
+// 21.0-21.1 Gpts/s against 20.5 at four (56 registers); five with groups of
+// two (no spills) 20.5, six with groups of two (40 registers) 20.8.
+constexpr int T1_BLOCKS = 5;
 
 __device__ __forceinline__ uint8_t leaf_label_fp32(const QueryView& Q, const LeafRec& L, const PointCtx& P,
                                                  uint32_t& mask)
