@@ -1867,10 +1867,18 @@ __global__ void __launch_bounds__(TPB, T1_BLOCKS) k_leaf_t1(VS vs, const double2
     if (ctr) count_stats(ctr, inside, boundary, fp64, 0);
 }
 
+// Tier 2's shape: blocks of 128 threads, five per SM (96 registers, about
+// 60 bytes spilled) hold 20 warps per SM where 256-thread blocks at 110
+// registers held 16: FP64-filter queries of C2 (tier 2 over the whole
+// pass-1 queue) 15.8 -> 16.6 Gpts/s; six blocks (80 registers, 200 bytes
+// spilled) 12.8; the FP32 filter's tier 2 is unchanged by any of them.
+constexpr int T2_TPB = 128;
+constexpr int T2_BLOCKS = 5;
+
 // Tier 2 over the tier-1 queue, or (FROM_PASS1, FP64-filter queries) over
 // the pass-1 queue itself.
 template <class VS, bool FROM_PASS1>
-__global__ void __launch_bounds__(TPB) k_leaf_t2(VS vs, const double2* __restrict__ ll, uint8_t* __restrict__ out,
+__global__ void __launch_bounds__(T2_TPB, T2_BLOCKS) k_leaf_t2(VS vs, const double2* __restrict__ ll, uint8_t* __restrict__ out,
                                                 const uint32_t* __restrict__ src, const uint32_t* __restrict__ src_leaf,
                                                 const unsigned int* __restrict__ src_count, unsigned int src_cap,
                                                 Tiers T, unsigned long long* ctr)
@@ -2242,12 +2250,12 @@ void leaf_tiers_launch(const VS& vs, const double2* ll, uint8_t* out, const uint
                        cudaStream_t s)
 {
     if (precision == GAHHG_QUERY_FP64_FILTER) {
-        launch_dependent(k_leaf_t2<VS, true>, sms * 4, s, vs, ll, out, queue, (const uint32_t*)T.l1, qcount,
-                         0xffffffffu, T, ctr);
+        launch_dependent_tpb(k_leaf_t2<VS, true>, sms * T2_BLOCKS, T2_TPB, s, vs, ll, out, queue,
+                             (const uint32_t*)T.l1, qcount, 0xffffffffu, T, ctr);
     } else {
         launch_dependent(k_leaf_t1<VS>, sms * T1_BLOCKS, s, vs, ll, out, queue, qcount, T, ctr);
-        launch_dependent(k_leaf_t2<VS, false>, sms * 4, s, vs, ll, out, (const uint32_t*)T.q2,
-                         (const uint32_t*)T.l2, (const unsigned int*)T.cnt, T.cap2, T, ctr);
+        launch_dependent_tpb(k_leaf_t2<VS, false>, sms * T2_BLOCKS, T2_TPB, s, vs, ll, out, (const uint32_t*)T.q2,
+                             (const uint32_t*)T.l2, (const unsigned int*)T.cnt, T.cap2, T, ctr);
     }
     launch_dependent(k_leaf_t3<VS>, sms * 2, s, vs, ll, out, queue, qcount, T, ctr);
 }
