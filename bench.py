@@ -768,7 +768,7 @@ def leg_c2(args, g, gref, rings, stream):
     # pass 2 over the queue in leaf-window order and in leaf order (the
     # default keeps pass-1 order), both precisions, for comparison
     old = G.set_knob(G.KNOB_GROUPED_PASS2, 0)
-    for order, oname in ((1, "window_ordered"), (2, "leaf_sorted")):
+    for order, oname in ((1, "window_ordered"), (2, "leaf_sorted"), (3, "leaf_sorted_staged")):
         G.set_knob(G.KNOB_GROUPED_PASS2, order)
         for name, prec in (("fp32_filter", G.QUERY_FP32_FILTER), ("fp64_filter", G.QUERY_FP64_FILTER)):
             for _ in range(max(3, args.warmup)):

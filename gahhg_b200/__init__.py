@@ -344,8 +344,9 @@ def write_result(path, labels):
 
 
 def staging_fallbacks(device=0):
-    """Locate blocks on `device` whose bulk copy of the coarse summary ran out
-    of time and fell back to plain loads (0 in normal operation)."""
+    """Blocks on `device` whose bulk copy into shared memory (the locate
+    pass's coarse summary, or a staged tier-1 tile's edge lists) ran out of
+    time and fell back to plain loads (0 in normal operation)."""
     v = ctypes.c_ulonglong(0)
     check(_lib.lib().gahhg_staging_fallbacks(int(device), ctypes.byref(v)))
     return int(v.value)

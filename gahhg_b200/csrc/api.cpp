@@ -209,7 +209,7 @@ constexpr int KNOB_COUNT = 8;
 constexpr long long KNOB_DEFAULT[KNOB_COUNT] = {0, 0, 1 << 16, 1 << 22, 1 << 20, 0, 0, 0};  // index = gahhg_knob
 std::atomic<long long> g_knobs[KNOB_COUNT] = {0, 0, 1 << 16, 1 << 22, 1 << 20, 0, 0, 0};
 // knobs that choose among a few modes (0 .. knob_modes - 1) rather than limits
-inline int knob_modes(int k) { return k == GAHHG_KNOB_GROUPED_PASS2 ? 3 : 0; }
+inline int knob_modes(int k) { return k == GAHHG_KNOB_GROUPED_PASS2 ? 4 : 0; }
 }  // namespace
 
 long long knob(int k) { return (k > 0 && k < KNOB_COUNT) ? g_knobs[k].load(std::memory_order_relaxed) : 0; }

@@ -40,6 +40,7 @@
 #include <cstring>
 #include <mutex>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "exact_pred.cuh"
@@ -1207,14 +1208,25 @@ constexpr int T1_GROUP = 4;
 // two (no spills) 20.5, six with groups of two (40 registers) 20.8.
 constexpr int T1_BLOCKS = 5;
 
-__device__ __forceinline__ uint8_t leaf_label_fp32(const QueryView& Q, const LeafRec& L, const PointCtx& P,
-                                                 uint32_t& mask)
+// A record of tier 1: from global memory through the read-only path, or
+// from a copy in shared memory (SHARED).
+template <bool SHARED>
+__device__ __forceinline__ float4 t1_record(const float4* p)
 {
-    const float4* rec = Q.recs + L.off;
+    if constexpr (SHARED) return *p;
+    else return __ldg(p);
+}
+
+// Tier 1 on the leaf L whose records start at rec (global memory, or the
+// staged copy in shared memory when SHARED).
+template <bool SHARED>
+__device__ __forceinline__ uint8_t leaf_label_fp32_at(const float4* rec, const LeafRec& L, const PointCtx& P,
+                                                    uint32_t& mask)
+{
     const int cnt = L.cnt;
     float4 r[T1_GROUP];
 #pragma unroll
-    for (int j = 0; j < T1_GROUP; j++) r[j] = j < cnt ? __ldg(rec + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int j = 0; j < T1_GROUP; j++) r[j] = j < cnt ? t1_record<SHARED>(rec + j) : make_float4(0.f, 0.f, 0.f, 0.f);
     local_frame::Frame f;
     if (!(fabs(P.lon) <= 540.0) || !local_frame::frame_at(P.lon, P.lat, L.lon, L.lat, L.sb, L.cb, f)) {
         mask = MASK_ALL;
@@ -1229,7 +1241,7 @@ __device__ __forceinline__ uint8_t leaf_label_fp32(const QueryView& Q, const Lea
         if (k0 > 0) {
 #pragma unroll
             for (int j = 0; j < T1_GROUP; j++)
-                r[j] = k0 + j < cnt ? __ldg(rec + k0 + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+                r[j] = k0 + j < cnt ? t1_record<SHARED>(rec + k0 + j) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
 #pragma unroll
         for (int j = 0; j < T1_GROUP; j++) {
@@ -1254,6 +1266,12 @@ __device__ __forceinline__ uint8_t leaf_label_fp32(const QueryView& Q, const Lea
         return LABEL_DEFER;
     }
     return (uint8_t)(par ? 3 - L.label : L.label);
+}
+
+__device__ __forceinline__ uint8_t leaf_label_fp32(const QueryView& Q, const LeafRec& L, const PointCtx& P,
+                                                 uint32_t& mask)
+{
+    return leaf_label_fp32_at<false>(Q.recs + L.off, L, P, mask);
 }
 
 // Edges of a leaf whose FP64 endpoints the FP64 tier loads together: their
@@ -1733,15 +1751,19 @@ struct Tiers {
     const uint32_t* spts = nullptr;
     const uint32_t* sleaf = nullptr;
     const unsigned int* sorted = nullptr;
+    int sstride = 1;  // words from one ordered entry to the next (2: leaf order's interleaved pairs)
 };
 
 // The pass-1 queue as the first tier reads it: in window order when
 // k_part_scatter ran, else in pass-1 order.
-__device__ __forceinline__ void first_tier_source(const Tiers& T, const uint32_t*& pts, const uint32_t*& leaf)
+__device__ __forceinline__ void first_tier_source(const Tiers& T, const uint32_t*& pts, const uint32_t*& leaf,
+                                                  unsigned int& stride)
 {
+    stride = 1;
     if (T.sorted && *(const volatile unsigned int*)T.sorted == 1u) {
         pts = T.spts;
         leaf = T.sleaf;
+        stride = (unsigned int)T.sstride;
     }
 }
 
@@ -1808,7 +1830,8 @@ __global__ void __launch_bounds__(TPB, T1_BLOCKS) k_leaf_t1(VS vs, const double2
     const unsigned int m = *qcount;
     const uint32_t* src = queue;
     const uint32_t* src_leaf = T.l1;
-    first_tier_source(T, src, src_leaf);
+    unsigned int st;
+    first_tier_source(T, src, src_leaf, st);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int inside = 0, boundary = 0, fp64 = 0;
     // block-uniform loop: the deferred points of a block's round take one
@@ -1819,10 +1842,10 @@ __global__ void __launch_bounds__(TPB, T1_BLOCKS) k_leaf_t1(VS vs, const double2
         bool defer = false;
         uint32_t i = 0, w = 0, mask = 0;
         if (t < m) {
-            i = src[t];
+            i = src[t * st];
             const QueryView& Q = vs.of(i);
             PointCtx P;
-            w = point_leaf(Q, ll[i], P, src_leaf[t]);
+            w = point_leaf(Q, ll[i], P, src_leaf[t * st]);
             uint8_t lab;
             if ((w & KIND_MASK) == KIND_PURE) {
                 lab = (uint8_t)(w & 3u);
@@ -1867,6 +1890,202 @@ __global__ void __launch_bounds__(TPB, T1_BLOCKS) k_leaf_t1(VS vs, const double2
     if (ctr) count_stats(ctr, inside, boundary, fp64, 0);
 }
 
+// ---------------------------------- tier 1 with the edge lists staged --
+//
+// Over the pass-1 queue in leaf order (k_ls_*), the entries of a tile of TPB
+// consecutive entries lie in a run of consecutive leaves, and leaves are
+// numbered so that their records are contiguous: the tile's leaf records and
+// the edge records of those leaves are two contiguous slices of the index.
+// One thread copies both into shared memory (TMA: two untiled cp.async.bulk
+// global -> shared, completion counted in bytes on one mbarrier; no
+// multicast, the source is this GPU's index) while the block loads its
+// points and their frames, and every crossing test of the tile then reads
+// its leaf record and edge list from shared memory.  A tile whose slices do
+// not fit the buffers, a tile holding points pass 1 did not locate, and every
+// tile of a queue left in pass-1 order (below PART_MIN_QUEUE entries) read
+// the index from global memory as k_leaf_t1 does.  Every wait is bounded: a
+// wait that runs out makes the block stop staging (its later tiles read
+// global memory, so the late copy is never read), is counted once in
+// g_tma_timeouts, and before exiting the block waits (bounded again) for
+// that copy.  Both slices start on 16-byte boundaries (pool allocations are
+// 256-byte aligned; leaf records are 32 bytes, edge records 16) and their
+// sizes are multiples of 16 bytes.
+constexpr int T1S_LEAVES = 256;  // 8 KB of leaf records per tile
+constexpr int T1S_RECS = 1536;   // 24 KB of edge records per tile
+constexpr int T1S_BLOCKS = 5;
+
+__global__ void __launch_bounds__(TPB, T1S_BLOCKS) k_leaf_t1s(QueryView Q, const double2* __restrict__ ll,
+                                                            uint8_t* __restrict__ out,
+                                                            const uint32_t* __restrict__ queue,
+                                                            const unsigned int* __restrict__ qcount, Tiers T,
+                                                            unsigned long long* ctr, int polls)
+{
+    __shared__ __align__(16) LeafRec s_leaf[T1S_LEAVES];
+    __shared__ __align__(16) float4 s_rec[T1S_RECS];
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ unsigned int s_wcnt[TPB / 32];
+    __shared__ unsigned int s_base;
+    __shared__ uint32_t s_l0, s_r0, s_nr;  // first staged leaf, first staged record, records staged
+    __shared__ int s_nl;                   // leaves staged for the tile (0: none)
+    __shared__ int s_broken;               // a wait ran out: no more staging
+    if (threadIdx.x == 0) {
+        mbar_init(&s_bar);
+        s_broken = 0;
+    }
+    __syncthreads();
+    wait_for_predecessor();
+    const unsigned int m = *qcount;
+    const uint32_t* src = queue;
+    const uint32_t* src_leaf = T.l1;
+    unsigned int st;
+    first_tier_source(T, src, src_leaf, st);
+    const bool sorted = src_leaf != T.l1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int inside = 0, boundary = 0, fp64 = 0;
+    uint32_t phase = 0;  // parity of the barrier's current phase
+    // Thread 0 works a tile ahead so that a tile's copy goes out as the tile
+    // starts: while the block labels tile k it loads the first and last leaf
+    // words of tile k + 1, and after the labels those leaves' record
+    // offsets (the bounds, state 1; 2 when the slices do not fit).
+    // (thread 0's state is kept in shared memory, off the other threads'
+    // registers)
+    const unsigned int bstep = gridDim.x * blockDim.x;
+    __shared__ uint32_t s_nw0, s_nw1;                 // next tile's first and last leaf words
+    __shared__ uint32_t s_bL0, s_bL1, s_br0, s_br1;  // its leaves and record range
+    __shared__ int s_bstate;                          // 0 not known, 1 staged, 2 not staged
+    auto tile_words = [&](unsigned int b) {
+        s_nw0 = src_leaf[b * st];
+        s_nw1 = src_leaf[(min(b + TPB, m) - 1) * st];
+    };
+    auto tile_bounds = [&]() {
+        const uint32_t w0 = s_nw0, w1 = s_nw1;
+        s_bstate = 2;
+        if ((w0 & KIND_MASK) != KIND_LEAF || (w1 & KIND_MASK) != KIND_LEAF) return;
+        const uint32_t L0 = w0 & INDEX_MASK, L1 = w1 & INDEX_MASK;
+        if (L1 < L0 || L1 - L0 >= (uint32_t)T1S_LEAVES) return;
+        const uint32_t r0 = Q.leaves[L0].off, r1 = Q.leaves[L1].off + Q.leaves[L1].cnt;
+        if (r1 < r0 || r1 - r0 > (uint32_t)T1S_RECS) return;
+        s_bL0 = L0;
+        s_bL1 = L1;
+        s_br0 = r0;
+        s_br1 = r1;
+        s_bstate = 1;
+    };
+    if (threadIdx.x == 0) s_bstate = 0;
+    if (threadIdx.x == 0 && sorted && blockIdx.x * blockDim.x < m) tile_words(blockIdx.x * blockDim.x);
+    for (unsigned int b0 = blockIdx.x * blockDim.x; b0 < m; b0 += bstep) {
+        if (threadIdx.x == 0) {
+            int nl = 0;
+            if (sorted && !s_broken) {
+                if (s_bstate == 0) tile_bounds();  // the first tile
+                if (s_bstate == 1) {
+                    const uint32_t bL0 = s_bL0, br0 = s_br0;
+                    nl = (int)(s_bL1 - bL0 + 1);
+                    s_l0 = bL0;
+                    s_r0 = br0;
+                    s_nr = s_br1 - br0;
+                    const uint32_t lb = (uint32_t)nl * (uint32_t)sizeof(LeafRec);
+                    const uint32_t rb = (s_br1 - br0) * (uint32_t)sizeof(float4);
+                    // the previous tile's reads of the buffers (ordered by
+                    // the block barrier) come before these writes
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&s_bar)),
+                                 "r"(lb + rb)
+                                 : "memory");
+                    asm volatile(
+                        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                            smem_u32(s_leaf)),
+                        "l"(Q.leaves + bL0), "r"(lb), "r"(smem_u32(&s_bar))
+                        : "memory");
+                    if (rb)
+                        asm volatile(
+                            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+                            "[%3];" ::"r"(smem_u32(s_rec)),
+                            "l"(Q.recs + br0), "r"(rb), "r"(smem_u32(&s_bar))
+                            : "memory");
+                }
+            }
+            s_nl = nl;
+            s_bstate = 0;
+            if (sorted && b0 + bstep < m) tile_words(b0 + bstep);
+        }
+        // every thread's point and frame while the copy is in flight
+        const unsigned int t = b0 + threadIdx.x;
+        bool defer = false;
+        uint32_t i = 0, w = 0, mask = 0;
+        PointCtx P;
+        if (t < m) {
+            i = src[t * st];
+            w = point_leaf(Q, ll[i], P, src_leaf[t * st]);
+        }
+        __syncthreads();
+        const int nl = s_nl;
+        bool staged = false;
+        if (nl) {
+            staged = mbar_wait(&s_bar, phase, polls);
+            phase ^= 1u;
+            if (!staged) s_broken = 1;
+        }
+        if (t < m) {
+            uint8_t lab;
+            if ((w & KIND_MASK) == KIND_PURE) {
+                lab = (uint8_t)(w & 3u);
+            } else {
+                boundary++;
+                const uint32_t li = (w & INDEX_MASK) - s_l0;  // wraps above nl below the first leaf
+                bool done = false;
+                if (staged && li < (uint32_t)nl) {
+                    const LeafRec L = s_leaf[li];
+                    const uint32_t ro = L.off - s_r0;
+                    if (ro <= s_nr && (uint32_t)L.cnt <= s_nr - ro) {
+                        lab = leaf_label_fp32_at<true>(s_rec + ro, L, P, mask);
+                        done = true;
+                    }
+                }
+                if (!done) lab = leaf_label_fp32(Q, Q.leaves[w & INDEX_MASK], P, mask);
+            }
+            if (lab == LABEL_DEFER) {
+                fp64++;
+                defer = true;
+            } else {
+                out[i] = lab;
+                inside += lab == CELL_IN;
+            }
+        }
+        if (threadIdx.x == 0 && sorted && b0 + bstep < m) tile_bounds();  // the next tile's, ahead of its start
+        const unsigned int bal = __ballot_sync(0xffffffffu, defer);
+        if (lane == 0) s_wcnt[warp] = __popc(bal);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned int tot = 0;
+            for (int k = 0; k < TPB / 32; k++) {
+                const unsigned int c = s_wcnt[k];
+                s_wcnt[k] = tot;
+                tot += c;
+            }
+            s_base = tot ? atomicAdd(T.cnt, tot) : 0u;
+        }
+        __syncthreads();
+        if (defer) {
+            const unsigned int pos = s_base + s_wcnt[warp] + __popc(bal & ((1u << lane) - 1u));
+            if (pos < T.cap2) {
+                T.q2[pos] = i;
+                T.l2[pos] = w;
+                T.m2[pos] = mask;
+            } else {
+                T.cnt[2] = 1;  // the tier-3 sweep labels it
+            }
+        }
+        __syncthreads();  // s_wcnt / s_base and the staged slices are rewritten next round
+    }
+    allow_dependents();
+    if (threadIdx.x == 0 && s_broken) {
+        atomicAdd(&g_tma_timeouts, 1u);
+        mbar_wait(&s_bar, phase ^ 1u);  // the copy whose wait ran out
+    }
+    if (ctr) count_stats(ctr, inside, boundary, fp64, 0);
+}
+
 // Tier 2's shape: blocks of 128 threads, five per SM (96 registers, about
 // 60 bytes spilled) hold 20 warps per SM where 256-thread blocks at 110
 // registers held 16: FP64-filter queries of C2 (tier 2 over the whole
@@ -1887,13 +2106,14 @@ __global__ void __launch_bounds__(T2_TPB, T2_BLOCKS) k_leaf_t2(VS vs, const doub
     const unsigned int m = min(*src_count, src_cap);
     const uint32_t* sp = src;
     const uint32_t* sl = src_leaf;
-    if (FROM_PASS1) first_tier_source(T, sp, sl);
+    unsigned int st = 1;
+    if (FROM_PASS1) first_tier_source(T, sp, sl, st);
     int inside = 0, boundary = 0, exact = 0;
     for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
-        const uint32_t i = sp[t];
+        const uint32_t i = sp[t * st];
         const QueryView& Q = vs.of(i);
         PointCtx P;
-        const uint32_t w = point_leaf(Q, ll[i], P, sl[t]);
+        const uint32_t w = point_leaf(Q, ll[i], P, sl[t * st]);
         uint8_t lab;
         if ((w & KIND_MASK) == KIND_PURE) {
             lab = (uint8_t)(w & 3u);
@@ -2093,7 +2313,9 @@ __global__ void __launch_bounds__(P_TPB) k_part_scatter(const uint32_t* __restri
 //   k_ls_tile_sums  the counts' sums per tile of LS_TILE leaves;
 //   k_ls_scan       each block scans one tile, starting from the sum of the
 //                   tiles before it (no waits between blocks);
-//   k_ls_scatter    each entry goes to its leaf's start plus its rank.
+//   k_ls_scatter    each entry goes to its leaf's start plus its rank, point
+//                   index and leaf word as one 8-byte pair (one random store
+//                   per entry, where two arrays took two).
 // The counts, ranks and the sorted arrays of a C2 pass fit in L2, so the
 // random atomics and writes of the sort do not reach DRAM.
 constexpr int LS_TPB = 256;
@@ -2105,11 +2327,11 @@ struct LeafSortScratch {
     unsigned int* start;  // [nb + 1] exclusive prefix of cnt
     unsigned int* tsum;   // [tiles] sums of cnt per tile
     unsigned int* rank;   // [queue] an entry's rank in its bucket
-    uint32_t* spts;       // point indices in leaf order
-    uint32_t* sleaf;      // their leaf words
+    uint2* sent;          // (point index, leaf word) in leaf order: one 8-byte store per entry
     unsigned int* done;   // set to 1 with the sorted arrays; zero before the pass
     int nb;               // buckets: leaves + 1
     int tiles;            // ceil(nb / LS_TILE)
+    bool stage;           // tier 1 stages each tile's edge lists (k_leaf_t1s)
 };
 
 __device__ __forceinline__ int leaf_bucket(uint32_t w, int nb)
@@ -2211,8 +2433,7 @@ __global__ void __launch_bounds__(LS_TPB) k_ls_scatter(const uint32_t* __restric
             const uint32_t w = l1[t];
             const unsigned int at = S.start[leaf_bucket(w, S.nb)] + S.rank[t];
             if (at < m) {  // counts and entries agree; never write past the queue
-                S.spts[at] = queue[t];
-                S.sleaf[at] = w;
+                S.sent[at] = make_uint2(queue[t], w);
             }
         }
     }
@@ -2243,17 +2464,27 @@ void launch_dependent(void (*kernel)(KArgs...), int grid, cudaStream_t s, Args..
     launch_dependent_tpb(kernel, grid, TPB, s, args...);
 }
 
-// Tier counters (T.cnt[0..2]) must be zero.
+// Tier counters (T.cnt[0..2]) must be zero.  stage_t1 (one polygon, queue
+// in leaf order): tier 1 reads each tile's edge lists from shared memory
+// (k_leaf_t1s).
 template <class VS>
 void leaf_tiers_launch(const VS& vs, const double2* ll, uint8_t* out, const uint32_t* queue,
                        const unsigned int* qcount, const Tiers& T, int precision, unsigned long long* ctr, int sms,
-                       cudaStream_t s)
+                       cudaStream_t s, bool stage_t1 = false)
 {
     if (precision == GAHHG_QUERY_FP64_FILTER) {
         launch_dependent_tpb(k_leaf_t2<VS, true>, sms * T2_BLOCKS, T2_TPB, s, vs, ll, out, queue,
                              (const uint32_t*)T.l1, qcount, 0xffffffffu, T, ctr);
     } else {
-        launch_dependent(k_leaf_t1<VS>, sms * T1_BLOCKS, s, vs, ll, out, queue, qcount, T, ctr);
+        bool staged = false;
+        if constexpr (std::is_same<VS, OneView>::value) {
+            if (stage_t1) {
+                launch_dependent(k_leaf_t1s, sms * T1S_BLOCKS, s, vs.Q, ll, out, queue, qcount, T, ctr,
+                                 (int)knob(GAHHG_KNOB_STAGING_POLL_LIMIT));
+                staged = true;
+            }
+        }
+        if (!staged) launch_dependent(k_leaf_t1<VS>, sms * T1_BLOCKS, s, vs, ll, out, queue, qcount, T, ctr);
         launch_dependent_tpb(k_leaf_t2<VS, false>, sms * T2_BLOCKS, T2_TPB, s, vs, ll, out, (const uint32_t*)T.q2,
                              (const uint32_t*)T.l2, (const unsigned int*)T.cnt, T.cap2, T, ctr);
     }
@@ -4075,12 +4306,13 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
     tier_caps(chunk, &cap2, &cap3);
     const long long order = knob(GAHHG_KNOB_GROUPED_PASS2);
     const bool windows = order == 1 && Q.nparts > 1 && chunk >= PART_MIN_QUEUE;
-    const bool leaves = order == 2 && chunk >= PART_MIN_QUEUE && g->lattice->nleaves > 0 &&
+    const bool leaves = (order == 2 || order == 3) && chunk >= PART_MIN_QUEUE && g->lattice->nleaves > 0 &&
                         g->lattice->nleaves < (1LL << 30);
     const int nb = leaves ? (int)g->lattice->nleaves + 1 : 0;
     const int tiles = (nb + LS_TILE - 1) / LS_TILE;
     const size_t l1_at = (size_t)chunk + 192;
-    const size_t sorted_at = l1_at + (size_t)chunk + 3 * (size_t)cap2 + 2 * (size_t)cap3;
+    // even, so that the leaf order's (point, leaf word) pairs are 8-byte aligned
+    const size_t sorted_at = (l1_at + (size_t)chunk + 3 * (size_t)cap2 + 2 * (size_t)cap3 + 1) & ~(size_t)1;
     const size_t ls_at = sorted_at + 2 * (size_t)chunk;
     const size_t words = windows ? ls_at : leaves ? ls_at + 2 * (size_t)nb + 1 + tiles + (size_t)chunk : sorted_at;
     uint32_t* queue = nullptr;
@@ -4106,14 +4338,14 @@ gahhg_status lattice_query(Grid* g, const double* d_lonlat, size_t n, uint8_t* d
     W.scale = Q.part_scale;
     LeafSortScratch LS;
     LS.done = qcount + 4;
-    LS.spts = queue + sorted_at;
-    LS.sleaf = queue + sorted_at + chunk;
+    LS.sent = (uint2*)(queue + sorted_at);
     LS.cnt = queue + ls_at;
     LS.start = LS.cnt + nb;
     LS.tsum = LS.start + nb + 1;
     LS.rank = LS.tsum + tiles;
     LS.nb = nb;
     LS.tiles = tiles;
+    LS.stage = order == 3;
     const gahhg_status st = lattice_query_with(Q, d_lonlat, (long long)n, d_labels, precision, s, d_counters,
                                                queue, qcount, chunk, g->device, &T, windows ? &W : nullptr,
                                                leaves ? &LS : nullptr);
@@ -4165,10 +4397,12 @@ gahhg_status lattice_query_with(const QueryView& Q, const double* d_lonlat, long
             launch_dependent_tpb(k_ls_scan, std::min(lsort->tiles, sms * 8), LS_TPB, s, qc, *lsort);
             launch_dependent_tpb(k_ls_scatter, sms * 8, LS_TPB, s, (const uint32_t*)queue, l1, qc, *lsort);
             Tiers T = *tiers;
-            T.spts = lsort->spts;
-            T.sleaf = lsort->sleaf;
+            T.spts = (const uint32_t*)lsort->sent;
+            T.sleaf = T.spts + 1;
+            T.sstride = 2;
             T.sorted = lsort->done;
-            leaf_tiers_launch(OneView{Q}, ll, d_labels + off, queue, qcount, T, precision, ctr, sms, s);
+            leaf_tiers_launch(OneView{Q}, ll, d_labels + off, queue, qcount, T, precision, ctr, sms, s,
+                              lsort->stage);
         } else if (tiers) {
             leaf_tiers_launch(OneView{Q}, ll, d_labels + off, queue, qcount, *tiers, precision, ctr, sms, s);
         }

@@ -354,10 +354,12 @@ gahhg_status gahhg_result_write(const char* path, const uint8_t* labels, size_t 
 /* The level-0 grid (80 vertices, 240 borders, 42 cells). */
 gahhg_status gahhg_grid0_export(double* v, void* b, void* c);
 
-/* Pass-1 (locate) blocks on `device` whose bulk copy (TMA) of the coarse
- * summary into shared memory did not complete within the bounded wait, since
- * the library was loaded.  Such a block loads the summary with plain loads
- * instead, so labels are unaffected; 0 in normal operation. */
+/* Blocks on `device` whose bulk copy (TMA) into shared memory did not
+ * complete within the bounded wait, since the library was loaded: pass-1
+ * (locate) blocks staging the coarse summary, and tier-1 blocks staging a
+ * tile's leaf and edge records (pass-2 order 3).  Such a block loads the
+ * data with plain loads instead, so labels are unaffected; 0 in normal
+ * operation. */
 gahhg_status gahhg_staging_fallbacks(int device, unsigned long long* count);
 
 /* Process-wide tuning and test knobs.  No counterpart in the reference.
@@ -365,7 +367,9 @@ gahhg_status gahhg_staging_fallbacks(int device, unsigned long long* count);
  * points that pass 1 of a single-polygon exact query could not label, when
  * there are at least 2^18 of them: 0 (default) input order; 1 windows of
  * consecutive leaves (about 24 MB of index each; only when the index spans
- * several windows); 2 leaf order (a counting sort by leaf).  Labels are the
+ * several windows); 2 leaf order (a counting sort by leaf); 3 leaf order, with
+ * the first (FP32) tier reading each tile's leaf and edge records from shared
+ * memory, where one bulk copy (TMA) per tile staged them.  Labels are the
  * same in every order.
  * Values take effect for work enqueued after the call. */
 typedef enum {
@@ -378,7 +382,8 @@ typedef enum {
      *                     tile before summing that tile's inputs itself
      *                     (counted in scan_fallbacks) [4,194,304];
      * STAGING_POLL_LIMIT  polls a pass-1 block waits for the bulk copy of the
-     *                     coarse summary before reading it from global memory
+     *                     coarse summary, and a staging tier-1 block for a
+     *                     tile's records, before reading global memory instead
      *                     (counted by gahhg_staging_fallbacks) [1,048,576]. */
     GAHHG_KNOB_WALK_STEP_LIMIT = 2,
     GAHHG_KNOB_SCAN_SPIN_LIMIT = 3,

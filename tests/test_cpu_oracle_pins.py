@@ -175,11 +175,11 @@ def test_knobs_host_side():
     assert G.get_knob(G.KNOB_WALK_STEP_LIMIT) == 1 << 16
     assert G.get_knob(G.KNOB_SCAN_SPIN_LIMIT) == 1 << 22
     assert G.get_knob(G.KNOB_STAGING_POLL_LIMIT) == 1 << 20
-    for k, bad in [(G.KNOB_GROUPED_PASS2, 3), (G.KNOB_GROUPED_PASS2, -1), (G.KNOB_WALK_STEP_LIMIT, -1),
+    for k, bad in [(G.KNOB_GROUPED_PASS2, 4), (G.KNOB_GROUPED_PASS2, -1), (G.KNOB_WALK_STEP_LIMIT, -1),
                    (G.KNOB_SCAN_SPIN_LIMIT, 1 << 23), (0, 1), (99, 1)]:
         with pytest.raises(G.GahhgError):
             G.set_knob(k, bad)
-    for mode in (2, 1, 0):
+    for mode in (3, 2, 1, 0):
         G.set_knob(G.KNOB_GROUPED_PASS2, mode)
         assert G.get_knob(G.KNOB_GROUPED_PASS2) == mode
     old = G.set_knob(G.KNOB_WALK_STEP_LIMIT, 1)

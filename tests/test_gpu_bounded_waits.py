@@ -13,7 +13,12 @@ gahhg_set_knob lowered), on the GPU, without a fault:
   summary staging      every pass-1 block gives up at once on the bulk copy of
                        the coarse summary and reads it from global memory: the
                        labels are unchanged and gahhg_staging_fallbacks counts
-                       the blocks (single polygons and batches).
+                       the blocks (single polygons and batches);
+  edge-list staging    every tier-1 block over a leaf-ordered queue (pass-2
+                       order 3) gives up at once on the bulk copy of its
+                       tile's leaf and edge records and reads them from global
+                       memory: the labels and tier counts are unchanged and
+                       the blocks are counted on top of the pass-1 ones.
 
 Each knob is put back to its default whatever the outcome.  The reference's
 walks are unbounded (source/GPISPAHHG.cu:736,872,1210); its scan and staging
@@ -101,3 +106,32 @@ def test_summary_staging_runs_out():
     assert np.array_equal(got, want)
     assert np.array_equal(lab.cpu().numpy(), want_b)
     assert mid > before and after > mid
+
+
+def test_edge_list_staging_runs_out():
+    import torch
+    # a C1-style polygon a tenth the size, so that a tile of the leaf-ordered
+    # queue of 1e6 C2 points spans few enough leaves to be staged
+    rings = synth.c1_polygon(n_outer=100_000, hole_n=1_000)
+    g = G.Grid(G.Polygon.from_rings(rings), semantics=G.SEMANTICS_EXACT, device=0).classify()
+    d = synth.device_c2_points(rings, 1_000_000, 17, "cuda:0")
+    lab = torch.empty(d.shape[0], dtype=torch.uint8, device="cuda")
+
+    def run(order):
+        with knob(G.KNOB_GROUPED_PASS2, order):
+            lab.fill_(9)
+            before = G.staging_fallbacks(0)
+            g.query_device(d.data_ptr(), d.shape[0], lab.data_ptr(), G.QUERY_FP32_FILTER, sync=True)
+            return lab.cpu().numpy(), g.stats(), G.staging_fallbacks(0) - before
+
+    want, sw, f0 = run(0)
+    assert f0 == 0
+    got, sg, f3 = run(3)
+    assert f3 == 0 and np.array_equal(got, want)
+    with knob(G.KNOB_STAGING_POLL_LIMIT, 0):
+        _, _, f2 = run(2)       # pass-1 blocks only
+        late, sl, f3 = run(3)   # and the staging tier-1 blocks
+    assert np.array_equal(late, want)
+    for k in ("boundary_points", "esc_fp64", "esc_exact", "in_count"):
+        assert sl[k] == sw[k] == sg[k], k
+    assert f2 > 0 and f3 > f2

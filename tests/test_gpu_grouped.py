@@ -1,9 +1,10 @@
 """The pass-1 queue put in leaf-window order before the tiers run
 (knob GAHHG_KNOB_GROUPED_PASS2 = 1; k_part_count / k_part_scatter: a
 counting sort of the queue by window of consecutive leaves, each window
-about 24 MB of index records) or in leaf order (= 2; k_ls_*: a counting sort
-by leaf) against the tiers over the queue in pass-1 order (= 0, the
-default): the same labels and the same per-tier escalation counts, for both
+about 24 MB of index records), in leaf order (= 2; k_ls_*: a counting sort
+by leaf) or in leaf order with tier 1 reading each tile's leaf and edge
+records from shared memory, staged there by bulk copies (= 3; k_leaf_t1s),
+against the tiers over the queue in pass-1 order (= 0, the default): the same labels and the same per-tier escalation counts, for both
 precisions, on near-edge points of the 1.1M-edge C1 polygon (a long queue:
 ordered) and on uniform points and the shipped NA0 polygon (short queues or
 one window: pass-1 order kept).  Labels are also checked against the exact
@@ -40,10 +41,10 @@ def c1_grid():
     return rings, P, G.Grid(P, semantics=G.SEMANTICS_EXACT, device=0).classify()
 
 
-ORDERS = {1: "leaf-window", 2: "leaf"}
+ORDERS = {1: "leaf-window", 2: "leaf", 3: "leaf (tier 1 on staged edge lists)"}
 
 
-@pytest.mark.parametrize("order", [1, 2])
+@pytest.mark.parametrize("order", [1, 2, 3])
 @pytest.mark.parametrize("prec", [G.QUERY_FP32_FILTER, G.QUERY_FP64_FILTER])
 def test_grouped_equals_per_point_c2(c1_grid, prec, order):
     rings, _P, g = c1_grid
@@ -61,7 +62,7 @@ def test_grouped_equals_per_point_c2(c1_grid, prec, order):
                                sa["boundary_points"], sa["esc_fp64"], sa["esc_exact"]))
 
 
-@pytest.mark.parametrize("order", [1, 2])
+@pytest.mark.parametrize("order", [1, 2, 3])
 def test_grouped_equals_per_point_uniform(c1_grid, order):
     _rings, _P, g = c1_grid
     pts = synth.device_points(4_000_000, 11, "cuda:0")
@@ -83,7 +84,7 @@ def test_grouped_against_oracle_small(inputs, tmp_path):
     q = np.concatenate([inputs.query("uniform"), synth.near_edge_points(rings, 40_000, rng)])
     d = torch.from_numpy(q).cuda()
     want = E.query_lonlat(q)
-    for order in (1, 2):
+    for order in (1, 2, 3):
         for prec in (G.QUERY_FP32_FILTER, G.QUERY_FP64_FILTER):
             a, _ = _run(g, d, prec, order)
             assert np.array_equal(a, want), (order, prec)
