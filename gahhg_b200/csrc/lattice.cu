@@ -1284,9 +1284,10 @@ constexpr int T2_GROUP = 4;
 __device__ uint8_t leaf_label_fp64(const QueryView& Q, uint32_t leaf, PointCtx& P, uint32_t mask = MASK_ALL)
 {
     const LeafRec L = Q.leaves[leaf];
-    P.need64();
+    // the leaf's loads go out before the point's canonical XYZ is computed
     const double LR[3] = {__ldg(Q.leafR + 3 * (size_t)leaf), __ldg(Q.leafR + 3 * (size_t)leaf + 1),
                           __ldg(Q.leafR + 3 * (size_t)leaf + 2)};
+    P.need64();
     const bool all = mask == MASK_ALL;
     const int cnt = L.cnt;
     int par = all ? 0 : (int)(mask >> 31);
@@ -1843,15 +1844,21 @@ __global__ void __launch_bounds__(TPB, T1_BLOCKS) k_leaf_t1(VS vs, const double2
         uint32_t i = 0, w = 0, mask = 0;
         if (t < m) {
             i = src[t * st];
+            const uint32_t known = src_leaf[t * st];
             const QueryView& Q = vs.of(i);
+            // the leaf record (a point pass 1 located in a leaf) is loaded
+            // with the point's coordinates, not after them
+            const bool in_leaf = (known & KIND_MASK) == KIND_LEAF;
+            LeafRec L0;
+            if (in_leaf) L0 = Q.leaves[known & INDEX_MASK];
             PointCtx P;
-            w = point_leaf(Q, ll[i], P, src_leaf[t * st]);
+            w = point_leaf(Q, ll[i], P, known);
             uint8_t lab;
             if ((w & KIND_MASK) == KIND_PURE) {
                 lab = (uint8_t)(w & 3u);
             } else {
                 boundary++;
-                lab = leaf_label_fp32(Q, Q.leaves[w & INDEX_MASK], P, mask);
+                lab = leaf_label_fp32(Q, in_leaf ? L0 : Q.leaves[w & INDEX_MASK], P, mask);
             }
             if (lab == LABEL_DEFER) {
                 fp64++;
