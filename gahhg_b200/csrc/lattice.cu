@@ -1916,7 +1916,11 @@ __global__ void __launch_bounds__(TPB, T1_BLOCKS) k_leaf_t1(VS vs, const double2
 // g_tma_timeouts, and before exiting the block waits (bounded again) for
 // that copy.  Both slices start on 16-byte boundaries (pool allocations are
 // 256-byte aligned; leaf records are 32 bytes, edge records 16) and their
-// sizes are multiples of 16 bytes.
+// sizes are multiples of 16 bytes.  Measured on 2e7 C2 points (9.1M queued):
+// 337 us against 283 us for k_leaf_t1 on the same leaf-ordered queue, whose
+// per-warp gathers leaf order already makes one request per warp and leaf;
+// the staging adds a block barrier and a wait per tile and copies every
+// leaf of the tile's range.  It is therefore an option (pass-2 order 3).
 constexpr int T1S_LEAVES = 256;  // 8 KB of leaf records per tile
 constexpr int T1S_RECS = 1536;   // 24 KB of edge records per tile
 constexpr int T1S_BLOCKS = 5;
