@@ -1287,14 +1287,15 @@ __device__ uint8_t leaf_label_fp64(const QueryView& Q, uint32_t leaf, PointCtx& 
     // the leaf's loads go out before the point's canonical XYZ is computed
     const double LR[3] = {__ldg(Q.leafR + 3 * (size_t)leaf), __ldg(Q.leafR + 3 * (size_t)leaf + 1),
                           __ldg(Q.leafR + 3 * (size_t)leaf + 2)};
-    P.need64();
     const bool all = mask == MASK_ALL;
     const int cnt = L.cnt;
     int par = all ? 0 : (int)(mask >> 31);
     uint32_t sel = all ? 0u : (mask & 0x7fffffffu);
-    for (int k0 = 0; all ? k0 < cnt : sel != 0u; k0 += T2_GROUP) {
-        // the next T2_GROUP records: consecutive ones, or the next set bits of sel
-        int kk[T2_GROUP];
+    int kk[T2_GROUP];
+    uint32_t es[T2_GROUP];
+    // the next T2_GROUP records (consecutive ones, or the next set bits of
+    // sel) and their edge words
+    auto next_group = [&](int k0) {
 #pragma unroll
         for (int j = 0; j < T2_GROUP; j++) {
             if (all) {
@@ -1306,10 +1307,15 @@ __device__ uint8_t leaf_label_fp64(const QueryView& Q, uint32_t leaf, PointCtx& 
                 kk[j] = -1;
             }
         }
-        uint32_t es[T2_GROUP];
-        double2 e[T2_GROUP][3];
 #pragma unroll
         for (int j = 0; j < T2_GROUP; j++) es[j] = kk[j] >= 0 ? __ldg(Q.eids + L.off + kk[j]) : 0u;
+    };
+    // the first group's edge words are in flight while the point's canonical
+    // XYZ is computed
+    next_group(0);
+    P.need64();
+    for (int k0 = 0; kk[0] >= 0; k0 += T2_GROUP) {
+        double2 e[T2_GROUP][3];
 #pragma unroll
         for (int j = 0; j < T2_GROUP; j++) {
             if (kk[j] >= 0) {
@@ -1337,6 +1343,8 @@ __device__ uint8_t leaf_label_fp64(const QueryView& Q, uint32_t leaf, PointCtx& 
             if (s4 == 0) return LABEL_DEFER;
             if (s4 == -s2) par ^= 1;
         }
+        if (all ? k0 + T2_GROUP >= cnt : sel == 0u) break;
+        next_group(k0 + T2_GROUP);
     }
     return (uint8_t)(par ? 3 - L.label : L.label);
 }
