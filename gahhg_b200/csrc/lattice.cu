@@ -2043,7 +2043,7 @@ __global__ void __launch_bounds__(TPB, T1S_BLOCKS) k_leaf_t1s(QueryView Q, const
         if (nl) {
             staged = mbar_wait(&s_bar, phase, polls);
             phase ^= 1u;
-            if (!staged) s_broken = 1;
+            if (!staged) atomicOr(&s_broken, 1);  // any thread whose wait ran out
         }
         if (t < m) {
             uint8_t lab;
