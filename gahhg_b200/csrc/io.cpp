@@ -449,6 +449,16 @@ gahhg_status load_points_file(const char* path, Points* T)
     }
     const char* base = f.data;
     const char* end = base + f.size;
+    // The reference reads each line with getline(buf, size), size = the
+    // file's size, which stores at most size - 1 characters: a non-empty file
+    // without any '\n' (one line, no line end) fails on its first line, and
+    // the reference's loop stops there with no points and no error.
+    if (f.size > 0 && !memchr(base, '\n', f.size)) {
+        T->lonlat.reset();
+        T->n = 0;
+        T->path = path;
+        return GAHHG_OK;
+    }
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     const int nt = (int)std::min<size_t>(std::min(hw, 64u), std::max<size_t>(1, f.size >> 22));  // >= 4 MB each
     std::vector<const char*> cut(nt + 1);

@@ -212,3 +212,30 @@ def test_polygon_edge_cases_match_reference(text, tmp_path, capfd, oracle_ref):
     assert (ours is None) == (ref is None)
     if ours is not None:
         assert np.array_equal(ours[0], ref[0]) and np.array_equal(ours[1], ref[1])
+
+
+@pytest.mark.parametrize("text", ["1,2", "1,2\n", "1,2\n3,4", "1,2\r3,4\r", "170.5,-3.25 tail", "x,y"])
+def test_points_line_ends_match_reference_program(text, tmp_path, oracle_ref):
+    """The number of points the reference program reads (its result CSV has
+    one line per point) for files whose last line has no line end: a file
+    without any '\\n' is read as no points, since getline(buf, size) stores
+    at most size - 1 characters of its only line and then fails."""
+    import subprocess
+    poly = tmp_path / "sq.txt"
+    poly.write_text("POLYGON 1 0\n0 5\n0 0\n10 0\n10 10\n0 10\n0 0\n")
+    csv = tmp_path / "q.csv"
+    with open(csv, "w", newline="") as f:
+        f.write(text)
+    res = tmp_path / "res.csv"
+    r = subprocess.run([oracle_ref.REF_EXE, "/polyfile", str(poly), "/tpfile", str(csv), "/reportfile",
+                        str(tmp_path / "rep.txt"), "/resultfile", str(res)], capture_output=True, text=True,
+                       timeout=120, cwd=str(tmp_path))
+    try:
+        ours = len(G.load_points(str(csv)))
+    except G.GahhgError:
+        ours = None
+    if r.returncode != 0:
+        assert ours is None, (text, r.stdout)
+        return
+    with open(res) as f:
+        assert ours == len(f.read().splitlines()), (text, ours)
