@@ -367,11 +367,13 @@ struct MappedFile {
 
 inline bool in_line_space(char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\v' || c == '\f'; }
 
-// The serial loader's reading of one line [s, e) ("%lf,%lf": strtod for each
-// number, ',' right after the first, anything after the second ignored), on
-// a NUL-terminated copy: a number never spans a line end, and where strtod
-// skipped white space into the next line the line was rejected anyway.
-bool parse_point_strtod(const char* s, const char* e, double* lo, double* la)
+// The reference's reading of one line [s, e): sscanf(line, "%lf,%lf") of the
+// platform's C library, as GPISPTP::loadTPFromCSV does (source/GPISPTP.cu:
+// 36), on a NUL-terminated copy of the line.  (glibc's %lf takes the digits
+// of a number whose exponent has no digits, "1e,2" -> 1, 2, where strtod
+// would stop before the 'e'; reading through sscanf keeps the reference's
+// answer on every such line.)
+bool parse_point_scanf(const char* s, const char* e, double* lo, double* la)
 {
     char small[256];
     std::string big;
@@ -384,17 +386,12 @@ bool parse_point_strtod(const char* s, const char* e, double* lo, double* la)
         memcpy(small, s, len);
         small[len] = 0;
     }
-    const char* le = buf + len;
-    char* q;
-    *lo = strtod(buf, &q);
-    if (q == buf || q >= le || *q != ',') return false;
-    const char* p = q + 1;
-    *la = strtod(p, &q);
-    return q != p && q <= le;
+    return sscanf(buf, "%lf,%lf", lo, la) == 2;
 }
 
-// Fast path for the usual "lon,lat" line; false sends the line to the serial
-// reading above (a '+' sign, hex, out-of-range values, unusual separators).
+// Fast path for the usual "lon,lat" line; false sends the line to the
+// reading above (a '+' sign, hex, out-of-range values, an exponent without
+// digits, unusual separators).
 inline bool parse_point_fast(const char* s, const char* e, double* lo, double* la)
 {
     const char* p = s;
@@ -437,7 +434,8 @@ int64_t mtime_ns(const struct stat& st) { return (int64_t)st.st_mtim.tv_sec * 10
 // GPISPTP::loadTPFromCSV (source/GPISPTP.cu:13-79).  The file is mapped and
 // split at line starts into one chunk per host thread; a first pass counts
 // each chunk's lines, a second parses them in place.  Values and the first
-// rejected line (and its message) are those of a serial strtod reading.
+// rejected line (and its message) are those of the reference's serial
+// sscanf("%lf,%lf") reading.
 gahhg_status load_points_file(const char* path, Points* T)
 {
     printf("Load test points from a CSV file: %s.\n", path);
@@ -495,7 +493,7 @@ gahhg_status load_points_file(const char* path, Points* T)
             const char* e = (const char*)memchr(s, '\n', ce - s);
             if (!e) e = ce;
             double lo, la;
-            if (!parse_point_fast(s, e, &lo, &la) && !parse_point_strtod(s, e, &lo, &la)) {
+            if (!parse_point_fast(s, e, &lo, &la) && !parse_point_scanf(s, e, &lo, &la)) {
                 bad[t] = first[t] + k;
                 return;
             }

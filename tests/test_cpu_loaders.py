@@ -1,6 +1,7 @@
 """The CSV point loader (GPISPTP::loadTPFromCSV, source/GPISPTP.cu:13-79):
 parsed by all host threads, it must give the values and the rejected line of
-the reference's serial "%lf,%lf" reading, on small files (one thread) and on
+the reference's serial sscanf("%lf,%lf") reading (the platform's C library,
+as in the reference built for the CPU here), on small files (one thread) and on
 files large enough to be split into chunks; binary sidecars must round-trip
 and be ignored once the CSV changes.  Host code only.
 """
@@ -30,7 +31,9 @@ def test_line_forms(tmp_path):
         ("180.000001,-90.000000\r", (180.000001, -90.0)),  # CRLF files
         ("12,13,14", (12.0, 13.0)),                    # anything after the second number is ignored
         ("5,6 junk", (5.0, 6.0)),
-        ("1e,2", None),                                # "1" then 'e': not followed by ','
+        ("1e,2", (1.0, 2.0)),                          # glibc's %lf, as the reference built here: "1e" -> 1
+        ("1.5e-,3", (1.5, 3.0)),
+        ("0x,1", None),                                # no digits after "0x": rejected
         ("0.1,1e-320", (0.1, 1e-320)),                 # subnormal
         ("inf,-inf", (math.inf, -math.inf)),
         ("170.12345678901234567,-0.000000000000000001", (170.12345678901234567, -1e-18)),
@@ -239,3 +242,45 @@ def test_points_line_ends_match_reference_program(text, tmp_path, oracle_ref):
         return
     with open(res) as f:
         assert ours == len(f.read().splitlines()), (text, ours)
+
+
+def test_points_files_match_reference_program(tmp_path, oracle_ref):
+    """Seeded files of valid and malformed lines (other separators, blanks,
+    signs, hex, exponents, trailing text, CR LF ends, a missing last line
+    end): the reference program built for the CPU and this loader accept the
+    same files with the same number of points, or name the same first bad
+    line."""
+    import random
+    import re
+    import subprocess
+    forms = ["1.5,2.5", "-10.25,3e-3", "\t-1,2", "+4,5", "0x1p3,7", "1e,2", "1;2", "1 2", "", " ", "a,b",
+             "12,13,14", "5,6 junk", "inf,-inf", "3,", ",3", "170.123456789012345,-0.5", "-0,0", "1e308,1e-308"]
+    poly = tmp_path / "sq.txt"
+    poly.write_text("POLYGON 1 0\n0 5\n0 0\n10 0\n10 10\n0 10\n0 0\n")
+    rng = random.Random(4242)
+    csv = tmp_path / "q.csv"
+    res = tmp_path / "res.csv"
+    for case in range(150):
+        lines = [rng.choice(forms) for _ in range(rng.randint(1, 6))]
+        sep = rng.choice(["\n", "\n", "\r\n"])
+        text = sep.join(lines) + (sep if rng.random() < 0.7 else "")
+        with open(csv, "w", newline="") as f:
+            f.write(text)
+        if res.exists():
+            res.unlink()
+        r = subprocess.run([oracle_ref.REF_EXE, "/polyfile", str(poly), "/tpfile", str(csv), "/reportfile",
+                            str(tmp_path / "rep.txt"), "/resultfile", str(res)], capture_output=True, text=True,
+                           timeout=120, cwd=str(tmp_path))
+        m = re.search(r"Error\. Line (\d+) of .*\. Wrong format\.", r.stdout)
+        try:
+            ours = len(G.load_points(str(csv)))
+            ours_bad = None
+        except G.GahhgError as e:
+            ours = None
+            ours_bad = int(re.search(r"line (\d+) ", str(e)).group(1))
+        if m:
+            assert ours_bad == int(m.group(1)), (case, repr(text), ours_bad, m.group(1))
+        else:
+            assert r.returncode == 0 and ours is not None, (case, repr(text), r.stdout[-300:])
+            with open(res) as f:
+                assert ours == len(f.read().splitlines()), (case, repr(text), ours)
