@@ -57,3 +57,16 @@ extern "C" void local_signs(const double* cfg, long n, int* out)
         s[3] = local_frame::record_crossing(t, r[0], r[1], r[2], r[3]);
     }
 }
+
+// The kernels' exact predicate for the rational-arithmetic test
+// (tests/test_cpu_oracle_exact_sign.py): out[2i] = the exact sign of
+// det[a; b; c] by expansions (stage 2, 0 when it vanishes), out[2i+1] =
+// orient (stages 1-3, simulation of simplicity for a vanishing determinant).
+extern "C" void exact_signs(const double* xyz, long n, int* out)
+{
+    for (long i = 0; i < n; i++) {
+        const double* a = xyz + 9 * i;
+        out[2 * i] = gahhg::exact::det3_sign(a, a + 3, a + 6);
+        out[2 * i + 1] = gahhg::exact::orient(a, a + 3, a + 6);
+    }
+}

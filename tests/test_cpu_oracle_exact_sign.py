@@ -6,14 +6,23 @@ with fractions.Fraction from the same doubles.  Random, near-coplanar
 triples.  With simulation of simplicity the sign must equal the exact sign
 wherever that is not zero, never be zero for three distinct points (two
 identical points give 0: the callers apply the vertex rule before), and flip
-when two arguments are exchanged.  Host only; pins the oracle that every
-exact-label test relies on.
+when two arguments are exchanged.  The kernels' own predicate header
+(gahhg_b200/csrc/exact_pred.cuh, built for the host) is held to the same
+rational signs and to the oracle's separately written simulation of
+simplicity.  Host only; pins the oracle that every exact-label test relies
+on, and the exact tier's arithmetic.
 """
+import ctypes
+import os
+import subprocess
 from fractions import Fraction
 
 import numpy as np
+import pytest
 
 from oracle import exact
+
+HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def _exact_sign(a, b, c):
@@ -72,3 +81,38 @@ def test_orient_matches_rational_arithmetic():
             assert exact.orient(b, c, a, sos=True) == s, i
     # both the exact-zero and the near-degenerate branches were exercised
     assert zeros > 1000 and nonzero_near > 5000
+
+
+@pytest.fixture(scope="module")
+def kernel_signs(tmp_path_factory):
+    """The kernels' predicate header (gahhg_b200/csrc/exact_pred.cuh) built
+    for the host: (exact sign by expansions, orient with simulation of
+    simplicity) per triple."""
+    out = str(tmp_path_factory.mktemp("pred") / "libpred_probe.so")
+    subprocess.check_call(["g++", "-O2", "-ffp-contract=off", "-shared", "-fPIC", "-I",
+                           os.path.join(os.path.dirname(HERE), "include"), "-o", out,
+                           os.path.join(HERE, "native", "pred_probe.cpp")])
+    lib = ctypes.CDLL(out)
+    lib.exact_signs.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p]
+    lib.exact_signs.restype = None
+
+    def signs(triples):
+        xyz = np.ascontiguousarray(np.array([np.concatenate(t) for t in triples]), dtype=np.float64)
+        res = np.zeros((len(triples), 2), dtype=np.int32)
+        lib.exact_signs(xyz.ctypes.data, len(triples), res.ctypes.data)
+        return res
+    return signs
+
+
+def test_kernel_predicate_matches_rational_arithmetic_and_oracle(kernel_signs):
+    """The exact tier's own code (the header the kernels compile), built for
+    the host: its expansion sign equals rational arithmetic, and its
+    simulation of simplicity equals the oracle's separately written one."""
+    triples = _triples(15_000, 98)
+    got = kernel_signs(triples)
+    for i, (a, b, c) in enumerate(triples):
+        want = _exact_sign(a, b, c)
+        assert got[i, 0] == want, (i, got[i, 0], want)
+        assert got[i, 1] == exact.orient(a, b, c, sos=True), i
+        if want != 0:
+            assert got[i, 1] == want, i
